@@ -1,0 +1,185 @@
+"""Pin the CPU oracle to the reference.
+
+Fixtures in tests/golden/ were produced by running the reference's own Numba
+kernels (tests/golden/make_golden.py). The oracle restates each kernel with
+Numba's arithmetic types, so non-fastmath kernels must match bit for bit; the
+reference compiles red-black SOR, Gauss-Seidel and the emitters with
+fastmath=True (red_black_sor_gauss_seidel.py:8, gauss_seidel.py:8,
+emitters.py:37), which allows reassociation, so those get a few-ulp tolerance.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import GOLDEN, golden
+
+OPS_FILES = sorted(os.path.basename(f)[:-4] for f in glob.glob(os.path.join(GOLDEN, "ops_*.npz")))
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-30))
+
+
+def _fastmath_tol(dtype):
+    return 1e-6 if dtype == np.float32 else 1e-13
+
+
+def oracle_ops(d):
+    """Run every operator on the fixture's inputs; returns {name: output}."""
+    h, dt = float(d["h"]), float(d["dt"])
+    fl, fmu, fmv, solid = d["fl"], d["fmu"], d["fmv"], d["solid"]
+    out = {}
+    o = np.zeros_like(d["dens"])
+    O.advect_scalar_field(d["dens"], o, d["u"], d["v"], fl, dt, h)
+    out["adv_scalar"] = o
+    o = np.zeros_like(d["u"])
+    O.advect_velocity_u(d["u"], o, d["v"], fmu, dt, h)
+    out["adv_u"] = o
+    o = np.zeros_like(d["v"])
+    O.advect_velocity_v(d["v"], o, d["u"], fmv, dt, h)
+    out["adv_v"] = o
+    vv = d["v"].copy()
+    O.apply_forces(vv, d["dens"], d["temp"], dt, -0.5, 5.0, 1.0, 0.1)
+    out["forces_v"] = vv
+    tt = d["temp"].copy()
+    O.cool_temperature(tt, 0.1, 0.5, dt)
+    out["cool_t"] = tt
+    o = np.zeros_like(d["dens"])
+    O.compute_divergence(d["u"], d["v"], o, fmu, fmv, h)
+    out["divergence"] = o
+    alpha = O.alpha_coeff(h, 1.0, dt)
+    o = np.zeros_like(d["dens"])
+    O.compute_residual(d["p"], d["div"], fl, fmu, fmv, alpha, 0.25, o)
+    out["residual"] = o
+    uu, vv = d["u"].copy(), d["v"].copy()
+    O.apply_pressure_gradient(uu, vv, d["p"], fmu, fmv, 1.3, h, dt)
+    out["grad_u"], out["grad_v"] = uu, vv
+    uu, vv = d["u"].copy(), d["v"].copy()
+    O.enforce_boundary_conditions(uu, vv, solid)
+    out["bc_u"], out["bc_v"] = uu, vv
+    pp = np.zeros_like(d["p"])
+    O.jacobi_pressure_solver(pp, d["div"], fmu, fmv, 1.0, h, dt, iterations=23)
+    out["jacobi"] = pp
+    pp = d["p"].copy()
+    O.rb_sor_pressure_solver(pp, d["div"], fmu, fmv, 1.0, h, dt, iterations=9, omega=1.7)
+    out["rbsor"] = pp
+    pp = d["p"].copy()
+    O.rb_sor_pressure_solver(pp, d["div"], fmu, fmv, 1.0, h, dt, iterations=5, omega=0.0)
+    out["rbsor_auto"] = pp
+    pp = d["p"].copy()
+    O.gauss_seidel_pressure_solver(pp, d["div"], fmu, fmv, 1.0, h, dt, iterations=4)
+    out["gauss_seidel"] = pp
+    if "restrict" in d:
+        H, W = d["p"].shape
+        c = np.zeros((H // 2, W // 2), d["p"].dtype)
+        O.restrict_avg(d["p"], fl, c)
+        out["restrict"] = c
+        f = np.zeros_like(d["p"])
+        O.prolong(d["restrict"], fl, f)
+        out["prolong"] = f
+        out["coarsen"] = O.coarsen_solid_mask(~fl)
+    return out
+
+
+FASTMATH = {"rbsor", "rbsor_auto", "gauss_seidel"}
+
+
+@pytest.mark.parametrize("name", OPS_FILES)
+def test_oracle_operators_match_reference(name):
+    d = golden(name)
+    dtype = d["dens"].dtype
+    for key, val in oracle_ops(d).items():
+        if key in FASTMATH:
+            assert _rel(val, d[key]) <= _fastmath_tol(dtype), key
+        else:
+            assert np.array_equal(val, d[key]), f"{key} not bit-exact"
+
+
+def test_oracle_kat_square_uv_shapes():
+    d = golden("kat_square_uv")
+    for t in ("f32", "f64"):
+        o = np.zeros_like(d[f"{t}_src"])
+        O.advect_scalar_field(d[f"{t}_src"], o, d[f"{t}_u"], d[f"{t}_v"], d["fl"], 1.0, 1.0)
+        assert np.array_equal(o, d[f"{t}_out"])
+
+
+@pytest.mark.parametrize("dt_name", ["f32", "f64"])
+@pytest.mark.parametrize("case", ["jac", "sor", "jac5"])
+def test_oracle_multigrid_matches_reference(case, dt_name):
+    d = golden("multigrid")
+    kw = {
+        "jac": dict(smoother_type="jacobi", v_cycles=1, num_levels=4, smoother_iterations=2, coarsest_iterations=30),
+        "sor": dict(smoother_type="rb_sor_gauss_seidel", v_cycles=2, num_levels=3, smoother_iterations=2,
+                    coarsest_iterations=20),
+        "jac5": dict(smoother_type="jacobi", v_cycles=2, num_levels=5, smoother_iterations=3, coarsest_iterations=40),
+    }[case]
+    H = W = 32
+    fmu, fmv = O.face_masks_from_solid(O.box_solid(H, W))
+    div = d["div_" + dt_name]
+    p = np.zeros_like(div)
+    O.MultigridReference()(p, div, fmu, fmv, 1.0, 1.0 / H, 0.5 / H, **kw)
+    ref = d[f"mg_{case}_{dt_name}"]
+    if case == "sor":
+        assert _rel(p, ref) <= _fastmath_tol(div.dtype) * 10
+    else:
+        assert np.array_equal(p, ref)
+
+
+@pytest.mark.parametrize("approach", ["linear", "gaussian", "quadratic", "hard_cutoff"])
+def test_oracle_emitters_match_reference(approach):
+    d = golden("emitters")
+    f = np.zeros((24, 20), np.float32)
+    for _ in range(2):
+        O.emit_scalar(f, 1.7, 0.016, 8.5, 10.25, 5.5, approach)
+    assert _rel(f, d[approach + "_numba"]) <= 1e-6
+    assert _rel(f, d[approach + "_python"]) <= 1e-6
+
+
+SIM_CASES = {
+    "jacobi": (O.jacobi_pressure_solver, dict(iterations=30)),
+    "rbsor": (O.rb_sor_pressure_solver, dict(iterations=20, omega=1.8)),
+    "mg": (None, dict(smoother_type="jacobi", num_levels=3, v_cycles=2, smoother_iterations=2,
+                      coarsest_iterations=20)),
+    "gs": (O.gauss_seidel_pressure_solver, dict(iterations=10)),
+}
+
+
+@pytest.mark.parametrize("name", list(SIM_CASES))
+def test_oracle_substeps_match_reference(name):
+    d = golden("sim")
+    solver, kw = SIM_CASES[name]
+    sim = O.OracleSim(32, 32, 1 / 32, solver or O.MultigridReference(), kw)
+    sim.emitters.append(O.EmitterSpec((16, 6), 4.0, 3.0, 2.0, (0.3, 2.0), "linear"))
+    for step in range(8):
+        sim.substep(sim.dt)
+        if step in (0, 7):
+            for k, attr in (("density", "density"), ("u", "velocity_u"), ("v", "velocity_v"), ("p", "pressure"),
+                            ("t", "temperature"), ("div", "divergence"), ("res", "pressure_residual")):
+                got, ref = getattr(sim, attr), d[f"{name}_s{step}_{k}"]
+                if name == "rbsor":
+                    # fastmath SOR: ulp-level differences, amplified in the small post-projection divergence
+                    assert np.max(np.abs(got - ref)) <= 1e-5 * max(np.max(np.abs(ref)), 1.0), (step, k)
+                else:
+                    assert np.array_equal(got, ref), (step, k)
+
+
+def test_gmg_oracle_converges_on_box():
+    """The project's convergent multigrid: FP64 V(2,2) reaches 1e-10, mixed reaches 1e-8."""
+    H = W = 64
+    fmu, fmv = O.face_masks_from_solid(np.zeros((H, W), bool))
+    fl = O.is_fluid_from_faces(fmu, fmv)
+    rng = np.random.default_rng(0)
+    b = rng.standard_normal((H, W)) * fl
+    b[fl] -= b[fl].mean()
+    g = O.GMGOracle(fmu, fmv, fl)
+    p = np.zeros((H, W))
+    cycles, hist = g.solve(p, b, tol=1e-10, max_cycles=30)
+    assert hist[-1] <= 1e-10 and cycles <= 15
+    p2 = np.zeros((H, W))
+    cycles2, hist2 = g.solve(p2, b, tol=1e-8, max_cycles=30, precision="mixed")
+    assert hist2[-1] <= 1e-8 and cycles2 <= 15
