@@ -1,0 +1,333 @@
+"""Benchmark: cell-steps/s of the smoke step at 2048^2 with the mixed-precision solve.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload ``mixed_2048``: one SmokeSimulation2D substep of the 2048^2 four-source
+scene (float32 state), pressure solved by the convergent multigrid (V(2,2),
+red-black Gauss-Seidel omega 1.4, full weighting, bilinear prolongation, 8^2
+coarsest) with FP32 cycles inside FP64 iterative refinement to a relative residual
+of 1e-8, then projection and the reference's metrics tail. The same scene is also
+timed with a float64 state and an all-FP64 solve to the same residual ("fp64_gpu").
+
+A step runs on data resident in HBM (``value``); ``e2e`` repeats it through the
+public API with a pinned-host -> device copy of the step's source table and a
+device -> pinned-host read of the density field and solve residual every step. The
+working set (~190 MB) exceeds the 126 MB L2, so no explicit flush runs between
+steps. Multi-GPU (torchrun): the scene does not shard, so each rank advances its own
+replica (weak scaling) and ``value`` counts every rank's cells over the slowest
+rank's time.
+
+--impl reference times the CPU oracle (a C/OpenMP restatement of the reference's
+kernels plus the same multigrid) on the host cores: each step is one substep of the
+same scene; rank 0 alone runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-steps/s at 2048² mixed vs FP64 GPU at equal resid 1e-8; % HBM roofline"
+UNIT = "cell-steps/s"
+TOL = 1e-8
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 8:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[4 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ----------------------------------------------------------------------------- reference arm
+def cpu_oracle_steps(n_steps, warmup):
+    """Time the CPU oracle on the same scene: returns (seconds per step list, cycles, threads)."""
+    import numpy as np
+
+    import oracle as O
+
+    sg = importlib.import_module("python-game-engine_b200")
+    sc = sg.scenes.mixed_2048(steps=n_steps + warmup)
+    fmu, fmv = O.face_masks_from_solid(np.zeros((sc.H, sc.W), bool))
+    fl = O.is_fluid_from_faces(fmu, fmv)
+    gmg = O.GMGOracle(fmu, fmv, fl, coarsest=8, omega=1.4)
+    cycles = []
+
+    def solver(p, div, fmu_, fmv_, rho, h, dt, **_):
+        alpha = O.alpha_coeff(h, rho, dt)
+        b = alpha * div.astype(np.float64) * fl
+        p64 = np.zeros(p.shape)
+        c, _hist = gmg.solve(p64, b, tol=TOL, max_cycles=40, precision="mixed")
+        cycles.append(c)
+        p[:] = p64.astype(p.dtype)
+
+    sim = O.OracleSim(sc.H, sc.W, sc.cell_size, solver, {}, dtype=np.float32)
+    sim.dt, sim.gravity = sc.dt, sc.gravity
+    sim.plumes = [O.PlumeSpec(*row, seed=sc.seed) for row in sc.plumes]
+    times = []
+    for k in range(n_steps + warmup):
+        t0 = time.perf_counter()
+        sim.substep(sc.dt)
+        if k >= warmup:
+            times.append(time.perf_counter() - t0)
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return times, cycles[warmup:], threads
+
+
+def run_reference(args):
+    world, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    steps = max(1, args.steps)
+    times, cycles, threads = cpu_oracle_steps(steps, args.warmup)
+    cells = 2048 * 2048
+    value = cells * len(times) / sum(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
+        "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 state, f64/f32 mixed solve", "data": "synthetic",
+        "config": {"workload": "mixed_2048", "grid": [2048, 2048], "solver": "multigrid V(2,2) mixed IR",
+                   "tol": TOL, "mean_cycles": sum(cycles) / max(len(cycles), 1)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{len(times)} substeps of mixed_2048 on the CPU oracle (C/OpenMP restatement of "
+                                   f"the reference kernels + the same multigrid), after {args.warmup} warm-up"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    sg = importlib.import_module("python-game-engine_b200")
+    lib = sg._lib.load()
+    dev = torch.device("cuda", local)
+    sc = sg.scenes.mixed_2048(steps=args.steps)
+    cells = sc.cells
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def make(dtype, precision):
+        params = sg.GeometricMultigridParams(tol=TOL, max_cycles=40, precision=precision, omega=1.4)
+        return sg.scenes.make_sim(sc, "geometric_multigrid", params, dtype=dtype, device=dev)
+
+    solver = sg.get_solver("geometric_multigrid", "cuda")
+
+    def timed(sim, steps, warmup, e2e=False, sample_clocks=False):
+        stream = torch.cuda.current_stream()
+        host_table = host_density = dev_table = None
+        if e2e:
+            host_table = torch.tensor([p.row() for p in sim.plumes], dtype=torch.float64).pin_memory()
+            dev_table = torch.empty_like(host_table, device=dev)
+            sim.set_plume_table(dev_table)
+            host_density = torch.empty(sim.density.shape, dtype=sim.density.dtype).pin_memory()
+            host_res = torch.empty(1, dtype=torch.float64).pin_memory()
+        for _ in range(warmup):
+            if e2e:
+                dev_table.copy_(host_table, non_blocking=True)
+            sim.substep(sc.dt)
+        barrier()
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        l0 = lib.sg_launch_count()
+        cycles = []
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        start.record(stream)
+        for _ in range(steps):
+            if e2e:
+                dev_table.copy_(host_table, non_blocking=True)
+            sim.substep(sc.dt)
+            cycles.append(solver.last_cycles)
+            if e2e:
+                host_density.copy_(sim.density, non_blocking=True)
+                host_res.fill_(solver.last_relres)
+        end.record(stream)
+        barrier()
+        ms = start.elapsed_time(end)
+        launches = lib.sg_launch_count() - l0
+        clocks = sampler.stop() if sampler else None
+        if e2e:
+            sim.set_plume_table(None)
+            sim._plume_table = None
+        return ms, cycles, launches, clocks
+
+    # ---- mixed precision (headline)
+    sim = make(torch.float32, "mixed")
+    ms, cycles, launches, clocks = timed(sim, args.steps, args.warmup, sample_clocks=True)
+    ms_max = max_over_ranks(ms)
+    value = world * cells * args.steps / (ms_max / 1e3)
+    relres_ok = solver.converged
+    # ---- end to end through the public API with host buffers
+    ms_e2e, _, _, _ = timed(sim, args.steps, 1, e2e=True)
+    ms_e2e = max_over_ranks(ms_e2e)
+    e2e_value = world * cells * args.steps / (ms_e2e / 1e3)
+    h2d = 6 * 8 * len(sim.plumes)
+    d2h = sim.density.numel() * sim.density.element_size()
+    # ---- dominant kernel roofline: level-0 smoother of the mixed plan, timed alone with events
+    plan = next(iter(solver._plans.values()))
+    peak, peak_kind = _peaks()
+    H0, W0 = sc.H, sc.W
+    n_rep = 20
+    stream = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    sp = sg._lib.stream_ptr()
+    sg._lib.check(lib.sg_gmg_smooth_async(plan.handle, 0, 1, sp), "smooth")
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    for _ in range(n_rep):
+        sg._lib.check(lib.sg_gmg_smooth_async(plan.handle, 0, 1, sp), "smooth")
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    half_sweep_ms = ev[0].elapsed_time(ev[1]) / (2 * n_rep)
+    # algorithmic bytes of one half sweep (float32): read every e (S N), read this colour's b
+    # (S N / 2), write this colour's e (S N / 2) = 2 S N
+    alg_bytes = 2 * 4 * H0 * W0
+    achieved = alg_bytes / (half_sweep_ms / 1e3) / 1e9
+    # ---- all-FP64 GPU path at the same residual
+    del sim
+    torch.cuda.empty_cache()
+    sim64 = make(torch.float64, "fp64")
+    ms64, cycles64, _, _ = timed(sim64, args.steps, args.warmup)
+    ms64 = max_over_ranks(ms64)
+    value64 = world * cells * args.steps / (ms64 / 1e3)
+    fp64_ok = solver.converged
+    del sim64
+    # ---- CPU baseline on a bounded sample (rank 0, one GPU only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        times, ccyc, threads = cpu_oracle_steps(args.cpu_steps, 1)
+        cpu = {"value": cells * len(times) / sum(times), "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{len(times)} substeps of mixed_2048 on the CPU oracle (C/OpenMP restatement of the "
+                         f"reference kernels + the same multigrid to 1e-8), after 1 warm-up substep; "
+                         f"mean {sum(ccyc) / max(len(ccyc), 1):.1f} cycles/step"}
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 state + f64/f32 mixed solve", "data": "synthetic",
+        "config": {"workload": "mixed_2048", "grid": [2048, 2048], "sources": 4, "solver":
+                   "multigrid V(2,2) RBGS w=1.4, full weighting, bilinear, 8x8 exact coarsest; FP32 cycles in FP64 "
+                   "iterative refinement", "tol": TOL, "mean_cycles_per_step": sum(cycles) / len(cycles),
+                   "converged": bool(relres_ok), "l2": "working set > 126 MB L2; no flush",
+                   "parallelism": f"replicas x{world}"},
+        "fp64_gpu": {"value": value64, "ms_per_step": ms64 / args.steps,
+                     "mean_cycles_per_step": sum(cycles64) / len(cycles64), "converged": bool(fp64_ok),
+                     "mixed_speedup": value / value64},
+        "clocks": clocks,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h + 8},
+        "gpu_launches": int(launches),
+        "roofline": {"kernel": "k_gmg_rbgs<float> (level 0 half sweep)", "bound": "hbm", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": None, "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": half_sweep_ms},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    sys.exit(run_reference(args) if args.impl == "reference" else run_ours(args))
+
+
+if __name__ == "__main__":
+    main()

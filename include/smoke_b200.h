@@ -1,0 +1,249 @@
+/*
+ * smoke_b200 -- C ABI of the B200 (sm_100a) smoke-simulation step.
+ *
+ * Every entry point takes plain device pointers, sizes and row strides (in
+ * elements), a dtype code, and a CUDA stream (cudaStream_t passed as void*).
+ * Calls are stream-ordered and asynchronous unless stated otherwise; none
+ * allocates device memory except where "allocates" is written below. Return
+ * value: SG_OK (0) or an SG_ERR_* code; sg_last_error() gives the message of the
+ * calling thread's last failure. No C++ exception crosses this boundary.
+ *
+ * Arrays are row-major [row j = y][column i = x]. For a grid of H rows and W
+ * columns: cell fields are H x W, u faces H x (W+1), v faces (H+1) x W
+ * (reference: src/cfd/common/simulation.py:76-84).
+ *
+ * Masks (uint8, 0/1) are selected by a mask mode:
+ *   SG_MASK_PLANES  explicit planes, as the reference passes them;
+ *   SG_MASK_OPEN    all interior faces open, outer faces closed (what
+ *                   SmokeSimulation2D builds at construction,
+ *                   common/simulation.py:102-113); planes may be NULL;
+ *   SG_MASK_RING    faces of a box whose outermost cells are solid
+ *                   (the solid ring of simulation.py:126-131); planes may be NULL.
+ * The outermost face columns/rows must be closed in SG_MASK_PLANES mode, as every
+ * mask the reference builds is (simulation.py:103-107).
+ *
+ * Reference citations name files of LCEBurton/python-game-engine under src/cfd/.
+ */
+#ifndef SMOKE_B200_H
+#define SMOKE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SG_F32 0
+#define SG_F64 1
+
+#define SG_MASK_PLANES 0
+#define SG_MASK_OPEN 1
+#define SG_MASK_RING 2
+#define SG_MASK_NONE 3 /* enforce_boundary_conditions only: no solid cells */
+
+#define SG_OK 0
+#define SG_ERR_ARG 1          /* null pointer, bad size, stride, mode or parameter */
+#define SG_ERR_DTYPE 2        /* unsupported dtype code */
+#define SG_ERR_CUDA 3         /* a CUDA runtime call failed */
+#define SG_ERR_NOT_CONVERGED 4 /* tolerance not reached within the cycle/iteration cap */
+#define SG_ERR_NONFINITE 5    /* a NaN or Inf was detected in a residual norm */
+#define SG_ERR_WORKSPACE 6    /* workspace missing or too small */
+#define SG_ERR_CAPACITY 7     /* size above a fixed capacity */
+
+const char* sg_version(void);
+/* Message of the calling thread's last failing call ("" if none). */
+const char* sg_last_error(void);
+/* Number of kernel launches this library has issued since it was loaded (all threads). */
+uint64_t sg_launch_count(void);
+
+/* ---------------------------------------------------------------- operators */
+
+/* backends/numba/operators/advection.py:112-128 (advect_scalar_field) and the
+ * dissipation of common/simulation.py:232 fused in: dst = round(sample) * dissipation
+ * in the field's dtype (pass 1.0 for none). u is u_rows x u_cols, v is v_rows x v_cols
+ * (the reference samples them with clamping to their own shapes). is_fluid: H x W. */
+int sg_advect_scalar(int dtype, int64_t H, int64_t W, const void* src, int64_t ld_src, void* dst,
+                     int64_t ld_dst, const void* u, int64_t u_rows, int64_t u_cols, int64_t ld_u,
+                     const void* v, int64_t v_rows, int64_t v_cols, int64_t ld_v, int mask_mode,
+                     const uint8_t* is_fluid, int64_t ld_fluid, double dt, double cell_size,
+                     double dissipation, void* stream);
+
+/* advection.py:130-154 (advect_velocity_u). u is u_rows x u_cols, v is v_rows x v_cols. */
+int sg_advect_velocity_u(int dtype, int64_t u_rows, int64_t u_cols, const void* u_src, int64_t ld_us,
+                         void* u_dst, int64_t ld_ud, const void* v, int64_t v_rows, int64_t v_cols,
+                         int64_t ld_v, int mask_mode, const uint8_t* fmu, int64_t ld_fmu, double dt,
+                         double cell_size, void* stream);
+
+/* advection.py:156-180 (advect_velocity_v). */
+int sg_advect_velocity_v(int dtype, int64_t v_rows, int64_t v_cols, const void* v_src, int64_t ld_vs,
+                         void* v_dst, int64_t ld_vd, const void* u, int64_t u_rows, int64_t u_cols,
+                         int64_t ld_u, int mask_mode, const uint8_t* fmv, int64_t ld_fmv, double dt,
+                         double cell_size, void* stream);
+
+/* Both of the above in one launch on MAC-shaped fields (common/simulation.py:280-286:
+ * both read the old u and v). */
+int sg_advect_velocity(int dtype, int64_t H, int64_t W, const void* u_src, int64_t ld_us, void* u_dst,
+                       int64_t ld_ud, const void* v_src, int64_t ld_vs, void* v_dst, int64_t ld_vd,
+                       int mask_mode, const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv,
+                       int64_t ld_fmv, double dt, double cell_size, void* stream);
+
+/* backends/numba/operators/forces.py:78-105 (apply_forces). v is (H+1) x W; density and
+ * temperature are H x W. temperature may be NULL (treated as ambient everywhere).
+ * f32_temporaries=1 rounds both force terms to float32 as the reference does
+ * (forces.py:33, :62); 0 keeps them in the field's dtype. */
+int sg_apply_forces(int dtype, int64_t H, int64_t W, void* v, int64_t ld_v, const void* density,
+                    int64_t ld_d, const void* temperature, int64_t ld_t, double dt, double gravity,
+                    double buoyancy_coefficient, double density_coefficient, double ambient_temperature,
+                    int f32_temporaries, void* stream);
+
+/* forces.py:108-123 (cool_temperature). */
+int sg_cool_temperature(int dtype, int64_t H, int64_t W, void* temperature, int64_t ld_t, double ambient,
+                        double cooling_rate, double dt, void* stream);
+
+/* backends/numba/operators/divergence.py:4-25 (compute_divergence). */
+int sg_compute_divergence(int dtype, int64_t H, int64_t W, const void* u, int64_t ld_u, const void* v,
+                          int64_t ld_v, void* div, int64_t ld_div, int mask_mode, const uint8_t* fmu,
+                          int64_t ld_fmu, const uint8_t* fmv, int64_t ld_fmv, double cell_size,
+                          void* stream);
+
+/* backends/numba/operators/residual.py:6-42 (compute_residual). If sumsq (device, one
+ * double) is non-NULL, the sum over fluid cells of residual^2 (evaluated in double) is
+ * ADDED to it. */
+int sg_compute_residual(int dtype, int64_t H, int64_t W, const void* p, int64_t ld_p, const void* div,
+                        int64_t ld_div, int mask_mode, const uint8_t* is_fluid, int64_t ld_fluid,
+                        const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv, int64_t ld_fmv,
+                        double alpha, double reciprocal_beta, void* out, int64_t ld_out, double* sumsq,
+                        void* stream);
+
+/* backends/numba/operators/pressure_gradient.py:4-37 (apply_pressure_gradient). */
+int sg_apply_pressure_gradient(int dtype, int64_t H, int64_t W, void* u, int64_t ld_u, void* v,
+                               int64_t ld_v, const void* p, int64_t ld_p, int mask_mode, const uint8_t* fmu,
+                               int64_t ld_fmu, const uint8_t* fmv, int64_t ld_fmv, double fluid_density,
+                               double cell_size, double dt, void* stream);
+
+/* backends/numba/operators/boundaries.py:7-39 (enforce_boundary_conditions).
+ * solid_mode: SG_MASK_PLANES (solid plane H x W), SG_MASK_RING, or SG_MASK_NONE. */
+int sg_enforce_boundary_conditions(int dtype, int64_t H, int64_t W, void* u, int64_t ld_u, void* v,
+                                   int64_t ld_v, int solid_mode, const uint8_t* solid, int64_t ld_s,
+                                   void* stream);
+
+/* apply_pressure_gradient followed by enforce_boundary_conditions in one pass over the
+ * faces (common/simulation.py:244-249). */
+int sg_project(int dtype, int64_t H, int64_t W, void* u, int64_t ld_u, void* v, int64_t ld_v,
+               const void* p, int64_t ld_p, int mask_mode, const uint8_t* fmu, int64_t ld_fmu,
+               const uint8_t* fmv, int64_t ld_fmv, int solid_mode, const uint8_t* solid, int64_t ld_s,
+               double fluid_density, double cell_size, double dt, void* stream);
+
+/* common/emitters.py:37-66 (_apply_scalar_field_numba); approach 0 hard_cutoff,
+ * 1 linear, 2 quadratic, 3 gaussian (emitters.py:6-35). */
+int sg_emit_scalar(int dtype, int64_t H, int64_t W, void* field, int64_t ld, double value, double dt,
+                   double pos_x, double pos_y, double radius, int approach, void* stream);
+
+/* Plume sources of the benchmark scenes (no reference counterpart; the reference's
+ * emitters add, these overwrite). sources: device array of n_sources x 6 doubles
+ * (cx, cy, radius, density_value, v_value, noise_amp) in cell units. Cells whose
+ * centre (i+.5, j+.5) is strictly inside get density; v faces at (i+.5, j) get
+ * v_value + noise, u faces at (i, j+.5) get noise; noise is uniform in
+ * [-amp, amp), keyed by (seed, step, component, row, column). */
+int sg_plume_sources(int dtype, int64_t H, int64_t W, void* density, int64_t ld_d, void* u, int64_t ld_u,
+                     void* v, int64_t ld_v, int n_sources, const double* sources, uint64_t seed,
+                     int64_t step, void* stream);
+
+/* common/simulation.py:103-108 / multigrid/masks.py:30-74: face masks and is_fluid
+ * from a solid plane (any output may be NULL). */
+int sg_build_masks(int64_t H, int64_t W, const uint8_t* solid, int64_t ld_s, uint8_t* fmu, int64_t ld_fmu,
+                   uint8_t* fmv, int64_t ld_fmv, uint8_t* is_fluid, int64_t ld_fluid, void* stream);
+
+/* ---------------------------------------------------------------- reference solvers */
+
+/* backends/numba/solvers/jacobi.py:8-52: `iterations` ping-pong sweeps. scratch: device
+ * buffer of H*W elements of dtype (row stride W); the result always ends in p. */
+int sg_jacobi_solve(int dtype, int64_t H, int64_t W, void* p, int64_t ld_p, const void* div,
+                    int64_t ld_div, int mask_mode, const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv,
+                    int64_t ld_fmv, double alpha, double reciprocal_beta, int iterations, void* scratch,
+                    void* stream);
+
+/* backends/numba/solvers/red_black_sor_gauss_seidel.py:8-42: in place, colour 0 = (i+j) even.
+ * omega as given (the caller resolves the reference's auto-omega rule). */
+int sg_rbsor_solve(int dtype, int64_t H, int64_t W, void* p, int64_t ld_p, const void* div, int64_t ld_div,
+                   int mask_mode, const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv, int64_t ld_fmv,
+                   double alpha, double reciprocal_beta, double omega, int iterations, void* stream);
+
+/* backends/numba/solvers/gauss_seidel.py:8-48 (lexicographic order), run as an
+ * anti-diagonal wavefront in one thread block; intended for small grids. */
+int sg_gauss_seidel_solve(int dtype, int64_t H, int64_t W, void* p, int64_t ld_p, const void* div,
+                          int64_t ld_div, int mask_mode, const uint8_t* fmu, int64_t ld_fmu,
+                          const uint8_t* fmv, int64_t ld_fmv, double alpha, double reciprocal_beta,
+                          int iterations, void* stream);
+
+/* multigrid/transfer.py:5-36 (restrict: mean of the fluid children) with the coarse
+ * rhs division of multigrid/solver.py:124-125 fused (coarse = round(mean) / round(divisor)
+ * in dtype; pass 1.0 for none). */
+int sg_mg_restrict_average(int dtype, int64_t H, int64_t W, const void* fine, int64_t ld_f, int mask_mode,
+                           const uint8_t* is_fluid, int64_t ld_fluid, void* coarse, int64_t ld_c,
+                           int64_t Hc, int64_t Wc, double divisor, void* stream);
+
+/* multigrid/transfer.py:38-72 (prolong). accumulate=0 writes fine = P coarse;
+ * accumulate=1 performs the `pressure += correction` of multigrid/solver.py:133-134
+ * (fine = fine + round(P coarse)). */
+int sg_mg_prolong(int dtype, int64_t Hc, int64_t Wc, const void* coarse, int64_t ld_c, int64_t H, int64_t W,
+                  int mask_mode, const uint8_t* is_fluid, int64_t ld_fluid, void* fine, int64_t ld_f,
+                  int accumulate, void* stream);
+
+/* multigrid/masks.py:3-27 (any solid child makes the coarse cell solid). */
+int sg_mg_coarsen_solid(int64_t H, int64_t W, const uint8_t* solid, int64_t ld_s, uint8_t* coarse,
+                        int64_t ld_c, void* stream);
+
+/* ---------------------------------------------------------------- convergent multigrid */
+/*
+ * Geometric multigrid for A p = b with A p = sum over open faces (p - p_nb) on fluid
+ * cells and b = alpha * div (so r = b - A p equals residual.py:39-40). No reference
+ * counterpart: the reference V-cycle (multigrid/solver.py) does not converge to
+ * tight tolerances. Any-fluid 2x2 coarsening, red-black Gauss-Seidel smoother with
+ * over-relaxation, full-weighting restriction (transpose of bilinear prolongation),
+ * exact coarsest solve (pseudo-inverse). precision: SG_GMG_FP32, SG_GMG_FP64, or
+ * SG_GMG_MIXED (FP64 fine residual and pressure accumulation, FP32 cycles, FP64
+ * coarsest solve).
+ */
+#define SG_GMG_FP32 0
+#define SG_GMG_FP64 1
+#define SG_GMG_MIXED 2
+
+typedef struct sg_gmg_plan sg_gmg_plan;
+
+/* Host-side planning (allocates host memory only). The masks are HOST arrays
+ * (NULL in SG_MASK_OPEN / SG_MASK_RING modes). cycle: 0 = V, 1 = W. */
+int sg_gmg_plan_create(sg_gmg_plan** plan, int64_t H, int64_t W, int mask_mode, const uint8_t* is_fluid,
+                       const uint8_t* fmu, const uint8_t* fmv, int coarsest, double omega, int pre_sweeps,
+                       int post_sweeps, int cycle, int precision);
+void sg_gmg_plan_destroy(sg_gmg_plan* plan);
+int64_t sg_gmg_workspace_bytes(const sg_gmg_plan* plan);
+int sg_gmg_num_levels(const sg_gmg_plan* plan);
+/* Copy the plan's level masks and coarsest operator into a caller-provided device
+ * workspace of sg_gmg_workspace_bytes() bytes (256-byte aligned). */
+int sg_gmg_bind(sg_gmg_plan* plan, void* workspace, void* stream);
+/* Solve in place from the current p (p is float32 for SG_GMG_FP32, float64 otherwise;
+ * div is float32 or float64 as div_dtype says). Runs cycles until ||b - A p|| / ||b|| <= tol
+ * (checked on the host every check_every cycles) or max_cycles. Outputs (host): cycles
+ * run and the last relative residual. Returns SG_ERR_NOT_CONVERGED if tol was not
+ * reached. Synchronises stream. */
+int sg_gmg_solve(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div, int div_dtype,
+                 double alpha, double tol, int max_cycles, int check_every, int* cycles_out,
+                 double* relres_out, void* stream);
+/* Stream-ordered variant without host synchronisation: runs exactly n_cycles cycles and
+ * writes the relative residual after each cycle into relres_dev[0..n_cycles] (device;
+ * relres_dev[0] is the initial value). Capturable in a CUDA graph. */
+int sg_gmg_cycles_async(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div,
+                        int div_dtype, double alpha, int n_cycles, double* relres_dev, void* stream);
+
+/* Shape of one level of the hierarchy (level 0 is the fine grid). */
+int sg_gmg_level_shape(const sg_gmg_plan* plan, int level, int* H, int* W);
+/* Run `sweeps` smoother sweeps on one level's workspace buffers (whatever they hold);
+ * a building block exposed for timing the smoother in isolation. */
+int sg_gmg_smooth_async(sg_gmg_plan* plan, int level, int sweeps, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SMOKE_B200_H */

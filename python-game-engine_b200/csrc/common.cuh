@@ -1,0 +1,179 @@
+// Shared device/host helpers for the smoke_b200 CUDA library (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "smoke_b200.h"
+
+namespace sg {
+
+// ------------------------------------------------------------------ errors
+void set_error(const char* fmt, ...);
+int fail(int code, const char* fmt, ...);
+int check_launch(const char* what);
+// Count of kernel launches issued by this library (read with sg_launch_count()).
+void note_launch();
+
+// Launch a kernel and count it: SG_LAUNCH(k<T><<<grid, block, smem, stream>>>(args));
+#define SG_LAUNCH(...)   \
+  do {                   \
+    __VA_ARGS__;         \
+    ::sg::note_launch(); \
+  } while (0)
+
+#define SG_REQUIRE(cond, ...)                        \
+  do {                                               \
+    if (!(cond)) return ::sg::fail(SG_ERR_ARG, __VA_ARGS__); \
+  } while (0)
+
+#define SG_DISPATCH(dtype, ...)                                     \
+  do {                                                              \
+    if ((dtype) == SG_F32) {                                        \
+      using T = float;                                              \
+      __VA_ARGS__                                                   \
+    } else if ((dtype) == SG_F64) {                                 \
+      using T = double;                                             \
+      __VA_ARGS__                                                   \
+    } else {                                                        \
+      return ::sg::fail(SG_ERR_DTYPE, "unsupported dtype code %d", (int)(dtype)); \
+    }                                                               \
+  } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ------------------------------------------------------------------ launch shapes
+constexpr int kBX = 32;
+constexpr int kBY = 8;
+inline dim3 grid2d(int64_t cols, int64_t rows) {
+  return dim3((unsigned)((cols + kBX - 1) / kBX), (unsigned)((rows + kBY - 1) / kBY));
+}
+inline dim3 block2d() { return dim3(kBX, kBY); }
+
+// ------------------------------------------------------------------ masks
+// Face/fluid masks of an H x W cell grid, either explicit planes (as the reference
+// passes them) or analytic: SG_MASK_OPEN (all interior faces open) or SG_MASK_RING
+// (a box whose outermost cells are solid).
+struct Masks {
+  const uint8_t* fmu;
+  int64_t ldu;
+  const uint8_t* fmv;
+  int64_t ldv;
+  const uint8_t* fl;
+  int64_t ldf;
+  int mode;
+  int H, W;
+
+  __device__ __forceinline__ bool u(int j, int i) const {
+    if (mode == SG_MASK_PLANES) return fmu[(int64_t)j * ldu + i] != 0;
+    if (mode == SG_MASK_OPEN) return i >= 1 && i <= W - 1;
+    return j >= 1 && j <= H - 2 && i >= 2 && i <= W - 2;
+  }
+  __device__ __forceinline__ bool v(int j, int i) const {
+    if (mode == SG_MASK_PLANES) return fmv[(int64_t)j * ldv + i] != 0;
+    if (mode == SG_MASK_OPEN) return j >= 1 && j <= H - 1;
+    return i >= 1 && i <= W - 2 && j >= 2 && j <= H - 2;
+  }
+  // common/simulation.py:108: a cell is fluid when any of its four faces is open.
+  __device__ __forceinline__ bool fluid(int j, int i) const {
+    if (mode == SG_MASK_PLANES && fl) return fl[(int64_t)j * ldf + i] != 0;
+    return u(j, i) || u(j, i + 1) || v(j, i) || v(j + 1, i);
+  }
+};
+
+inline Masks make_masks(int mode, int64_t H, int64_t W, const uint8_t* fmu, int64_t ldu, const uint8_t* fmv,
+                        int64_t ldv, const uint8_t* fl, int64_t ldf) {
+  Masks m;
+  m.fmu = fmu;
+  m.ldu = ldu;
+  m.fmv = fmv;
+  m.ldv = ldv;
+  m.fl = fl;
+  m.ldf = ldf;
+  m.mode = mode;
+  m.H = (int)H;
+  m.W = (int)W;
+  return m;
+}
+
+// ------------------------------------------------------------------ reference arithmetic
+// advection.py:6-49. For float fields Numba evaluates (b - a) in float32 and the rest in
+// float64 (every expression meets a Python float); the same order is kept here so a
+// float32 result is rounded once from the same double value.
+__device__ __forceinline__ int64_t clampi(int64_t v, int64_t lo, int64_t hi) {
+  return v < lo ? lo : (v > hi ? hi : v);
+}
+
+template <typename T>
+__device__ __forceinline__ double lerp_ref(T a, T b, double t) {
+  T d = b - a;
+  return (double)a + (double)d * t;
+}
+
+template <typename T>
+__device__ __forceinline__ double sample_ref(const T* __restrict__ f, int64_t ld, int64_t rows, int64_t cols,
+                                             double x, double y) {
+  int64_t x0 = (int64_t)floor(x), x1 = (int64_t)ceil(x);
+  int64_t y0 = (int64_t)floor(y), y1 = (int64_t)ceil(y);
+  x0 = clampi(x0, 0, cols - 1);
+  x1 = clampi(x1, 0, cols - 1);
+  y0 = clampi(y0, 0, rows - 1);
+  y1 = clampi(y1, 0, rows - 1);
+  double tx = x - (double)x0;
+  double ty = y - (double)y0;
+  T c00 = f[y0 * ld + x0], c10 = f[y0 * ld + x1];
+  T c01 = f[y1 * ld + x0], c11 = f[y1 * ld + x1];
+  double c0 = lerp_ref(c00, c10, tx);
+  double c1 = lerp_ref(c01, c11, tx);
+  return c0 + (c1 - c0) * ty;
+}
+
+// SplitMix64 finaliser (Steele, Lea, Flood 2014); the plume noise hash.
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+__host__ __device__ __forceinline__ double noise(uint64_t seed, int64_t step, int comp, int64_t j, int64_t i,
+                                                 double amp) {
+  uint64_t h = mix64(seed ^ mix64((uint64_t)step));
+  h = mix64(h ^ (((uint64_t)comp << 62) | ((uint64_t)j << 31) | (uint64_t)i));
+  double u = (double)(h >> 11) * (1.0 / 9007199254740992.0);
+  return amp * (2.0 * u - 1.0);
+}
+
+// ------------------------------------------------------------------ reductions
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sum of one value per thread over the block; the result is valid in thread 0.
+template <typename T>
+__device__ __forceinline__ T block_sum(T v) {
+  __shared__ T partial[32];
+  int lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31;
+  int warp = (threadIdx.x + threadIdx.y * blockDim.x) >> 5;
+  int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+  v = warp_sum(v);
+  if (lane == 0) partial[warp] = v;
+  __syncthreads();
+  T s = 0;
+  if (warp == 0) {
+    s = lane < nwarps ? partial[lane] : (T)0;
+    s = warp_sum(s);
+  }
+  __syncthreads();
+  return s;
+}
+
+}  // namespace sg

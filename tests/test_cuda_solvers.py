@@ -1,0 +1,178 @@
+"""CUDA solvers and multi-step scenes against the CPU oracle.
+
+* plume_128 (128^2, Jacobi x100, float64): 200 CUDA steps vs 200 oracle steps; the
+  stated tolerance is 1e-12 absolute on density (the operators are bit-exact).
+* Convergent multigrid (no reference counterpart; oracle = the project's FP64 C
+  restatement, GMGOracle): one cycle within 1e-10 relative of the oracle's cycle,
+  the tolerance targets float64 1e-10, mixed 1e-8, float32 1e-5, and the converged
+  pressure (mean removed) within 1e-6 / 1e-4 / 5e-2 relative of the oracle's.
+* Failure detection without faulting the GPU: non-finite input and an unreachable
+  tolerance come back as host exceptions.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import package
+
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():
+    pytest.skip("CUDA device required", allow_module_level=True)
+
+import oracle as O  # noqa: E402
+from cuda_adapter import dev  # noqa: E402
+
+sg = package()
+scenes = sg.scenes
+
+
+def _oracle_sim(scene, solver, kw, dtype):
+    s = O.OracleSim(scene.H, scene.W, scene.cell_size, solver, kw, dtype=dtype)
+    s.dt = scene.dt
+    s.gravity = scene.gravity
+    s.plumes = [O.PlumeSpec(*row, seed=scene.seed) for row in scene.plumes]
+    return s
+
+
+def test_plume_128_200_steps_fp64_vs_oracle():
+    sc = scenes.plume_128(steps=200)
+    cu = scenes.make_sim(sc, "jacobi", sg.JacobiParams(iterations=100), dtype=torch.float64)
+    ora = _oracle_sim(sc, O.jacobi_pressure_solver, dict(iterations=100), np.float64)
+    for _ in range(sc.steps):
+        cu.substep(sc.dt)
+        ora.substep(sc.dt)
+    d_err = np.max(np.abs(cu.density.cpu().numpy() - ora.density))
+    u_err = np.max(np.abs(cu.velocity_u.cpu().numpy() - ora.velocity_u))
+    p_err = np.max(np.abs(cu.pressure.cpu().numpy() - ora.pressure))
+    assert np.max(ora.density) > 0.5
+    assert d_err <= 1e-12 and u_err <= 1e-12 and p_err <= 1e-12, (d_err, u_err, p_err)
+
+
+def test_plume_128_fp32_20_steps_vs_oracle():
+    sc = scenes.plume_128(steps=20)
+    cu = scenes.make_sim(sc, "jacobi", sg.JacobiParams(iterations=100), dtype=torch.float32)
+    ora = _oracle_sim(sc, O.jacobi_pressure_solver, dict(iterations=100), np.float32)
+    for _ in range(sc.steps):
+        cu.substep(sc.dt)
+        ora.substep(sc.dt)
+    assert np.array_equal(cu.density.cpu().numpy(), ora.density)
+    assert np.array_equal(cu.velocity_v.cpu().numpy(), ora.velocity_v)
+
+
+def _problem(H, W, obstacles, seed):
+    rng = np.random.default_rng(seed)
+    solid = np.zeros((H, W), bool)
+    if obstacles:
+        solid = O.box_solid(H, W)
+        solid[H // 3:H // 3 + H // 8, W // 4:W // 2] = True
+    fmu, fmv = O.face_masks_from_solid(solid)
+    fl = O.is_fluid_from_faces(fmu, fmv)
+    div = rng.standard_normal((H, W)) * fl
+    div[fl] -= div[fl].mean()
+    return fmu, fmv, fl, div
+
+
+@pytest.mark.parametrize("shape,obstacles", [((64, 64), False), ((96, 80), True), ((37, 50), True)])
+def test_gmg_one_cycle_vs_oracle(shape, obstacles):
+    H, W = shape
+    fmu, fmv, fl, div = _problem(H, W, obstacles, 1)
+    alpha = -0.7
+    g = O.GMGOracle(fmu, fmv, fl, coarsest=8, omega=1.4)
+    pe = np.zeros((H, W))
+    g.vcycle(0, pe, alpha * div)
+    solver = sg.GeometricMultigridSolver()
+    masks = (sg.OPEN_BOX, sg.OPEN_BOX) if not obstacles else (dev(fmu), dev(fmv))
+    p = torch.zeros((H, W), dtype=torch.float64, device="cuda")
+    # cell_size, rho, dt chosen so that alpha = -(h^2) rho / dt = -0.7
+    solver(p, dev(div), masks[0], masks[1], 0.7, 1.0, 1.0, precision="fp64", fixed_cycles=1)
+    got = p.cpu().numpy()
+    assert np.max(np.abs(got - pe)) <= 1e-10 * np.max(np.abs(pe))
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 1e-8), ("fp32", 1e-5)])
+@pytest.mark.parametrize("obstacles", [False, True])
+def test_gmg_reaches_tolerance(precision, tol, obstacles):
+    H = W = 128
+    fmu, fmv, fl, div = _problem(H, W, obstacles, 2)
+    solver = sg.GeometricMultigridSolver()
+    masks = (sg.OPEN_BOX, sg.OPEN_BOX) if not obstacles else (dev(fmu), dev(fmv))
+    dtype = torch.float32 if precision == "fp32" else torch.float64
+    p = torch.zeros((H, W), dtype=dtype, device="cuda")
+    d = dev(div.astype(np.float32 if precision != "fp64" else np.float64))
+    solver(p, d, masks[0], masks[1], 1.0, 1.0 / H, 0.5 / H, tol=tol, max_cycles=40, precision=precision, strict=True)
+    assert solver.converged and solver.last_relres <= tol and solver.last_cycles <= 20
+    # converged solution vs the oracle's FP64 solve of the same problem (mean removed)
+    alpha = O.alpha_coeff(1.0 / H, 1.0, 0.5 / H)
+    g = O.GMGOracle(fmu, fmv, fl)
+    pe = np.zeros((H, W))
+    g.solve(pe, alpha * d.double().cpu().numpy() * fl, tol=1e-12, max_cycles=60)
+    got = p.double().cpu().numpy()
+    a = got[fl] - got[fl].mean()
+    b = pe[fl] - pe[fl].mean()
+    # two solutions with relative residuals <= tol differ by at most ~ (lambda_max / lambda_min) * tol
+    # relative (about 1.3e4 * tol at 128^2); the bounds below sit well inside that
+    bound = {"fp64": 1e-6, "mixed": 1e-4, "fp32": 5e-2}[precision]
+    assert np.max(np.abs(a - b)) <= bound * np.max(np.abs(b))
+
+
+def test_gmg_fixed_cycles_residual_history():
+    H = W = 256
+    fmu, fmv, fl, div = _problem(H, W, False, 3)
+    solver = sg.GeometricMultigridSolver()
+    p = torch.zeros((H, W), dtype=torch.float64, device="cuda")
+    solver(p, dev(div), sg.OPEN_BOX, sg.OPEN_BOX, 1.0, 1.0 / H, 0.5 / H, precision="mixed", fixed_cycles=8)
+    hist = solver.last_relres_dev.cpu().numpy()
+    assert hist[0] == pytest.approx(1.0)
+    assert np.all(np.diff(hist) < 0) and hist[-1] < 1e-7
+
+
+def test_sor_tolerance_reaches_1e6():
+    H = W = 48
+    fmu, fmv, fl, div = _problem(H, W, False, 4)
+    s = sg.SORToleranceSolver()
+    p = torch.zeros((H, W), dtype=torch.float64, device="cuda")
+    s(p, dev(div), sg.OPEN_BOX, sg.OPEN_BOX, 1.0, 1.0 / H, 0.5 / H, omega=1.9, tol=1e-6, check_every=50, strict=True)
+    assert s.converged and s.last_relres <= 1e-6
+
+
+def test_nonfinite_input_is_reported():
+    H = W = 32
+    div = np.zeros((H, W))
+    div[5, 5] = np.nan
+    p = torch.zeros((H, W), dtype=torch.float64, device="cuda")
+    with pytest.raises(sg.SmokeCudaError):
+        sg.GeometricMultigridSolver()(p, dev(div), sg.OPEN_BOX, sg.OPEN_BOX, 1.0, 1.0, 1.0, precision="fp64")
+    # the context stays usable after the reported failure
+    q = torch.ones(4, device="cuda")
+    assert float(q.sum()) == 4.0
+
+
+def test_unreachable_tolerance_is_reported():
+    H = W = 64
+    fmu, fmv, fl, div = _problem(H, W, False, 5)
+    p = torch.zeros((H, W), dtype=torch.float64, device="cuda")
+    s = sg.GeometricMultigridSolver()
+    with pytest.raises(sg.NotConverged):
+        s(p, dev(div), sg.OPEN_BOX, sg.OPEN_BOX, 1.0, 1.0, 1.0, precision="fp64", tol=1e-30, max_cycles=3, strict=True)
+    assert s.last_cycles == 3
+
+
+def test_bad_arguments_raise_before_launch():
+    t = torch.zeros((8, 8), device="cuda")
+    with pytest.raises(ValueError):
+        sg.operators.compute_divergence(t, t, t, sg.OPEN_BOX, sg.OPEN_BOX, 1.0)  # wrong u/v shapes
+    with pytest.raises(TypeError):
+        sg.operators.cool_temperature(torch.zeros((4, 4), dtype=torch.int32, device="cuda"), 0.0, 0.5, 0.1)
+
+
+def test_gmg_step_sim_mixed_2048_short():
+    """Two steps of the 2048^2 scene: mixed precision reaches 1e-8 each step."""
+    sc = scenes.mixed_2048(steps=2)
+    params = sg.GeometricMultigridParams(tol=1e-8, precision="mixed", max_cycles=30)
+    sim = scenes.make_sim(sc, "geometric_multigrid", params, dtype=torch.float32)
+    solver = sg.get_solver("geometric_multigrid", "cuda")
+    for _ in range(2):
+        sim.substep(sc.dt)
+        assert solver.converged and solver.last_relres <= 1e-8
+    assert float(sim.density.max()) > 0.5

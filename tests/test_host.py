@@ -1,0 +1,182 @@
+"""Host-side checks that need no GPU: the C ABI library, argument validation,
+multigrid planning, registries, params and config (reference: src/cfd/solvers/
+registry.py, operators/registry.py, solvers/params.py, common/config.py)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, package
+
+sg = package()
+L = sg._lib
+
+
+def _declared():
+    with open(os.path.join(ROOT, "include", "smoke_b200.h")) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"\b(sg_\w+)\s*\(", text)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = L.load()
+    names = _declared()
+    assert len(names) >= 30
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(L.SIGNATURES), set(names) ^ set(L.SIGNATURES)
+    assert lib.sg_version().startswith(b"smoke_b200")
+    assert isinstance(lib.sg_launch_count(), int)
+
+
+def test_abi_rejects_bad_arguments_without_a_gpu():
+    lib = L.load()
+    null = None
+    # empty grid
+    rc = lib.sg_compute_divergence(L.SG_F32, 0, 4, null, 5, null, 4, null, 4, L.SG_MASK_OPEN, null, 0, null, 0, 1.0,
+                                   null)
+    assert rc == L.SG_ERR_ARG and b"grid" in lib.sg_last_error()
+    # null field pointers
+    rc = lib.sg_advect_scalar(L.SG_F32, 4, 4, null, 4, null, 4, null, 4, 5, 5, null, 5, 4, 4, L.SG_MASK_OPEN, null, 0,
+                              0.1, 1.0, 1.0, null)
+    assert rc == L.SG_ERR_ARG
+    # mask planes required in planes mode
+    fake = ctypes.c_void_p(16)
+    rc = lib.sg_compute_divergence(L.SG_F32, 4, 4, fake, 5, fake, 4, fake, 4, L.SG_MASK_PLANES, null, 0, null, 0, 1.0,
+                                   null)
+    assert rc == L.SG_ERR_ARG
+    # row stride below the row length
+    rc = lib.sg_cool_temperature(L.SG_F32, 4, 4, fake, 3, 0.0, 0.5, 0.1, null)
+    assert rc == L.SG_ERR_ARG
+    # unsupported dtype code
+    rc = lib.sg_cool_temperature(7, 4, 4, fake, 4, 0.0, 0.5, 0.1, null)
+    assert rc == L.SG_ERR_DTYPE
+    # bad cell size
+    rc = lib.sg_compute_divergence(L.SG_F64, 4, 4, fake, 5, fake, 4, fake, 4, L.SG_MASK_OPEN, null, 0, null, 0, 0.0,
+                                   null)
+    assert rc == L.SG_ERR_ARG
+    # the Python layer turns codes into exceptions
+    with pytest.raises(ValueError):
+        L.check(L.SG_ERR_ARG, "x")
+    with pytest.raises(L.NotConverged):
+        L.check(L.SG_ERR_NOT_CONVERGED, "x")
+    with pytest.raises(L.SmokeCudaError):
+        L.check(L.SG_ERR_NONFINITE, "x")
+
+
+def _plan(H, W, mode=L.SG_MASK_OPEN, masks=None, **kw):
+    lib = L.load()
+    h = ctypes.c_void_p()
+    args = dict(coarsest=8, omega=1.4, pre=2, post=2, cycle=0, precision=L.SG_GMG_MIXED)
+    args.update(kw)
+    ptrs = [None, None, None] if masks is None else [m.ctypes.data_as(ctypes.c_void_p) for m in masks]
+    rc = lib.sg_gmg_plan_create(ctypes.byref(h), H, W, mode, *ptrs, args["coarsest"], args["omega"], args["pre"],
+                                args["post"], args["cycle"], args["precision"])
+    return rc, h
+
+
+@pytest.mark.parametrize("H,W,levels", [(2048, 2048, 9), (512, 512, 7), (128, 128, 5), (96, 96, 5), (37, 50, 4),
+                                        (8, 8, 1), (2048, 1024, 9)])
+def test_gmg_plan_hierarchy(H, W, levels):
+    lib = L.load()
+    rc, h = _plan(H, W)
+    assert rc == L.SG_OK
+    try:
+        assert lib.sg_gmg_num_levels(h) == levels
+        hh, ww = ctypes.c_int(), ctypes.c_int()
+        assert lib.sg_gmg_level_shape(h, levels - 1, ctypes.byref(hh), ctypes.byref(ww)) == L.SG_OK
+        assert max(hh.value, ww.value) <= 8
+        assert lib.sg_gmg_workspace_bytes(h) > 0
+    finally:
+        lib.sg_gmg_plan_destroy(h)
+
+
+def test_gmg_plan_with_obstacle_planes():
+    import oracle as O
+
+    H, W = 64, 48
+    solid = O.box_solid(H, W)
+    solid[20:30, 10:20] = True
+    fmu, fmv = O.face_masks_from_solid(solid)
+    fl = O.is_fluid_from_faces(fmu, fmv)
+    masks = [np.ascontiguousarray(x.astype(np.uint8)) for x in (fl, fmu, fmv)]
+    rc, h = _plan(H, W, L.SG_MASK_PLANES, masks)
+    assert rc == L.SG_OK
+    L.load().sg_gmg_plan_destroy(h)
+
+
+@pytest.mark.parametrize("kw", [dict(omega=2.5), dict(coarsest=0), dict(pre=0, post=0), dict(cycle=3),
+                                dict(precision=9)])
+def test_gmg_plan_rejects_bad_parameters(kw):
+    rc, h = _plan(64, 64, **kw)
+    assert rc == L.SG_ERR_ARG and not h.value
+
+
+def test_registry_semantics():
+    key = ("__test_op__", "cuda")
+    sg.register_operator(*key, lambda: 1)
+    with pytest.raises(ValueError, match="already registered"):
+        sg.register_operator(*key, lambda: 2)
+    assert sg.get_operator(*key)() == 1
+    del sg.OPERATOR_REGISTRY[key]
+    with pytest.raises(ValueError, match="Available"):
+        sg.get_operator("__missing__", "cuda")
+    with pytest.raises(ValueError, match="Unknown pressure solver"):
+        sg.get_solver("jacobi", "numba")
+    names = {k[0] for k in sg.OPERATOR_REGISTRY}
+    assert names >= {"advection_scalar", "advection_velocity_u", "advection_velocity_v", "enforce_boundary_conditions",
+                     "compute_divergence", "apply_forces", "cool_temperature", "apply_pressure_gradient",
+                     "compute_residual"}
+    assert {k[0] for k in sg.SOLVER_REGISTRY} >= {"jacobi", "gauss_seidel", "rb_sor_gauss_seidel", "multigrid"}
+
+
+def test_params_match_reference_defaults():
+    assert sg.JacobiParams().iterations == 40
+    assert sg.GaussSeidelParams().iterations == 40
+    assert sg.SORParams().iterations == 40 and sg.SORParams().omega == 0.0
+    m = sg.MultigridParams()
+    assert (m.smoother_type, m.num_levels, m.v_cycles, m.smoother_iterations, m.coarsest_iterations,
+            m.rebuild_masks) == ("jacobi", 4, 2, 2, 30, False)
+    assert sg.JacobiParams(7).string() == "JacobiParams_iters_7"
+
+
+def test_config_round_trip_and_validation(tmp_path):
+    cfg = sg.SimulationConfig(grid=sg.GridConfig(size=(64, 32), cell_size=0.5),
+                              pressure_solver=sg.PressureSolverConfig(method="geometric_multigrid",
+                                                                      params=sg.GeometricMultigridParams(tol=1e-8)))
+    cfg.validate_config()
+    path = tmp_path / "c.json"
+    cfg.to_json(str(path))
+    back = sg.SimulationConfig.from_json(str(path))
+    assert back.grid.size == (64, 32) and back.pressure_solver.params.tol == 1e-8
+    back.validate_config()
+    bad = sg.SimulationConfig(grid=sg.GridConfig(size=(64, 0), cell_size=0.5))
+    with pytest.raises(ValueError):
+        bad.validate_config()
+    # a reference-shaped JSON (backend "numba") still loads
+    ref_json = {"grid": {"size": [16, 16], "cell_size": 1.0},
+                "pressure_solver": {"method": "jacobi", "backend": "numba", "params": {"iterations": 5}}}
+    c = sg.SimulationConfig.from_dict(ref_json)
+    assert c.pressure_solver.params.iterations == 5
+
+
+def test_scenes_are_seeded_and_sized():
+    a = sg.scenes.mixed_2048()
+    b = sg.scenes.mixed_2048()
+    assert a.plumes == b.plumes and len(a.plumes) == 4
+    assert all(16.0 <= p[2] <= 64.0 and 0.5 <= p[4] <= 1.5 for p in a.plumes)
+    batch = sg.scenes.batch_256(256)
+    assert {s.H for s in batch} <= set(sg.scenes.BATCH_SIZES)
+    assert all(0.5 <= -s.gravity <= 2.0 for s in batch)
+    assert sg.scenes.plume_128().dt == pytest.approx(0.5 / 128)
+
+
+def test_product_path_does_not_import_the_oracle():
+    pkg = os.path.join(ROOT, "python-game-engine_b200")
+    for fn in os.listdir(pkg):
+        if fn.endswith(".py"):
+            with open(os.path.join(pkg, fn)) as f:
+                src = f.read()
+            assert not re.search(r"^\s*(import|from)\s+oracle\b", src, re.M), fn
