@@ -209,7 +209,11 @@ __global__ void k_gmg_finalize(const double* __restrict__ partial, int n, double
   }
   if (threadIdx.x == 0) {
     double v = sqrt(red[0]);
-    if (mode == 1) v = nb[0] > 0.0 ? v / nb[0] : 0.0;
+    if (mode == 1) {
+      double n = nb[0];
+      if (!(n == n) || isinf(n)) v = n + v;  // a non-finite ||b|| makes the ratio non-finite
+      else v = n > 0.0 ? v / n : 0.0;
+    }
     out[0] = v;
   }
 }

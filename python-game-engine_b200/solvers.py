@@ -114,11 +114,11 @@ class MultigridSolver:
         self.levels = []
         self.buffers = []
 
-    def _ensure(self, fmu, fmv, num_levels, dtype, device, rebuild):
-        key = (tuple(fmu.shape), num_levels, dtype)
+    def _ensure(self, H, W, fmu, fmv, num_levels, dtype, device, rebuild):
+        kind = fmu.name if isinstance(fmu, AnalyticMask) else "planes"
+        key = ((H, W + 1), num_levels, dtype, kind)
         if not rebuild and key == self._key:
             return
-        H, W = fmu.shape[0], fmu.shape[1] - 1
         fmu = materialize_mask(fmu, H, W, "u", device)
         fmv = materialize_mask(fmv, H, W, "v", device)
         fl = is_fluid_from_faces(fmu.bool(), fmv.bool())
@@ -166,7 +166,8 @@ class MultigridSolver:
     def __call__(self, pressure, divergence, face_mask_u, face_mask_v, fluid_density, cell_size, dt, v_cycles=2,
                  smoother_type="jacobi", smoother_backend="cuda", num_levels=4, smoother_iterations=2,
                  coarsest_iterations=50, rebuild_masks=False, profiler=None, **_ignored):
-        self._ensure(face_mask_u, face_mask_v, num_levels, pressure.dtype, pressure.device, rebuild_masks)
+        H, W = pressure.shape
+        self._ensure(H, W, face_mask_u, face_mask_v, num_levels, pressure.dtype, pressure.device, rebuild_masks)
         backend = smoother_backend if smoother_backend == "cuda" else "cuda"
         smoother = get_solver(smoother_type, backend)
         fb = self.buffers[0]
