@@ -163,6 +163,26 @@ int sg_jacobi_solve(int dtype, int64_t H, int64_t W, void* p, int64_t ld_p, cons
                     int64_t ld_fmv, double alpha, double reciprocal_beta, int iterations, void* scratch,
                     void* stream);
 
+/* Same solve as sg_jacobi_solve for callers that cannot allocate device memory: a game
+ * loop or real-time host that must not call cudaMalloc during a frame (an allocation can
+ * synchronise the device and stall the frame), or a host that runs under a fixed device
+ * memory budget set at start-up. No counterpart in the reference (its Jacobi allocates a
+ * temporary per call, jacobi.py:45).
+ * The ping-pong buffer is a file-scope __device__ array of SG_JACOBI_NOALLOC_MAX_BYTES
+ * bytes that every GPU loading this library holds until exit, so H * W * sizeof(dtype)
+ * must not exceed it (1024 x 1024 float32, 724 x 724 float64); larger grids return
+ * SG_ERR_CAPACITY. The first call on each device looks the array's address up
+ * (cudaGetSymbolAddress) with that device current; make that first call before any
+ * stream capture. All calls share the one array: calls that overlap on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller. Nothing in
+ * the array needs clearing: the first sweep writes every cell before it is read.
+ * Allocates nothing and calls no allocating routine. */
+#define SG_JACOBI_NOALLOC_MAX_BYTES (4u << 20)
+int sg_jacobi_solve_noalloc(int dtype, int64_t H, int64_t W, void* p, int64_t ld_p, const void* div,
+                            int64_t ld_div, int mask_mode, const uint8_t* fmu, int64_t ld_fmu,
+                            const uint8_t* fmv, int64_t ld_fmv, double alpha, double reciprocal_beta,
+                            int iterations, void* stream);
+
 /* backends/numba/solvers/red_black_sor_gauss_seidel.py:8-42: in place, colour 0 = (i+j) even.
  * omega as given (the caller resolves the reference's auto-omega rule). */
 int sg_rbsor_solve(int dtype, int64_t H, int64_t W, void* p, int64_t ld_p, const void* div, int64_t ld_div,

@@ -44,6 +44,7 @@ SIGNATURES = {
     "sg_plume_sources": [I, I64, I64, P, I64, P, I64, P, I64, I, P, U64, I64, P],
     "sg_build_masks": [I64, I64, P, I64, P, I64, P, I64, P, I64, P],
     "sg_jacobi_solve": [I, I64, I64, P, I64, P, I64, I, P, I64, P, I64, D, D, I, P, P],
+    "sg_jacobi_solve_noalloc": [I, I64, I64, P, I64, P, I64, I, P, I64, P, I64, D, D, I, P],
     "sg_rbsor_solve": [I, I64, I64, P, I64, P, I64, I, P, I64, P, I64, D, D, D, I, P],
     "sg_gauss_seidel_solve": [I, I64, I64, P, I64, P, I64, I, P, I64, P, I64, D, D, I, P],
     "sg_mg_restrict_average": [I, I64, I64, P, I64, I, P, I64, P, I64, I64, I64, D, P],

@@ -7,6 +7,7 @@
 
 #include <atomic>
 #include <cstring>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -477,6 +478,31 @@ static int check_mask_mode(int mode, const void* a, const void* b) {
     if (_rc != SG_OK) return _rc; \
   } while (0)
 
+// Ping-pong buffer of sg_jacobi_solve_noalloc: a fixed array in device memory, so the
+// entry point allocates nothing. Host code cannot use the name as a device address;
+// its address is looked up once per device with that device current.
+static __device__ __align__(256) unsigned char g_jacobi_noalloc_scratch[SG_JACOBI_NOALLOC_MAX_BYTES];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[256];
+
+static int noalloc_scratch_address(void** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(SG_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= 256) return fail(SG_ERR_CAPACITY, "device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_jacobi_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(SG_ERR_CUDA, "cudaGetSymbolAddress(static Jacobi scratch): %s", cudaGetErrorString(e));
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return SG_OK;
+}
+
 extern "C" {
 
 const char* sg_version(void) { return "smoke_b200 1.0 (sm_100a)"; }
@@ -733,6 +759,22 @@ int sg_jacobi_solve(int dtype, int64_t H, int64_t W, void* p, int64_t ld_p, cons
     }
   });
   return SG_OK;
+}
+
+int sg_jacobi_solve_noalloc(int dtype, int64_t H, int64_t W, void* p, int64_t ld_p, const void* div, int64_t ld_div,
+                            int mask_mode, const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv, int64_t ld_fmv,
+                            double alpha, double reciprocal_beta, int iterations, void* stream) {
+  SG_CHECK(check_grid(H, W));
+  int64_t elem = dtype == SG_F32 ? 4 : (dtype == SG_F64 ? 8 : 0);
+  if (elem == 0) return fail(SG_ERR_DTYPE, "unsupported dtype code %d", dtype);
+  if (H * W * elem > (int64_t)SG_JACOBI_NOALLOC_MAX_BYTES)
+    return fail(SG_ERR_CAPACITY, "sg_jacobi_solve_noalloc: %lld x %lld cells of %lld bytes exceed the %u-byte static "
+                "scratch; use sg_jacobi_solve with a caller buffer", (long long)H, (long long)W, (long long)elem,
+                (unsigned)SG_JACOBI_NOALLOC_MAX_BYTES);
+  void* scratch = nullptr;
+  SG_CHECK(noalloc_scratch_address(&scratch));
+  return sg_jacobi_solve(dtype, H, W, p, ld_p, div, ld_div, mask_mode, fmu, ld_fmu, fmv, ld_fmv, alpha,
+                         reciprocal_beta, iterations, scratch, stream);
 }
 
 int sg_rbsor_solve(int dtype, int64_t H, int64_t W, void* p, int64_t ld_p, const void* div, int64_t ld_div,
