@@ -215,8 +215,9 @@ def run_ours(args):
         if sampler:
             sampler.start()
             time.sleep(0.3)
+        plan = solver.current_plan()
+        solves0, cycles0, fails0 = plan.counters()
         l0 = lib.sg_launch_count()
-        cycles = []
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
         start.record(stream)
@@ -224,26 +225,37 @@ def run_ours(args):
             if e2e:
                 dev_table.copy_(host_table, non_blocking=True)
             sim.substep(sc.dt)
-            cycles.append(solver.last_cycles)
             if e2e:
                 host_density.copy_(sim.density, non_blocking=True)
-                host_res.fill_(solver.last_relres)
+                host_res[0] = plan.stats()[1]  # device -> host read of the step's solve residual
         end.record(stream)
         barrier()
         ms = start.elapsed_time(end)
         launches = lib.sg_launch_count() - l0
         clocks = sampler.stop() if sampler else None
+        solves1, cycles1, fails1 = plan.counters()
+        prologue_nodes, body_nodes = plan.graph_nodes()
+        # eager launches counted by the library + kernel nodes run by the solve graphs
+        launches += prologue_nodes * (solves1 - solves0) + body_nodes * (cycles1 - cycles0)
+        info = {"cycles": cycles1 - cycles0, "solves": solves1 - solves0, "failures": fails1 - fails0}
         if e2e:
             sim.set_plume_table(None)
             sim._plume_table = None
-        return ms, cycles, launches, clocks
+        return ms, info, launches, clocks
 
     # ---- mixed precision (headline)
     sim = make(torch.float32, "mixed")
-    ms, cycles, launches, clocks = timed(sim, args.steps, args.warmup, sample_clocks=True)
+    ms, info, launches, clocks = timed(sim, args.steps, args.warmup, sample_clocks=True)
     ms_max = max_over_ranks(ms)
     value = world * cells * args.steps / (ms_max / 1e3)
-    relres_ok = solver.converged
+    relres_ok = info["failures"] == 0 and info["solves"] == args.steps
+    if args.only_mixed:  # profiler runs: the headline timed region only
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "ms_per_step": ms_max / args.steps,
+                              "cycles": info["cycles"], "converged": relres_ok, "gpu_launches": int(launches)}))
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
     # ---- end to end through the public API with host buffers
     ms_e2e, _, _, _ = timed(sim, args.steps, 1, e2e=True)
     ms_e2e = max_over_ranks(ms_e2e)
@@ -251,7 +263,7 @@ def run_ours(args):
     h2d = 6 * 8 * len(sim.plumes)
     d2h = sim.density.numel() * sim.density.element_size()
     # ---- dominant kernel roofline: level-0 smoother of the mixed plan, timed alone with events
-    plan = next(iter(solver._plans.values()))
+    plan = solver.current_plan()
     peak, peak_kind = _peaks()
     H0, W0 = sc.H, sc.W
     n_rep = 20
@@ -274,10 +286,10 @@ def run_ours(args):
     del sim
     torch.cuda.empty_cache()
     sim64 = make(torch.float64, "fp64")
-    ms64, cycles64, _, _ = timed(sim64, args.steps, args.warmup)
+    ms64, info64, _, _ = timed(sim64, args.steps, args.warmup)
     ms64 = max_over_ranks(ms64)
     value64 = world * cells * args.steps / (ms64 / 1e3)
-    fp64_ok = solver.converged
+    fp64_ok = info64["failures"] == 0 and info64["solves"] == args.steps
     del sim64
     # ---- CPU baseline on a bounded sample (rank 0, one GPU only)
     cpu = None
@@ -297,11 +309,11 @@ def run_ours(args):
         "dtype": "f32 state + f64/f32 mixed solve", "data": "synthetic",
         "config": {"workload": "mixed_2048", "grid": [2048, 2048], "sources": 4, "solver":
                    "multigrid V(2,2) RBGS w=1.4, full weighting, bilinear, 8x8 exact coarsest; FP32 cycles in FP64 "
-                   "iterative refinement", "tol": TOL, "mean_cycles_per_step": sum(cycles) / len(cycles),
+                   "iterative refinement", "tol": TOL, "mean_cycles_per_step": info["cycles"] / max(info["solves"], 1),
                    "converged": bool(relres_ok), "l2": "working set > 126 MB L2; no flush",
                    "parallelism": f"replicas x{world}"},
         "fp64_gpu": {"value": value64, "ms_per_step": ms64 / args.steps,
-                     "mean_cycles_per_step": sum(cycles64) / len(cycles64), "converged": bool(fp64_ok),
+                     "mean_cycles_per_step": info64["cycles"] / max(info64["solves"], 1), "converged": bool(fp64_ok),
                      "mixed_speedup": value / value64},
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h + 8},
@@ -323,6 +335,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only-mixed", action="store_true", help="time the mixed-precision step only (profiling)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -240,21 +240,38 @@ void sg_gmg_plan_destroy(sg_gmg_plan* plan);
 int64_t sg_gmg_workspace_bytes(const sg_gmg_plan* plan);
 int sg_gmg_num_levels(const sg_gmg_plan* plan);
 /* Copy the plan's level masks and coarsest operator into a caller-provided device
- * workspace of sg_gmg_workspace_bytes() bytes (256-byte aligned). */
+ * workspace of sg_gmg_workspace_bytes() bytes (256-byte aligned) and reset the solve
+ * statistics. Synchronises stream. */
 int sg_gmg_bind(sg_gmg_plan* plan, void* workspace, void* stream);
 /* Solve in place from the current p (p is float32 for SG_GMG_FP32, float64 otherwise;
- * div is float32 or float64 as div_dtype says). Runs cycles until ||b - A p|| / ||b|| <= tol
- * (checked on the host every check_every cycles) or max_cycles. Outputs (host): cycles
- * run and the last relative residual. Returns SG_ERR_NOT_CONVERGED if tol was not
- * reached. Synchronises stream. */
+ * div is float32 or float64 as div_dtype says) until ||b - A p|| / ||b|| <= tol or
+ * max_cycles (< 128) cycles, without host synchronisation: the first call for a given
+ * (p, div) pair captures the solve into a CUDA graph (instantiated once, kept by the
+ * plan) whose cycles run inside a conditional WHILE node; the convergence test runs on
+ * the device after every cycle. Read the outcome with sg_gmg_stats. */
+int sg_gmg_solve_async(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div, int div_dtype,
+                       double alpha, double tol, int max_cycles, void* stream);
+/* Outcome of the last solve (synchronises stream): cycles run, last relative residual,
+ * status (1 converged, 2 cycle cap reached, 3 non-finite residual) and the number of
+ * cycles run by all solves since sg_gmg_bind. Any output may be NULL. */
+int sg_gmg_stats(sg_gmg_plan* plan, int* cycles, double* relres, int* status, long long* total_cycles,
+                 void* stream);
+/* Counters since sg_gmg_bind (synchronises stream): solves started, cycles run, and
+ * solves that ended without reaching tol (cycle cap or non-finite residual). */
+int sg_gmg_counters(sg_gmg_plan* plan, long long* solves, long long* cycles, long long* failures, void* stream);
+/* sg_gmg_solve_async followed by sg_gmg_stats; returns SG_ERR_NOT_CONVERGED when tol was
+ * not reached and SG_ERR_NONFINITE for a NaN/Inf residual. Synchronises stream. */
 int sg_gmg_solve(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div, int div_dtype,
-                 double alpha, double tol, int max_cycles, int check_every, int* cycles_out,
-                 double* relres_out, void* stream);
-/* Stream-ordered variant without host synchronisation: runs exactly n_cycles cycles and
- * writes the relative residual after each cycle into relres_dev[0..n_cycles] (device;
- * relres_dev[0] is the initial value). Capturable in a CUDA graph. */
+                 double alpha, double tol, int max_cycles, int* cycles_out, double* relres_out, void* stream);
+/* Exactly n_cycles cycles (< 128) launched kernel by kernel, no host synchronisation and
+ * no graph (capturable by the caller); writes the relative residual before the first and
+ * after each cycle into relres_dev[0..n_cycles] (device). */
 int sg_gmg_cycles_async(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div,
                         int div_dtype, double alpha, int n_cycles, double* relres_dev, void* stream);
+/* Kernel nodes of the cached solve graph: before the WHILE node and per cycle. */
+int sg_gmg_graph_nodes(const sg_gmg_plan* plan, int* prologue_nodes, int* body_nodes);
+/* First level run by the single-block kernel (all coarser levels run inside it). */
+int sg_gmg_tail_start(const sg_gmg_plan* plan);
 
 /* Shape of one level of the hierarchy (level 0 is the fine grid). */
 int sg_gmg_level_shape(const sg_gmg_plan* plan, int level, int* H, int* W);

@@ -55,8 +55,14 @@ SIGNATURES = {
     "sg_gmg_workspace_bytes": [P],
     "sg_gmg_num_levels": [P],
     "sg_gmg_bind": [P, P, P],
-    "sg_gmg_solve": [P, P, I64, P, I64, I, D, D, I, I, PI, PD, P],
+    "sg_gmg_solve_async": [P, P, I64, P, I64, I, D, D, I, P],
+    "sg_gmg_stats": [P, PI, PD, PI, ctypes.POINTER(ctypes.c_longlong), P],
+    "sg_gmg_counters": [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                        ctypes.POINTER(ctypes.c_longlong), P],
+    "sg_gmg_solve": [P, P, I64, P, I64, I, D, D, I, PI, PD, P],
     "sg_gmg_cycles_async": [P, P, I64, P, I64, I, D, I, PD, P],
+    "sg_gmg_graph_nodes": [P, PI, PI],
+    "sg_gmg_tail_start": [P],
     "sg_gmg_level_shape": [P, I, PI, PI],
     "sg_gmg_smooth_async": [P, I, I, P],
     "sg_version": [],

@@ -19,6 +19,7 @@ int fail(int code, const char* fmt, ...);
 int check_launch(const char* what);
 // Count of kernel launches issued by this library (read with sg_launch_count()).
 void note_launch();
+unsigned long long launch_count();
 
 // Launch a kernel and count it: SG_LAUNCH(k<T><<<grid, block, smem, stream>>>(args));
 #define SG_LAUNCH(...)   \

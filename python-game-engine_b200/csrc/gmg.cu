@@ -11,6 +11,14 @@
 // Coarsest level: exact solve with the pseudo-inverse of its operator (host-built).
 // Outer loop: residual-correction form r = b - A p (precision of p), e = cycle(r) in the
 // cycle precision, p += e; SG_GMG_MIXED runs FP32 cycles inside FP64 refinement.
+//
+// Execution: levels up to 1024 x 1024 cells in total shared-memory footprint run as one
+// thread block (the "tail": every level <= 128^2 in FP32, <= 64^2 in FP64, down to the
+// exact coarsest solve) so the launch-latency-bound coarse levels cost one launch per
+// visit. Larger levels use grid-wide kernels (zero-initial-guess first sweep and the
+// residual fused into the restriction). The tolerance loop is one CUDA graph whose
+// cycles sit in a conditional WHILE node; the convergence test runs on the device, so
+// a solve needs no host synchronisation.
 
 #include <algorithm>
 #include <cstring>
@@ -24,12 +32,11 @@ namespace sg {
 enum : uint8_t { C_FLUID = 1, C_L = 2, C_R = 4, C_D = 8, C_U = 16 };
 
 struct LevelMask {
-  const uint8_t* code;  // planes mode only
-  int64_t ld;
-  int analytic;  // 1: all cells fluid and every interior face open
+  const uint8_t* code;  // H x W codes, row stride W (planes mode only)
+  int analytic;         // 1: all cells fluid and every interior face open
   int H, W;
   __device__ __forceinline__ uint8_t get(int j, int i) const {
-    if (!analytic) return code[(int64_t)j * ld + i];
+    if (!analytic) return code[(int64_t)j * W + i];
     uint8_t c = C_FLUID;
     if (i > 0) c |= C_L;
     if (i < W - 1) c |= C_R;
@@ -37,59 +44,63 @@ struct LevelMask {
     if (j < H - 1) c |= C_U;
     return c;
   }
-  __device__ __forceinline__ bool fluid(int j, int i) const { return analytic ? true : (code[(int64_t)j * ld + i] & C_FLUID); }
+  __device__ __forceinline__ bool fluid(int j, int i) const {
+    return analytic ? true : (code[(int64_t)j * W + i] & C_FLUID) != 0;
+  }
 };
 
-// ---------------------------------------------------------------- kernels
-// Red-black Gauss-Seidel half sweep with the exact diagonal and over-relaxation.
+constexpr int kHist = 128;  // relative residuals kept per solve (history[0] = initial)
+
+// Solve state in device memory (written by the graph, read by the host on demand).
+struct GmgState {
+  double bnorm;
+  double relres;
+  double tol;
+  double alpha;
+  int cycles;
+  int max_cycles;
+  int status;  // 0 running, 1 converged, 2 cycle cap reached, 3 non-finite residual
+  int pad;
+  long long total_cycles;  // cycles run since the plan was bound (all solves)
+  long long solves;
+  long long failures;      // solves that ended at the cycle cap or on a non-finite residual
+  double history[kHist];
+};
+
+// ---------------------------------------------------------------- point operations
+// Residual b - A e at (j, i) of a level (0 on non-fluid cells).
 template <typename T>
-__global__ void k_gmg_rbgs(int H, int W, T* __restrict__ e, int64_t ld, const T* __restrict__ b, LevelMask m, T omega,
-                           int color) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  int i = 2 * k + ((j + color) & 1);
-  if (i >= W || j >= H) return;
+__device__ __forceinline__ T residual_at(int j, int i, const T* e, int64_t lde, const T* b, int64_t ldb,
+                                         const LevelMask& m) {
+  uint8_t c = m.get(j, i);
+  if (!(c & C_FLUID)) return (T)0;
+  int64_t o = (int64_t)j * lde + i;
+  T x = e[o];
+  T acc = b[(int64_t)j * ldb + i];
+  if (c & C_L) acc += e[o - 1] - x;
+  if (c & C_R) acc += e[o + 1] - x;
+  if (c & C_D) acc += e[o - lde] - x;
+  if (c & C_U) acc += e[o + lde] - x;
+  return acc;
+}
+
+// One Gauss-Seidel update with over-relaxation at (j, i) (no-op on non-fluid / isolated cells).
+template <typename T>
+__device__ __forceinline__ void relax_at(int j, int i, T* e, int64_t lde, const T* b, int64_t ldb, const LevelMask& m,
+                                         T omega) {
   uint8_t c = m.get(j, i);
   if (!(c & C_FLUID)) return;
-  int64_t o = (int64_t)j * ld + i;
-  T acc = b[o];
+  int64_t o = (int64_t)j * lde + i;
+  T acc = b[(int64_t)j * ldb + i];
   int n = 0;
   if (c & C_L) { acc += e[o - 1]; ++n; }
   if (c & C_R) { acc += e[o + 1]; ++n; }
-  if (c & C_D) { acc += e[o - ld]; ++n; }
-  if (c & C_U) { acc += e[o + ld]; ++n; }
+  if (c & C_D) { acc += e[o - lde]; ++n; }
+  if (c & C_U) { acc += e[o + lde]; ++n; }
   if (n == 0) return;
   T x = e[o];
   T gs = acc / (T)n;
   e[o] = x + omega * (gs - x);
-}
-
-// r = b - A e on fluid cells (0 elsewhere), written in TO; per-block sums of r^2 (double).
-template <typename T, typename TO>
-__global__ void k_gmg_residual(int H, int W, const T* __restrict__ e, int64_t lde, const T* __restrict__ b,
-                               int64_t ldb, LevelMask m, TO* __restrict__ r, int64_t ldr, double* __restrict__ partial) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  double sq = 0.0;
-  if (i < W && j < H) {
-    uint8_t c = m.get(j, i);
-    T acc = (T)0;
-    if (c & C_FLUID) {
-      int64_t o = (int64_t)j * lde + i;
-      T x = e[o];
-      acc = b[(int64_t)j * ldb + i];
-      if (c & C_L) acc += e[o - 1] - x;
-      if (c & C_R) acc += e[o + 1] - x;
-      if (c & C_D) acc += e[o - lde] - x;
-      if (c & C_U) acc += e[o + lde] - x;
-      sq = (double)acc * (double)acc;
-    }
-    if (r) r[(int64_t)j * ldr + i] = (TO)acc;
-  }
-  if (partial) {
-    double s = block_sum(sq);
-    if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
-  }
 }
 
 // Coarse candidates of fine cell (j, i) for bilinear prolongation (weights 9,3,3,1 / 16).
@@ -107,76 +118,140 @@ __device__ __forceinline__ void pcand(int j, int i, int Hc, int Wc, const LevelM
     if (!cm.fluid(cj[q], ci[q])) { cj[q] = J; ci[q] = I; }
 }
 
-// bc = P^T r.
+// 1-D prolongation weight of fine index i onto coarse index I (grid of n coarse cells).
+__device__ __forceinline__ float w1(int i, int I, int n) {
+  int h = i >> 1;
+  int x = h + ((i & 1) ? 1 : -1);
+  x = x < 0 ? 0 : (x > n - 1 ? n - 1 : x);
+  return (h == I ? 0.75f : 0.0f) + (x == I ? 0.25f : 0.0f);
+}
+
+// (P^T r)(J, I) with r evaluated on the fly from e and b of the fine level.
 template <typename T>
-__global__ void k_gmg_restrict(int H, int W, const T* __restrict__ r, int64_t ldr, LevelMask fm, int Hc, int Wc,
-                               T* __restrict__ bc, int64_t ldc, LevelMask cm) {
-  int I = blockIdx.x * blockDim.x + threadIdx.x;
-  int J = blockIdx.y * blockDim.y + threadIdx.y;
-  if (I >= Wc || J >= Hc) return;
-  const T w[4] = {(T)(9.0 / 16.0), (T)(3.0 / 16.0), (T)(3.0 / 16.0), (T)(1.0 / 16.0)};
+__device__ __forceinline__ T restrict_at(int J, int I, const T* e, int64_t lde, const T* b, int64_t ldb,
+                                         const LevelMask& fm, const LevelMask& cm) {
+  int H = fm.H, W = fm.W, Hc = cm.H, Wc = cm.W;
   T acc = (T)0;
-  if (cm.fluid(J, I)) {
-    for (int j = 2 * J - 2; j <= 2 * J + 3; ++j) {
-      if (j < 0 || j >= H) continue;
-      for (int i = 2 * I - 2; i <= 2 * I + 3; ++i) {
-        if (i < 0 || i >= W || !fm.fluid(j, i)) continue;
-        int cj[4], ci[4];
-        pcand(j, i, Hc, Wc, cm, cj, ci);
-        T rv = r[(int64_t)j * ldr + i];
+  if (fm.analytic && cm.analytic) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-          if (cj[q] == J && ci[q] == I) acc += w[q] * rv;
+    for (int dj = 0; dj < 4; ++dj) {
+      int j = 2 * J - 1 + dj;
+      if (j < 0 || j >= H) continue;
+      T wy = (T)w1(j, J, Hc);
+#pragma unroll
+      for (int di = 0; di < 4; ++di) {
+        int i = 2 * I - 1 + di;
+        if (i < 0 || i >= W) continue;
+        T w = wy * (T)w1(i, I, Wc);
+        if (w != (T)0) acc += w * residual_at(j, i, e, lde, b, ldb, fm);
       }
     }
+    return acc;
   }
-  bc[(int64_t)J * ldc + I] = acc;
+  if (!cm.fluid(J, I)) return (T)0;
+  const T wq[4] = {(T)(9.0 / 16.0), (T)(3.0 / 16.0), (T)(3.0 / 16.0), (T)(1.0 / 16.0)};
+  for (int j = 2 * J - 2; j <= 2 * J + 3; ++j) {
+    if (j < 0 || j >= H) continue;
+    for (int i = 2 * I - 2; i <= 2 * I + 3; ++i) {
+      if (i < 0 || i >= W || !fm.fluid(j, i)) continue;
+      int cj[4], ci[4];
+      pcand(j, i, Hc, Wc, cm, cj, ci);
+      T w = (T)0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (cj[q] == J && ci[q] == I) w += wq[q];
+      if (w != (T)0) acc += w * residual_at(j, i, e, lde, b, ldb, fm);
+    }
+  }
+  return acc;
+}
+
+// (P ec)(j, i) on a fluid fine cell.
+template <typename T>
+__device__ __forceinline__ T prolong_at(int j, int i, const T* ec, int64_t ldc, const LevelMask& cm) {
+  const T wq[4] = {(T)(9.0 / 16.0), (T)(3.0 / 16.0), (T)(3.0 / 16.0), (T)(1.0 / 16.0)};
+  int cj[4], ci[4];
+  pcand(j, i, cm.H, cm.W, cm, cj, ci);
+  T acc = (T)0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) acc += wq[q] * ec[(int64_t)cj[q] * ldc + ci[q]];
+  return acc;
+}
+
+// ---------------------------------------------------------------- grid-wide kernels
+// Red-black half sweep. zero_init (first sweep of a zero initial guess, colour 0 only):
+// each thread owns the cell pair (2k, 2k+1) of its row, writes the relaxed red cell from
+// b alone and zeroes the black one, replacing a separate clearing pass.
+template <typename T>
+__global__ void k_gmg_rbgs(int H, int W, T* __restrict__ e, int64_t ld, const T* __restrict__ b, LevelMask m, T omega,
+                           int color, int zero_init) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (j >= H || 2 * k >= W) return;
+  int i = 2 * k + ((j + color) & 1);
+  if (zero_init) {
+    int i2 = 2 * k + 1 - ((j + color) & 1);
+    if (i2 < W) e[(int64_t)j * ld + i2] = (T)0;
+    if (i < W) {
+      uint8_t c = m.get(j, i);
+      int n = __popc(c & (C_L | C_R | C_D | C_U));
+      T v = (T)0;
+      if ((c & C_FLUID) && n > 0) v = omega * (b[(int64_t)j * ld + i] / (T)n);
+      e[(int64_t)j * ld + i] = v;
+    }
+    return;
+  }
+  if (i < W) relax_at(j, i, e, ld, b, ld, m, omega);
+}
+
+// bc = P^T (b - A e): residual fused into the full-weighting restriction.
+template <typename T>
+__global__ void k_gmg_residual_restrict(const T* __restrict__ e, const T* __restrict__ b, int64_t ld, LevelMask fm,
+                                        T* __restrict__ bc, int64_t ldc, LevelMask cm) {
+  int I = blockIdx.x * blockDim.x + threadIdx.x;
+  int J = blockIdx.y * blockDim.y + threadIdx.y;
+  if (I >= cm.W || J >= cm.H) return;
+  bc[(int64_t)J * ldc + I] = restrict_at(J, I, e, ld, b, ld, fm, cm);
 }
 
 // e += P ec on fluid fine cells.
 template <typename T>
-__global__ void k_gmg_prolong_add(int Hc, int Wc, const T* __restrict__ ec, int64_t ldc, LevelMask cm, int H, int W,
-                                  T* __restrict__ e, int64_t lde, LevelMask fm) {
+__global__ void k_gmg_prolong_add(const T* __restrict__ ec, int64_t ldc, LevelMask cm, T* __restrict__ e, int64_t lde,
+                                  LevelMask fm) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= W || j >= H) return;
-  if (!fm.fluid(j, i)) return;
-  const T w[4] = {(T)(9.0 / 16.0), (T)(3.0 / 16.0), (T)(3.0 / 16.0), (T)(1.0 / 16.0)};
-  int cj[4], ci[4];
-  pcand(j, i, Hc, Wc, cm, cj, ci);
-  T acc = (T)0;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) acc += w[q] * ec[(int64_t)cj[q] * ldc + ci[q]];
-  e[(int64_t)j * lde + i] += acc;
+  if (i >= fm.W || j >= fm.H || !fm.fluid(j, i)) return;
+  e[(int64_t)j * lde + i] += prolong_at(j, i, ec, ldc, cm);
 }
 
-// Exact coarsest solve e = A^+ b (one block; pinv is n x n doubles, n = H * W).
-template <typename T>
-__global__ void k_gmg_coarse_solve(int H, int W, const T* __restrict__ b, int64_t ldb, T* __restrict__ e, int64_t lde,
-                                   const double* __restrict__ pinv) {
-  extern __shared__ double sb[];
-  int n = H * W;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) sb[k] = (double)b[(int64_t)(k / W) * ldb + (k % W)];
-  __syncthreads();
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    const double* row = pinv + (int64_t)k * n;
-    double acc = 0.0;
-    for (int q = 0; q < n; ++q) acc += row[q] * sb[q];
-    e[(int64_t)(k / W) * lde + (k % W)] = (T)acc;
+// Fine residual r = bf - A p in the precision of p, stored as the cycle rhs (TO), with
+// per-block sums of r^2.
+template <typename T, typename TO>
+__global__ void k_gmg_fine_residual(int H, int W, const T* __restrict__ p, int64_t ldp, const T* __restrict__ bf,
+                                    int64_t ldb, LevelMask m, TO* __restrict__ r, int64_t ldr, double* __restrict__ partial) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  double sq = 0.0;
+  if (i < W && j < H) {
+    T acc = residual_at(j, i, p, ldp, bf, ldb, m);
+    sq = (double)acc * (double)acc;
+    r[(int64_t)j * ldr + i] = (TO)acc;
   }
+  double s = block_sum(sq);
+  if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
 }
 
-// b = alpha * div (in the fine precision) plus per-block sums of b^2.
+// bf = alpha * div on fluid cells (alpha from the solve state) plus per-block sums of bf^2.
 template <typename TD, typename TB>
-__global__ void k_gmg_rhs(int H, int W, const TD* __restrict__ div, int64_t ldd, double alpha, LevelMask m,
-                          TB* __restrict__ b, int64_t ldb, double* __restrict__ partial) {
+__global__ void k_gmg_rhs(int H, int W, const TD* __restrict__ div, int64_t ldd, const GmgState* __restrict__ st,
+                          LevelMask m, TB* __restrict__ b, int64_t ldb, double* __restrict__ partial) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
   double sq = 0.0;
   if (i < W && j < H) {
     TB v = (TB)0;
     if (m.fluid(j, i)) {
-      v = (TB)(alpha * (double)div[(int64_t)j * ldd + i]);
+      v = (TB)(st->alpha * (double)div[(int64_t)j * ldd + i]);
       sq = (double)v * (double)v;
     }
     b[(int64_t)j * ldb + i] = v;
@@ -194,10 +269,7 @@ __global__ void k_gmg_correct(int H, int W, TP* __restrict__ p, int64_t ldp, con
   p[(int64_t)j * ldp + i] += (TP)e[(int64_t)j * lde + i];
 }
 
-// Deterministic final sum of block partials; out = sqrt(sum) (mode 0) or
-// out = sqrt(sum) / nb[0] (mode 1, relative to a stored norm); NaN/Inf flags status.
-__global__ void k_gmg_finalize(const double* __restrict__ partial, int n, double* __restrict__ out,
-                               const double* __restrict__ nb, int mode) {
+__device__ __forceinline__ double sum_partials(const double* __restrict__ partial, int n) {
   double s = 0.0;
   for (int k = threadIdx.x; k < n; k += blockDim.x) s += partial[k];
   __shared__ double red[1024];
@@ -207,37 +279,178 @@ __global__ void k_gmg_finalize(const double* __restrict__ partial, int n, double
     if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    double v = sqrt(red[0]);
-    if (mode == 1) {
-      double n = nb[0];
-      if (!(n == n) || isinf(n)) v = n + v;  // a non-finite ||b|| makes the ratio non-finite
-      else v = n > 0.0 ? v / n : 0.0;
-    }
-    out[0] = v;
+  return red[0];
+}
+
+__global__ void k_gmg_set_params(GmgState* st, double alpha, double tol, int max_cycles) {
+  st->alpha = alpha;
+  st->tol = tol;
+  st->max_cycles = max_cycles;
+  st->cycles = 0;
+  st->status = 0;
+  st->solves += 1;
+}
+
+__global__ void k_gmg_finalize_norm(const double* __restrict__ partial, int n, GmgState* st) {
+  double s = sum_partials(partial, n);
+  if (threadIdx.x == 0) st->bnorm = sqrt(s);
+}
+
+// Relative residual after the prologue (body = 0) or a cycle (body = 1); decides whether
+// the WHILE node runs another cycle (when use_handle) and records the status.
+__global__ void k_gmg_finalize_rel(const double* __restrict__ partial, int n, GmgState* st, cudaGraphConditionalHandle h,
+                                   int use_handle, int body) {
+  double s = sum_partials(partial, n);
+  if (threadIdx.x != 0) return;
+  double nb = st->bnorm;
+  double rel = sqrt(s);
+  if (!(nb == nb) || isinf(nb)) rel = nb + rel;  // a non-finite ||b|| makes the ratio non-finite
+  else rel = nb > 0.0 ? rel / nb : 0.0;
+  if (body) {
+    st->cycles += 1;
+    st->total_cycles += 1;
+  }
+  int c = st->cycles;
+  st->relres = rel;
+  if (c < kHist) st->history[c] = rel;
+  bool finite = (rel == rel) && !isinf(rel);
+  int status = !finite ? 3 : (rel <= st->tol ? 1 : (c >= st->max_cycles ? 2 : 0));
+  st->status = status;
+  if (status >= 2) st->failures += 1;
+  if (use_handle) cudaGraphSetConditional(h, status == 0 ? 1u : 0u);
+}
+
+// ---------------------------------------------------------------- single-block tail
+constexpr int kMaxLevels = 16;
+constexpr int kTailThreads = 1024;
+
+template <typename T>
+struct TailArgs {
+  int n;                    // tail levels; the last one is the coarsest (exact solve)
+  LevelMask m[kMaxLevels];  // masks (codes in global memory)
+  int off_e[kMaxLevels];    // shared-memory offsets (elements of T), row stride = W
+  int off_b[kMaxLevels];
+  T* ge;                    // first tail level in global memory (e in/out, b in)
+  const T* gb;
+  int64_t gld;
+  const double* pinv;       // coarsest pseudo-inverse
+  T omega;
+  int pre, post, wcycle, zero_init;
+};
+
+template <typename T>
+__device__ void tail_relax(const LevelMask& m, T* e, const T* b, T omega, int color) {
+  int Wh = (m.W + 1) >> 1;
+  int n = m.H * Wh;
+  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+    int j = idx / Wh;
+    int i = 2 * (idx - j * Wh) + ((j + color) & 1);
+    if (i < m.W) relax_at(j, i, e, (int64_t)m.W, b, (int64_t)m.W, m, omega);
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ void tail_coarse_solve(const LevelMask& m, T* e, const T* b, const double* __restrict__ pinv) {
+  int n = m.H * m.W;
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int row = warp; row < n; row += nw) {
+    double acc = 0.0;
+    for (int q = lane; q < n; q += 32) acc += pinv[(int64_t)row * n + q] * (double)b[q];
+    acc = warp_sum(acc);
+    if (lane == 0) e[row] = (T)acc;
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ __noinline__ void tail_cycle(const TailArgs<T>& a, T* sm, int k) {
+  const LevelMask& m = a.m[k];
+  T* e = sm + a.off_e[k];
+  T* b = sm + a.off_b[k];
+  if (k == a.n - 1) {
+    tail_coarse_solve(m, e, b, a.pinv);
+    return;
+  }
+  for (int s = 0; s < a.pre; ++s) {
+    tail_relax(m, e, b, a.omega, 0);
+    tail_relax(m, e, b, a.omega, 1);
+  }
+  const LevelMask& cm = a.m[k + 1];
+  T* ec = sm + a.off_e[k + 1];
+  T* bc = sm + a.off_b[k + 1];
+  int nc = cm.H * cm.W;
+  for (int idx = threadIdx.x; idx < nc; idx += blockDim.x) {
+    int J = idx / cm.W, I = idx - J * cm.W;
+    bc[idx] = restrict_at(J, I, (const T*)e, (int64_t)m.W, (const T*)b, (int64_t)m.W, m, cm);
+    ec[idx] = (T)0;
+  }
+  __syncthreads();
+  int reps = (a.wcycle && k + 1 < a.n - 1) ? 2 : 1;
+  for (int q = 0; q < reps; ++q) tail_cycle(a, sm, k + 1);
+  int nf = m.H * m.W;
+  for (int idx = threadIdx.x; idx < nf; idx += blockDim.x) {
+    int j = idx / m.W, i = idx - j * m.W;
+    if (m.fluid(j, i)) e[idx] += prolong_at(j, i, (const T*)ec, (int64_t)cm.W, cm);
+  }
+  __syncthreads();
+  for (int s = 0; s < a.post; ++s) {
+    tail_relax(m, e, b, a.omega, 0);
+    tail_relax(m, e, b, a.omega, 1);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTailThreads) k_gmg_tail(const __grid_constant__ TailArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char tail_smem[];
+  T* sm = reinterpret_cast<T*>(tail_smem);
+  const LevelMask& m0 = a.m[0];
+  int n0 = m0.H * m0.W;
+  T* e0 = sm + a.off_e[0];
+  T* b0 = sm + a.off_b[0];
+  for (int idx = threadIdx.x; idx < n0; idx += blockDim.x) {
+    int j = idx / m0.W, i = idx - j * m0.W;
+    b0[idx] = a.gb[(int64_t)j * a.gld + i];
+    e0[idx] = a.zero_init ? (T)0 : a.ge[(int64_t)j * a.gld + i];
+  }
+  __syncthreads();
+  tail_cycle(a, sm, 0);
+  for (int idx = threadIdx.x; idx < n0; idx += blockDim.x) {
+    int j = idx / m0.W, i = idx - j * m0.W;
+    a.ge[(int64_t)j * a.gld + i] = e0[idx];
   }
 }
 
 // ---------------------------------------------------------------- plan
 struct Level {
   int H = 0, W = 0;
-  int64_t ld = 0;        // row stride of the real arrays
-  int analytic = 0;      // every cell fluid and every interior face open
-  std::vector<uint8_t> code;  // H * W codes (host), empty when analytic
-  int64_t off_e = 0, off_b = 0, off_r = 0, off_code = 0;
+  int64_t ld = 0;              // row stride of the real arrays
+  int analytic = 0;            // every cell fluid and every interior face open
+  std::vector<uint8_t> code;   // H * W codes (host), empty when analytic
+  int64_t off_e = 0, off_b = 0, off_code = 0;
 };
 
 }  // namespace sg
 
 struct sg_gmg_plan {
-  int H, W, precision, cycle, pre, post, coarsest;
-  double omega;
+  int H = 0, W = 0, precision = 0, cycle = 0, pre = 0, post = 0, coarsest = 0;
+  double omega = 1.0;
   std::vector<sg::Level> levels;
   std::vector<double> pinv;  // coarsest pseudo-inverse, n x n
-  int64_t off_pinv, off_bfine, off_partial, off_scalars, bytes;
-  int64_t ld_bfine;
-  int64_t n_partial;
-  char* ws;  // bound device workspace
+  int tail_start = 0;        // first level handled by the single-block tail kernel
+  int64_t tail_smem = 0;     // its dynamic shared memory (bytes)
+  int64_t off_pinv = 0, off_bfine = 0, off_partial = 0, off_state = 0, bytes = 0;
+  int64_t ld_bfine = 0;
+  int64_t n_partial = 0;
+  char* ws = nullptr;        // bound device workspace
+  // cached solve graph
+  cudaStream_t capture_stream = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const void* g_p = nullptr;
+  const void* g_div = nullptr;
+  int64_t g_ldp = 0, g_ldd = 0;
+  int g_div_dtype = -1;
+  int prologue_nodes = 0, body_nodes = 0;
 };
 
 namespace sg {
@@ -295,7 +508,6 @@ static bool coarsest_pinv(const std::vector<uint8_t>& code, int H, int W, std::v
           A[(size_t)k * n + nb[q]] -= 1.0;
         }
     }
-  // connected components over open faces
   std::vector<int> comp(n, -1);
   std::vector<int> stack;
   std::vector<int> sizes;
@@ -324,10 +536,9 @@ static bool coarsest_pinv(const std::vector<uint8_t>& code, int H, int W, std::v
       if (comp[a] >= 0 && comp[a] == comp[b]) M[(size_t)a * n + b] += 1.0 / sizes[comp[a]];
   for (int a = 0; a < n; ++a)
     if (comp[a] < 0) M[(size_t)a * n + a] = 1.0;  // non-fluid rows: identity, removed below
-  // Gauss-Jordan inversion with partial pivoting
   std::vector<double> I((size_t)n * n, 0.0);
   for (int a = 0; a < n; ++a) I[(size_t)a * n + a] = 1.0;
-  for (int col = 0; col < n; ++col) {
+  for (int col = 0; col < n; ++col) {  // Gauss-Jordan with partial pivoting
     int piv = col;
     for (int r = col + 1; r < n; ++r)
       if (std::fabs(M[(size_t)r * n + col]) > std::fabs(M[(size_t)piv * n + col])) piv = r;
@@ -367,7 +578,6 @@ static LevelMask level_mask(const sg_gmg_plan* p, int k) {
   const Level& L = p->levels[k];
   LevelMask m;
   m.code = L.analytic ? nullptr : (const uint8_t*)(p->ws + L.off_code);
-  m.ld = L.W;
   m.analytic = L.analytic;
   m.H = L.H;
   m.W = L.W;
@@ -375,103 +585,203 @@ static LevelMask level_mask(const sg_gmg_plan* p, int k) {
 }
 
 template <typename T>
-static T* lvl_ptr(const sg_gmg_plan* p, int64_t off) {
+static T* ws_ptr(const sg_gmg_plan* p, int64_t off) {
   return (T*)(p->ws + off);
 }
 
-// One cycle on level k: e_k updated in place for A_k e_k = b_k.
+static GmgState* state_ptr(const sg_gmg_plan* p) { return (GmgState*)(p->ws + p->off_state); }
+
 template <typename T>
-static void cycle(const sg_gmg_plan* p, int k, cudaStream_t s) {
-  const Level& L = p->levels[k];
-  LevelMask m = level_mask(p, k);
-  T* e = lvl_ptr<T>(p, L.off_e);
-  T* b = lvl_ptr<T>(p, L.off_b);
+static int tail_launch(const sg_gmg_plan* p, bool zero_init, cudaStream_t s) {
+  TailArgs<T> a;
+  std::memset(&a, 0, sizeof(a));
   int nl = (int)p->levels.size();
-  if (k == nl - 1) {
-    int n = L.H * L.W;
-    SG_LAUNCH(k_gmg_coarse_solve<T><<<1, 256, n * sizeof(double), s>>>(L.H, L.W, b, L.ld, e, L.ld,
-                                                             (const double*)(p->ws + p->off_pinv)));
+  a.n = nl - p->tail_start;
+  int64_t off = 0;
+  for (int q = 0; q < a.n; ++q) {
+    const Level& L = p->levels[p->tail_start + q];
+    a.m[q] = level_mask(p, p->tail_start + q);
+    a.off_e[q] = (int)off;
+    off += (int64_t)L.H * L.W;
+    a.off_b[q] = (int)off;
+    off += (int64_t)L.H * L.W;
+    off = (off + 3) & ~(int64_t)3;
+  }
+  const Level& L0 = p->levels[p->tail_start];
+  a.ge = ws_ptr<T>(p, L0.off_e);
+  a.gb = ws_ptr<T>(p, L0.off_b);
+  a.gld = L0.ld;
+  a.pinv = (const double*)(p->ws + p->off_pinv);
+  a.omega = (T)p->omega;
+  a.pre = p->pre;
+  a.post = p->post;
+  a.wcycle = p->cycle;
+  a.zero_init = zero_init ? 1 : 0;
+  SG_LAUNCH(k_gmg_tail<T><<<1, kTailThreads, p->tail_smem, s>>>(a));
+  return SG_OK;
+}
+
+// One cycle on level k for A_k e_k = b_k; zero_init: start from e_k = 0.
+template <typename T>
+static void cycle(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
+  if (k == p->tail_start) {
+    tail_launch<T>(p, zero_init, s);
     return;
   }
+  const Level& L = p->levels[k];
+  LevelMask m = level_mask(p, k);
+  T* e = ws_ptr<T>(p, L.off_e);
+  T* b = ws_ptr<T>(p, L.off_b);
   const Level& C = p->levels[k + 1];
   LevelMask cm = level_mask(p, k + 1);
   dim3 gh = grid2d((L.W + 1) / 2, L.H);
+  if (zero_init && p->pre == 0) cudaMemsetAsync(e, 0, sizeof(T) * L.ld * L.H, s);
   for (int sw = 0; sw < p->pre; ++sw)
     for (int color = 0; color < 2; ++color)
-      SG_LAUNCH(k_gmg_rbgs<T><<<gh, block2d(), 0, s>>>(L.H, L.W, e, L.ld, b, m, (T)p->omega, color));
-  T* r = lvl_ptr<T>(p, L.off_r);
-  SG_LAUNCH(k_gmg_residual<T, T><<<grid2d(L.W, L.H), block2d(), 0, s>>>(L.H, L.W, e, L.ld, b, L.ld, m, r, L.ld, nullptr));
-  T* bc = lvl_ptr<T>(p, C.off_b);
-  T* ec = lvl_ptr<T>(p, C.off_e);
-  SG_LAUNCH(k_gmg_restrict<T><<<grid2d(C.W, C.H), block2d(), 0, s>>>(L.H, L.W, r, L.ld, m, C.H, C.W, bc, C.ld, cm));
-  cudaMemsetAsync(ec, 0, sizeof(T) * C.ld * C.H, s);
+      SG_LAUNCH(k_gmg_rbgs<T><<<gh, block2d(), 0, s>>>(L.H, L.W, e, L.ld, b, m, (T)p->omega, color,
+                                                         (zero_init && sw == 0 && color == 0) ? 1 : 0));
+  SG_LAUNCH(k_gmg_residual_restrict<T><<<grid2d(C.W, C.H), block2d(), 0, s>>>(e, b, L.ld, m, ws_ptr<T>(p, C.off_b),
+                                                                               C.ld, cm));
+  int nl = (int)p->levels.size();
   int reps = (p->cycle == 1 && k + 1 < nl - 1) ? 2 : 1;
-  for (int q = 0; q < reps; ++q) cycle<T>(p, k + 1, s);
-  SG_LAUNCH(k_gmg_prolong_add<T><<<grid2d(L.W, L.H), block2d(), 0, s>>>(C.H, C.W, ec, C.ld, cm, L.H, L.W, e, L.ld, m));
+  for (int q = 0; q < reps; ++q) cycle<T>(p, k + 1, q == 0, s);
+  SG_LAUNCH(k_gmg_prolong_add<T><<<grid2d(L.W, L.H), block2d(), 0, s>>>(ws_ptr<T>(p, C.off_e), C.ld, cm, e, L.ld, m));
   for (int sw = 0; sw < p->post; ++sw)
     for (int color = 0; color < 2; ++color)
-      SG_LAUNCH(k_gmg_rbgs<T><<<gh, block2d(), 0, s>>>(L.H, L.W, e, L.ld, b, m, (T)p->omega, color));
+      SG_LAUNCH(k_gmg_rbgs<T><<<gh, block2d(), 0, s>>>(L.H, L.W, e, L.ld, b, m, (T)p->omega, color, 0));
 }
 
-// Fine-level residual r = bfine - A p -> cycle rhs b_0 (+ norm into scalars[slot]).
-template <typename TP, typename TC>
-static void fine_residual(const sg_gmg_plan* p, const TP* pp, int64_t ldp, double* out, cudaStream_t s) {
+// Prologue: bf = alpha div, ||bf||, r0 = bf - A p -> cycle rhs, relres0 and the loop condition.
+template <typename TP, typename TD, typename TC>
+static void prologue(const sg_gmg_plan* p, const TP* pp, int64_t ldp, const TD* div, int64_t ldd,
+                     cudaGraphConditionalHandle h, int use_handle, cudaStream_t s) {
   const Level& L = p->levels[0];
   LevelMask m = level_mask(p, 0);
   double* part = (double*)(p->ws + p->off_partial);
-  double* scal = (double*)(p->ws + p->off_scalars);
+  GmgState* st = state_ptr(p);
   dim3 g = grid2d(L.W, L.H);
-  SG_LAUNCH(k_gmg_residual<TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, pp, ldp, (const TP*)(p->ws + p->off_bfine), p->ld_bfine, m,
-                                                 lvl_ptr<TC>(p, L.off_b), L.ld, part));
-  SG_LAUNCH(k_gmg_finalize<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), out, scal, 1));
+  TP* bf = (TP*)(p->ws + p->off_bfine);
+  SG_LAUNCH(k_gmg_rhs<TD, TP><<<g, block2d(), 0, s>>>(L.H, L.W, div, ldd, st, m, bf, p->ld_bfine, part));
+  SG_LAUNCH(k_gmg_finalize_norm<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st));
+  SG_LAUNCH(k_gmg_fine_residual<TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, pp, ldp, bf, p->ld_bfine, m,
+                                                                   ws_ptr<TC>(p, L.off_b), L.ld, part));
+  SG_LAUNCH(k_gmg_finalize_rel<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st, h, use_handle, 0));
+}
+
+// Body: one cycle, p += e, new residual, relres and the loop condition.
+template <typename TP, typename TC>
+static void body(const sg_gmg_plan* p, TP* pp, int64_t ldp, cudaGraphConditionalHandle h, int use_handle,
+                 cudaStream_t s) {
+  const Level& L = p->levels[0];
+  LevelMask m = level_mask(p, 0);
+  double* part = (double*)(p->ws + p->off_partial);
+  GmgState* st = state_ptr(p);
+  dim3 g = grid2d(L.W, L.H);
+  cycle<TC>(p, 0, true, s);
+  SG_LAUNCH(k_gmg_correct<TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, pp, ldp, ws_ptr<TC>(p, L.off_e), L.ld));
+  SG_LAUNCH(k_gmg_fine_residual<TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, pp, ldp, (const TP*)(p->ws + p->off_bfine),
+                                                                   p->ld_bfine, m, ws_ptr<TC>(p, L.off_b), L.ld, part));
+  SG_LAUNCH(k_gmg_finalize_rel<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st, h, use_handle, 1));
+}
+
+static unsigned long long counter() { return launch_count(); }
+
+#define SG_CUDA_TRY(x, what)                                                              \
+  do {                                                                                    \
+    cudaError_t _e = (x);                                                                 \
+    if (_e != cudaSuccess) return fail(SG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(_e)); \
+  } while (0)
+
+// Capture prologue + WHILE(body) into one executable graph for these pointers.
+template <typename TP, typename TD, typename TC>
+static int build_graph(sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div, int64_t ldd) {
+  if (p->exec) {
+    cudaGraphExecDestroy(p->exec);
+    p->exec = nullptr;
+  }
+  if (!p->capture_stream) SG_CUDA_TRY(cudaStreamCreateWithFlags(&p->capture_stream, cudaStreamNonBlocking), "stream");
+  cudaStream_t cs = p->capture_stream;
+  cudaGraph_t g = nullptr;
+  SG_CUDA_TRY(cudaGraphCreate(&g, 0), "cudaGraphCreate");
+  cudaGraphConditionalHandle h;
+  SG_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, g, 0, 0), "cudaGraphConditionalHandleCreate");
+  SG_CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+              "begin capture");
+  unsigned long long c0 = counter();
+  prologue<TP, TD, TC>(p, pp, ldp, div, ldd, h, 1, cs);
+  unsigned long long c1 = counter();
+  cudaStreamCaptureStatus cst;
+  cudaGraph_t cg = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  SG_CUDA_TRY(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &cg, &deps, &ndeps), "capture info");
+  alignas(cudaGraphNodeParams) unsigned char cpbuf[sizeof(cudaGraphNodeParams)];
+  std::memset(cpbuf, 0, sizeof(cpbuf));
+  cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cpbuf);
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  SG_CUDA_TRY(cudaGraphAddNode(&cnode, cg, deps, ndeps, &cp), "add conditional node");
+  cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+  SG_CUDA_TRY(cudaStreamUpdateCaptureDependencies(cs, &cnode, 1, cudaStreamSetCaptureDependencies), "update deps");
+  SG_CUDA_TRY(cudaStreamEndCapture(cs, &g), "end capture");
+  SG_CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+              "begin body capture");
+  body<TP, TC>(p, pp, ldp, h, 1, cs);
+  unsigned long long c2 = counter();
+  SG_CUDA_TRY(cudaStreamEndCapture(cs, &bodyg), "end body capture");
+  cudaError_t e = cudaGraphInstantiate(&p->exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(SG_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+  p->prologue_nodes = (int)(c1 - c0);
+  p->body_nodes = (int)(c2 - c1);
+  p->g_p = pp;
+  p->g_ldp = ldp;
+  p->g_div = div;
+  p->g_ldd = ldd;
+  p->g_div_dtype = sizeof(TD) == 4 ? SG_F32 : SG_F64;
+  return SG_OK;
 }
 
 template <typename TP, typename TD, typename TC>
-static int solve_impl(sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div, int64_t ldd, double alpha, double tol,
-                      int max_cycles, int check_every, int* cycles_out, double* relres_out, double* relres_dev,
-                      int fixed_cycles, cudaStream_t s) {
-  const Level& L = p->levels[0];
-  LevelMask m = level_mask(p, 0);
-  double* part = (double*)(p->ws + p->off_partial);
-  double* scal = (double*)(p->ws + p->off_scalars);  // [0] = ||b||, [1] = relres
-  dim3 g = grid2d(L.W, L.H);
-  SG_LAUNCH(k_gmg_rhs<TD, TP><<<g, block2d(), 0, s>>>(L.H, L.W, div, ldd, alpha, m, (TP*)(p->ws + p->off_bfine), p->ld_bfine, part));
-  SG_LAUNCH(k_gmg_finalize<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), scal, nullptr, 0));
-  double* res_slot = relres_dev ? relres_dev : scal + 1;
-  fine_residual<TP, TC>(p, pp, ldp, res_slot, s);
-  TC* e0 = lvl_ptr<TC>(p, L.off_e);
-  int cycles = 0;
-  double rel = 0.0;
-  int n = fixed_cycles >= 0 ? fixed_cycles : max_cycles;
-  if (fixed_cycles < 0) {
-    if (cudaMemcpyAsync(&rel, res_slot, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess)
-      return check_launch("sg_gmg_solve");
-    if (!(rel == rel) || std::isinf(rel)) return fail(SG_ERR_NONFINITE, "non-finite initial residual");
-    if (rel <= tol) n = 0;
+static int solve_async_impl(sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div, int64_t ldd, double alpha, double tol,
+                            int max_cycles, cudaStream_t s) {
+  int dd = sizeof(TD) == 4 ? SG_F32 : SG_F64;
+  if (!p->exec || p->g_p != pp || p->g_ldp != ldp || p->g_div != div || p->g_ldd != ldd || p->g_div_dtype != dd) {
+    int rc = build_graph<TP, TD, TC>(p, pp, ldp, div, ldd);
+    if (rc != SG_OK) return rc;
   }
-  for (int c = 0; c < n; ++c) {
-    cudaMemsetAsync(e0, 0, sizeof(TC) * L.ld * L.H, s);
-    cycle<TC>(p, 0, s);
-    SG_LAUNCH(k_gmg_correct<TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, pp, ldp, e0, L.ld));
-    ++cycles;
-    double* slot = relres_dev ? relres_dev + cycles : scal + 1;
-    fine_residual<TP, TC>(p, pp, ldp, slot, s);
-    if (fixed_cycles < 0 && (cycles % check_every == 0 || cycles == n)) {
-      if (cudaMemcpyAsync(&rel, slot, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-          cudaStreamSynchronize(s) != cudaSuccess)
-        return check_launch("sg_gmg_solve");
-      if (!(rel == rel) || std::isinf(rel)) return fail(SG_ERR_NONFINITE, "non-finite residual after %d cycles", cycles);
-      if (rel <= tol) break;
-    }
-  }
-  int rc = check_launch("sg_gmg_solve");
-  if (rc != SG_OK) return rc;
-  if (cycles_out) *cycles_out = cycles;
-  if (relres_out) *relres_out = rel;
-  if (fixed_cycles < 0 && rel > tol)
-    return fail(SG_ERR_NOT_CONVERGED, "relative residual %.3e > tol %.3e after %d cycles", rel, tol, cycles);
-  return SG_OK;
+  SG_LAUNCH(k_gmg_set_params<<<1, 1, 0, s>>>(state_ptr(p), alpha, tol, max_cycles));
+  SG_CUDA_TRY(cudaGraphLaunch(p->exec, s), "cudaGraphLaunch");
+  return check_launch("sg_gmg_solve_async");
+}
+
+// Eager (non-graph) execution of exactly n cycles; capturable by the caller.
+template <typename TP, typename TD, typename TC>
+static int cycles_eager_impl(sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div, int64_t ldd, double alpha, int n,
+                             double* relres_dev, cudaStream_t s) {
+  SG_LAUNCH(k_gmg_set_params<<<1, 1, 0, s>>>(state_ptr(p), alpha, -1.0, n));
+  cudaGraphConditionalHandle none = 0;
+  prologue<TP, TD, TC>(p, pp, ldp, div, ldd, none, 0, s);
+  for (int c = 0; c < n; ++c) body<TP, TC>(p, pp, ldp, none, 0, s);
+  int m = std::min(n + 1, kHist);
+  SG_CUDA_TRY(cudaMemcpyAsync(relres_dev, state_ptr(p)->history, sizeof(double) * m, cudaMemcpyDeviceToDevice, s),
+              "history copy");
+  return check_launch("sg_gmg_cycles_async");
+}
+
+template <typename TP, typename TD, typename TC>
+static int solve_async_typed(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div, double alpha,
+                             double tol, int max_cycles, cudaStream_t s) {
+  return solve_async_impl<TP, TD, TC>(plan, (TP*)p, ld_p, (const TD*)div, ld_div, alpha, tol, max_cycles, s);
+}
+
+template <typename TP, typename TD, typename TC>
+static int cycles_typed(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div, double alpha, int n,
+                        double* relres_dev, cudaStream_t s) {
+  return cycles_eager_impl<TP, TD, TC>(plan, (TP*)p, ld_p, (const TD*)div, ld_div, alpha, n, relres_dev, s);
 }
 
 }  // namespace sg
@@ -489,6 +799,7 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
   SG_REQUIRE(coarsest >= 1 && coarsest <= 16, "coarsest must be in 1..16");
   SG_REQUIRE(omega > 0.0 && omega < 2.0, "omega must be in (0, 2)");
   SG_REQUIRE(pre_sweeps >= 0 && post_sweeps >= 0 && pre_sweeps + post_sweeps >= 1, "need at least one smoothing sweep");
+  SG_REQUIRE(pre_sweeps <= 16 && post_sweeps <= 16, "at most 16 sweeps per side");
   SG_REQUIRE(cycle_type == 0 || cycle_type == 1, "cycle must be 0 (V) or 1 (W)");
   SG_REQUIRE(precision >= SG_GMG_FP32 && precision <= SG_GMG_MIXED, "bad precision");
   std::vector<uint8_t> fl((size_t)H * W), fu((size_t)H * (W + 1), 0), fv((size_t)(H + 1) * W, 0);
@@ -521,7 +832,6 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
   p->post = post_sweeps;
   p->coarsest = coarsest;
   p->omega = omega;
-  p->ws = nullptr;
   int h = (int)H, w = (int)W;
   while (true) {
     Level L;
@@ -530,7 +840,7 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
     L.analytic = level_is_open(fl, fu, fv, h, w) ? 1 : 0;
     if (!L.analytic) L.code = pack_codes(fl, fu, fv, h, w);
     p->levels.push_back(L);
-    if (std::max(h, w) <= coarsest) break;
+    if (std::max(h, w) <= coarsest || (int)p->levels.size() == kMaxLevels) break;
     int hc = (h + 1) / 2, wc = (w + 1) / 2;
     std::vector<uint8_t> cfl((size_t)hc * wc, 0), cfu((size_t)hc * (wc + 1), 0), cfv((size_t)(hc + 1) * wc, 0);
     for (int J = 0; J < hc; ++J)
@@ -553,14 +863,33 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
     h = hc;
     w = wc;
   }
+  if (std::max(p->levels.back().H, p->levels.back().W) > coarsest) {
+    delete p;
+    return fail(SG_ERR_CAPACITY, "grid needs more than %d levels", kMaxLevels);
+  }
   Level& last = p->levels.back();
   std::vector<uint8_t> lastcode = last.analytic ? pack_codes(fl, fu, fv, last.H, last.W) : last.code;
   if (!coarsest_pinv(lastcode, last.H, last.W, p->pinv)) {
     delete p;
     return fail(SG_ERR_ARG, "coarsest operator could not be factorised");
   }
-  // workspace layout
+  // tail: the largest suffix of levels (each <= 128 cells a side) within the shared-memory budget
   size_t cyc = precision == SG_GMG_FP64 ? sizeof(double) : sizeof(float);
+  const int64_t budget = 200 * 1024;
+  int nl = (int)p->levels.size();
+  int64_t acc = 0;
+  p->tail_start = nl - 1;
+  for (int k = nl - 1; k >= 0; --k) {
+    const Level& L = p->levels[k];
+    int64_t need = ((2 * (int64_t)L.H * L.W + 3) & ~(int64_t)3) * (int64_t)cyc;
+    if (std::max(L.H, L.W) > 128 || acc + need > budget) break;
+    acc += need;
+    p->tail_start = k;
+  }
+  acc = 0;
+  for (int k = p->tail_start; k < nl; ++k) acc += ((2 * (int64_t)p->levels[k].H * p->levels[k].W + 3) & ~(int64_t)3);
+  p->tail_smem = acc * (int64_t)cyc;
+  // workspace layout
   size_t fine = precision == SG_GMG_FP32 ? sizeof(float) : sizeof(double);
   int64_t off = 0;
   for (auto& L : p->levels) {
@@ -569,8 +898,6 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
     L.off_e = off;
     off = align256(off + n * (int64_t)cyc);
     L.off_b = off;
-    off = align256(off + n * (int64_t)cyc);
-    L.off_r = off;
     off = align256(off + n * (int64_t)cyc);
     L.off_code = off;
     if (!L.analytic) off = align256(off + (int64_t)L.H * L.W);
@@ -584,14 +911,19 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
   p->n_partial = (int64_t)g.x * g.y;
   p->off_partial = off;
   off = align256(off + p->n_partial * 8);
-  p->off_scalars = off;
-  off = align256(off + 8 * 8);
+  p->off_state = off;
+  off = align256(off + (int64_t)sizeof(GmgState));
   p->bytes = off;
   *out = p;
   return SG_OK;
 }
 
-void sg_gmg_plan_destroy(sg_gmg_plan* plan) { delete plan; }
+void sg_gmg_plan_destroy(sg_gmg_plan* plan) {
+  if (!plan) return;
+  if (plan->exec) cudaGraphExecDestroy(plan->exec);
+  if (plan->capture_stream) cudaStreamDestroy(plan->capture_stream);
+  delete plan;
+}
 
 int64_t sg_gmg_workspace_bytes(const sg_gmg_plan* plan) { return plan ? plan->bytes : -1; }
 
@@ -601,59 +933,117 @@ int sg_gmg_bind(sg_gmg_plan* plan, void* workspace, void* stream) {
   SG_REQUIRE(plan && workspace, "null plan or workspace");
   SG_REQUIRE(((uintptr_t)workspace & 255) == 0, "workspace must be 256-byte aligned");
   plan->ws = (char*)workspace;
+  if (plan->exec) {
+    cudaGraphExecDestroy(plan->exec);
+    plan->exec = nullptr;
+  }
   cudaStream_t s = as_stream(stream);
   for (auto& L : plan->levels)
-    if (!L.analytic) {
-      cudaError_t e = cudaMemcpyAsync(plan->ws + L.off_code, L.code.data(), L.code.size(), cudaMemcpyHostToDevice, s);
-      if (e != cudaSuccess) return fail(SG_ERR_CUDA, "sg_gmg_bind: %s", cudaGetErrorString(e));
-    }
-  cudaError_t e = cudaMemcpyAsync(plan->ws + plan->off_pinv, plan->pinv.data(), plan->pinv.size() * 8,
-                                  cudaMemcpyHostToDevice, s);
-  if (e != cudaSuccess) return fail(SG_ERR_CUDA, "sg_gmg_bind: %s", cudaGetErrorString(e));
+    if (!L.analytic)
+      SG_CUDA_TRY(cudaMemcpyAsync(plan->ws + L.off_code, L.code.data(), L.code.size(), cudaMemcpyHostToDevice, s),
+                  "sg_gmg_bind codes");
+  SG_CUDA_TRY(cudaMemcpyAsync(plan->ws + plan->off_pinv, plan->pinv.data(), plan->pinv.size() * 8,
+                              cudaMemcpyHostToDevice, s),
+              "sg_gmg_bind pinv");
+  SG_CUDA_TRY(cudaMemsetAsync(plan->ws + plan->off_state, 0, sizeof(GmgState), s), "sg_gmg_bind state");
   // host vectors must outlive the asynchronous copies
-  e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return fail(SG_ERR_CUDA, "sg_gmg_bind: %s", cudaGetErrorString(e));
+  SG_CUDA_TRY(cudaStreamSynchronize(s), "sg_gmg_bind sync");
+  int smem = (int)plan->tail_smem;
+  if (plan->precision == SG_GMG_FP64)
+    SG_CUDA_TRY(cudaFuncSetAttribute(k_gmg_tail<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
+  else
+    SG_CUDA_TRY(cudaFuncSetAttribute(k_gmg_tail<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
   return SG_OK;
 }
 
-static int gmg_dispatch(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div, int div_dtype,
-                        double alpha, double tol, int max_cycles, int check_every, int* cycles_out, double* relres_out,
-                        double* relres_dev, int fixed, void* stream) {
+#define SG_GMG_TYPED(call_fp32_f32, ...)                                                           \
+  do {                                                                                             \
+    bool d32 = div_dtype == SG_F32;                                                                \
+    switch (plan->precision) {                                                                     \
+      case SG_GMG_FP32:                                                                            \
+        if (d32) return call_fp32_f32<float, float, float>(__VA_ARGS__);                           \
+        return call_fp32_f32<float, double, float>(__VA_ARGS__);                                   \
+      case SG_GMG_FP64:                                                                            \
+        if (d32) return call_fp32_f32<double, float, double>(__VA_ARGS__);                         \
+        return call_fp32_f32<double, double, double>(__VA_ARGS__);                                 \
+      default:                                                                                     \
+        if (d32) return call_fp32_f32<double, float, float>(__VA_ARGS__);                          \
+        return call_fp32_f32<double, double, float>(__VA_ARGS__);                                  \
+    }                                                                                              \
+  } while (0)
+
+static int check_solve_args(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div, int div_dtype) {
   SG_REQUIRE(plan && plan->ws, "plan not bound to a workspace");
   SG_REQUIRE(p && div && ld_p >= plan->W && ld_div >= plan->W, "bad pressure/divergence");
-  SG_REQUIRE(max_cycles >= 0 && check_every >= 1, "bad cycle limits");
   SG_REQUIRE(div_dtype == SG_F32 || div_dtype == SG_F64, "bad div dtype");
+  return SG_OK;
+}
+
+int sg_gmg_solve_async(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div, int div_dtype,
+                       double alpha, double tol, int max_cycles, void* stream) {
+  int rc = check_solve_args(plan, p, ld_p, div, ld_div, div_dtype);
+  if (rc != SG_OK) return rc;
+  SG_REQUIRE(max_cycles >= 0 && max_cycles < kHist, "max_cycles must be in 0..%d", kHist - 1);
   cudaStream_t s = as_stream(stream);
-  bool d32 = div_dtype == SG_F32;
-#define SG_GMG_CALL(TP, TD, TC)                                                                                  \
-  return solve_impl<TP, TD, TC>(plan, (TP*)p, ld_p, (const TD*)div, ld_div, alpha, tol, max_cycles, check_every, \
-                                cycles_out, relres_out, relres_dev, fixed, s)
-  switch (plan->precision) {
-    case SG_GMG_FP32:
-      if (d32) SG_GMG_CALL(float, float, float);
-      SG_GMG_CALL(float, double, float);
-    case SG_GMG_FP64:
-      if (d32) SG_GMG_CALL(double, float, double);
-      SG_GMG_CALL(double, double, double);
-    default:
-      if (d32) SG_GMG_CALL(double, float, float);
-      SG_GMG_CALL(double, double, float);
-  }
-#undef SG_GMG_CALL
+  SG_GMG_TYPED(solve_async_typed, plan, p, ld_p, div, ld_div, alpha, tol, max_cycles, s);
+}
+
+int sg_gmg_stats(sg_gmg_plan* plan, int* cycles, double* relres, int* status, long long* total_cycles, void* stream) {
+  SG_REQUIRE(plan && plan->ws, "plan not bound to a workspace");
+  GmgState st;
+  SG_CUDA_TRY(cudaMemcpyAsync(&st, state_ptr(plan), sizeof(GmgState), cudaMemcpyDeviceToHost, as_stream(stream)),
+              "sg_gmg_stats copy");
+  SG_CUDA_TRY(cudaStreamSynchronize(as_stream(stream)), "sg_gmg_stats sync");
+  if (cycles) *cycles = st.cycles;
+  if (relres) *relres = st.relres;
+  if (status) *status = st.status;
+  if (total_cycles) *total_cycles = st.total_cycles;
+  return SG_OK;
+}
+
+int sg_gmg_counters(sg_gmg_plan* plan, long long* solves, long long* cycles, long long* failures, void* stream) {
+  SG_REQUIRE(plan && plan->ws, "plan not bound to a workspace");
+  GmgState st;
+  SG_CUDA_TRY(cudaMemcpyAsync(&st, state_ptr(plan), sizeof(GmgState), cudaMemcpyDeviceToHost, as_stream(stream)),
+              "sg_gmg_counters copy");
+  SG_CUDA_TRY(cudaStreamSynchronize(as_stream(stream)), "sg_gmg_counters sync");
+  if (solves) *solves = st.solves;
+  if (cycles) *cycles = st.total_cycles;
+  if (failures) *failures = st.failures;
+  return SG_OK;
 }
 
 int sg_gmg_solve(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div, int div_dtype, double alpha,
-                 double tol, int max_cycles, int check_every, int* cycles_out, double* relres_out, void* stream) {
-  return gmg_dispatch(plan, p, ld_p, div, ld_div, div_dtype, alpha, tol, max_cycles, check_every, cycles_out,
-                      relres_out, nullptr, -1, stream);
+                 double tol, int max_cycles, int* cycles_out, double* relres_out, void* stream) {
+  int rc = sg_gmg_solve_async(plan, p, ld_p, div, ld_div, div_dtype, alpha, tol, max_cycles, stream);
+  if (rc != SG_OK) return rc;
+  int cycles = 0, status = 0;
+  double rel = 0.0;
+  rc = sg_gmg_stats(plan, &cycles, &rel, &status, nullptr, stream);
+  if (rc != SG_OK) return rc;
+  if (cycles_out) *cycles_out = cycles;
+  if (relres_out) *relres_out = rel;
+  if (status == 3) return fail(SG_ERR_NONFINITE, "non-finite residual after %d cycles", cycles);
+  if (status != 1)
+    return fail(SG_ERR_NOT_CONVERGED, "relative residual %.3e > tol %.3e after %d cycles", rel, tol, cycles);
+  return SG_OK;
 }
 
 int sg_gmg_cycles_async(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div, int div_dtype,
                         double alpha, int n_cycles, double* relres_dev, void* stream) {
+  int rc = check_solve_args(plan, p, ld_p, div, ld_div, div_dtype);
+  if (rc != SG_OK) return rc;
   SG_REQUIRE(relres_dev, "relres_dev required");
-  SG_REQUIRE(n_cycles >= 0, "n_cycles must be >= 0");
-  return gmg_dispatch(plan, p, ld_p, div, ld_div, div_dtype, alpha, 0.0, n_cycles, 1, nullptr, nullptr, relres_dev,
-                      n_cycles, stream);
+  SG_REQUIRE(n_cycles >= 0 && n_cycles < kHist, "n_cycles must be in 0..%d", kHist - 1);
+  cudaStream_t s = as_stream(stream);
+  SG_GMG_TYPED(cycles_typed, plan, p, ld_p, div, ld_div, alpha, n_cycles, relres_dev, s);
+}
+
+int sg_gmg_graph_nodes(const sg_gmg_plan* plan, int* prologue_nodes, int* body_nodes) {
+  SG_REQUIRE(plan, "null plan");
+  if (prologue_nodes) *prologue_nodes = plan->prologue_nodes;
+  if (body_nodes) *body_nodes = plan->body_nodes;
+  return SG_OK;
 }
 
 int sg_gmg_level_shape(const sg_gmg_plan* plan, int level, int* H, int* W) {
@@ -664,6 +1054,8 @@ int sg_gmg_level_shape(const sg_gmg_plan* plan, int level, int* H, int* W) {
   return SG_OK;
 }
 
+int sg_gmg_tail_start(const sg_gmg_plan* plan) { return plan ? plan->tail_start : -1; }
+
 int sg_gmg_smooth_async(sg_gmg_plan* plan, int level, int sweeps, void* stream) {
   SG_REQUIRE(plan && plan->ws, "plan not bound to a workspace");
   SG_REQUIRE(level >= 0 && level < (int)plan->levels.size() - 1, "level must be a smoothed (non-coarsest) level");
@@ -673,17 +1065,17 @@ int sg_gmg_smooth_async(sg_gmg_plan* plan, int level, int sweeps, void* stream) 
   cudaStream_t s = as_stream(stream);
   dim3 gh = grid2d((L.W + 1) / 2, L.H);
   if (plan->precision == SG_GMG_FP64) {
-    double* e = lvl_ptr<double>(plan, L.off_e);
-    const double* b = lvl_ptr<double>(plan, L.off_b);
+    double* e = ws_ptr<double>(plan, L.off_e);
+    const double* b = ws_ptr<double>(plan, L.off_b);
     for (int sw = 0; sw < sweeps; ++sw)
       for (int color = 0; color < 2; ++color)
-        SG_LAUNCH(k_gmg_rbgs<double><<<gh, block2d(), 0, s>>>(L.H, L.W, e, L.ld, b, m, plan->omega, color));
+        SG_LAUNCH(k_gmg_rbgs<double><<<gh, block2d(), 0, s>>>(L.H, L.W, e, L.ld, b, m, plan->omega, color, 0));
   } else {
-    float* e = lvl_ptr<float>(plan, L.off_e);
-    const float* b = lvl_ptr<float>(plan, L.off_b);
+    float* e = ws_ptr<float>(plan, L.off_e);
+    const float* b = ws_ptr<float>(plan, L.off_b);
     for (int sw = 0; sw < sweeps; ++sw)
       for (int color = 0; color < 2; ++color)
-        SG_LAUNCH(k_gmg_rbgs<float><<<gh, block2d(), 0, s>>>(L.H, L.W, e, L.ld, b, m, (float)plan->omega, color));
+        SG_LAUNCH(k_gmg_rbgs<float><<<gh, block2d(), 0, s>>>(L.H, L.W, e, L.ld, b, m, (float)plan->omega, color, 0));
   }
   return check_launch("sg_gmg_smooth_async");
 }

@@ -255,17 +255,35 @@ class GMGPlan:
             L._lib.sg_gmg_plan_destroy(h)
             self.handle = None
 
-    def solve(self, pressure, divergence, alpha, tol, max_cycles, check_every=1):
-        cycles = ctypes.c_int(0)
-        rel = ctypes.c_double(0.0)
+    def solve_async(self, pressure, divergence, alpha, tol, max_cycles):
+        """Graph solve without host synchronisation (outcome: stats())."""
         p, ldp = L.field(pressure, "pressure")
         d, ldd = L.field(divergence, "divergence")
-        status = L.load().sg_gmg_solve(self.handle, p, ldp, d, ldd, L.dtype_code(divergence), float(alpha), float(tol),
-                                       int(max_cycles), int(check_every), ctypes.byref(cycles), ctypes.byref(rel),
-                                       L.stream_ptr())
-        if status not in (L.SG_OK, L.SG_ERR_NOT_CONVERGED):
-            L.check(status, "sg_gmg_solve")
-        return status == L.SG_OK, cycles.value, rel.value
+        L.call("sg_gmg_solve_async", self.handle, p, ldp, d, ldd, L.dtype_code(divergence), float(alpha), float(tol),
+               int(max_cycles), L.stream_ptr())
+
+    def stats(self):
+        """(cycles, relres, status, total_cycles) of the last solve; synchronises the stream."""
+        c, s = ctypes.c_int(0), ctypes.c_int(0)
+        r = ctypes.c_double(0.0)
+        t = ctypes.c_longlong(0)
+        L.call("sg_gmg_stats", self.handle, ctypes.byref(c), ctypes.byref(r), ctypes.byref(s), ctypes.byref(t),
+               L.stream_ptr())
+        return c.value, r.value, s.value, t.value
+
+    def counters(self):
+        """(solves, cycles, failures) since the plan was bound; synchronises the stream."""
+        a, b, c = ctypes.c_longlong(0), ctypes.c_longlong(0), ctypes.c_longlong(0)
+        L.call("sg_gmg_counters", self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), L.stream_ptr())
+        return a.value, b.value, c.value
+
+    def graph_nodes(self):
+        a, b = ctypes.c_int(0), ctypes.c_int(0)
+        L.call("sg_gmg_graph_nodes", self.handle, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def tail_start(self):
+        return L.load().sg_gmg_tail_start(self.handle)
 
     def cycles_async(self, pressure, divergence, alpha, n_cycles, relres_out):
         p, ldp = L.field(pressure, "pressure")
@@ -279,17 +297,45 @@ class GeometricMultigridSolver:
 
     ``precision``: "fp32" (pressure float32), "fp64" or "mixed" (pressure float64; the
     mixed path runs FP32 cycles inside FP64 iterative refinement). A pressure tensor
-    of another dtype is solved through an internal buffer. With ``fixed_cycles > 0``
-    exactly that many cycles run without any host synchronisation (graph-capturable);
+    of another dtype is solved through an internal buffer kept across calls. A solve is
+    one CUDA graph launch (tolerance loop on the device); the outcome (``last_cycles``,
+    ``last_relres``, ``converged``) is read from the device only when asked for, and
+    ``strict=True`` reads it at once and raises NotConverged / SmokeCudaError. With
+    ``fixed_cycles > 0`` exactly that many cycles run kernel by kernel (capturable);
     per-cycle relative residuals then stay on the device in ``last_relres_dev``.
     """
 
     def __init__(self):
         self._plans = {}
-        self.last_cycles = 0
-        self.last_relres = None
-        self.converged = None
+        self._pending = None
+        self._last = (0, None, None)
         self.last_relres_dev = None
+        self._buffers = {}
+
+    def _outcome(self):
+        if self._pending is not None:
+            cycles, rel, status, _ = self._pending.stats()
+            self._pending = None
+            if status == 3:
+                self._last = (cycles, rel, False)
+                raise L.SmokeCudaError(f"multigrid: non-finite residual after {cycles} cycles")
+            self._last = (cycles, rel, status == 1)
+        return self._last
+
+    @property
+    def last_cycles(self):
+        return self._outcome()[0]
+
+    @property
+    def last_relres(self):
+        return self._outcome()[1]
+
+    @property
+    def converged(self):
+        return self._outcome()[2]
+
+    def current_plan(self):
+        return next(iter(self._plans.values()), None)
 
     def plan_for(self, H, W, fmu, fmv, device, coarsest, omega, pre, post, cycle, precision, rebuild=False):
         if isinstance(fmu, AnalyticMask):
@@ -310,19 +356,30 @@ class GeometricMultigridSolver:
         plan = self.plan_for(H, W, face_mask_u, face_mask_v, pressure.device, coarsest, omega, pre_sweeps, post_sweeps,
                              cycle, precision, rebuild_masks)
         want = torch.float32 if precision == "fp32" else torch.float64
-        p = pressure if pressure.dtype == want else pressure.to(want)
+        if pressure.dtype == want:
+            p = pressure
+        else:
+            key = (H, W, want, str(pressure.device))
+            p = self._buffers.get(key)
+            if p is None:
+                p = torch.empty((H, W), dtype=want, device=pressure.device)
+                self._buffers = {key: p}
+            p.copy_(pressure)
         alpha = calculate_alpha(cell_size, fluid_density, dt)
+        self._pending = None
         if fixed_cycles and fixed_cycles > 0:
             if self.last_relres_dev is None or self.last_relres_dev.numel() != fixed_cycles + 1:
                 self.last_relres_dev = torch.zeros(fixed_cycles + 1, dtype=torch.float64, device=pressure.device)
             plan.cycles_async(p, divergence, alpha, fixed_cycles, self.last_relres_dev)
-            self.last_cycles, self.last_relres, self.converged = fixed_cycles, None, None
+            self._last = (fixed_cycles, None, None)
         else:
-            ok, cycles, rel = plan.solve(p, divergence, alpha, tol, max_cycles, check_every)
-            self.last_cycles, self.last_relres, self.converged = cycles, rel, ok
-            if strict and not ok:
-                raise L.NotConverged(f"multigrid relative residual {rel:.3e} > {tol:.3e} after {cycles} cycles",
-                                     cycles, rel)
+            plan.solve_async(p, divergence, alpha, tol, max_cycles)
+            self._pending = plan
+            if strict:
+                cycles, rel, ok = self._outcome()
+                if not ok:
+                    raise L.NotConverged(f"multigrid relative residual {rel:.3e} > {tol:.3e} after {cycles} cycles",
+                                         cycles, rel)
         if p is not pressure:
             pressure.copy_(p)
 

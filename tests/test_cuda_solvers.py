@@ -73,19 +73,23 @@ def _problem(H, W, obstacles, seed):
     return fmu, fmv, fl, div
 
 
-@pytest.mark.parametrize("shape,obstacles", [((64, 64), False), ((96, 80), True), ((37, 50), True)])
-def test_gmg_one_cycle_vs_oracle(shape, obstacles):
+@pytest.mark.parametrize("shape,obstacles,cycle", [((64, 64), False, "V"), ((96, 80), True, "V"), ((37, 50), True, "V"),
+                                                  ((256, 256), False, "V"), ((300, 260), True, "V"),
+                                                  ((200, 176), False, "W"), ((96, 80), True, "W")])
+def test_gmg_one_cycle_vs_oracle(shape, obstacles, cycle):
+    """Grids up to ~100^2 run wholly in the single-block kernel; larger ones also use the
+    grid-wide smoother / fused restriction / prolongation kernels."""
     H, W = shape
     fmu, fmv, fl, div = _problem(H, W, obstacles, 1)
     alpha = -0.7
-    g = O.GMGOracle(fmu, fmv, fl, coarsest=8, omega=1.4)
+    g = O.GMGOracle(fmu, fmv, fl, coarsest=8, omega=1.4, cycle=cycle)
     pe = np.zeros((H, W))
     g.vcycle(0, pe, alpha * div)
     solver = sg.GeometricMultigridSolver()
     masks = (sg.OPEN_BOX, sg.OPEN_BOX) if not obstacles else (dev(fmu), dev(fmv))
     p = torch.zeros((H, W), dtype=torch.float64, device="cuda")
     # cell_size, rho, dt chosen so that alpha = -(h^2) rho / dt = -0.7
-    solver(p, dev(div), masks[0], masks[1], 0.7, 1.0, 1.0, precision="fp64", fixed_cycles=1)
+    solver(p, dev(div), masks[0], masks[1], 0.7, 1.0, 1.0, precision="fp64", fixed_cycles=1, cycle=cycle)
     got = p.cpu().numpy()
     assert np.max(np.abs(got - pe)) <= 1e-10 * np.max(np.abs(pe))
 
@@ -142,7 +146,7 @@ def test_nonfinite_input_is_reported():
     div[5, 5] = np.nan
     p = torch.zeros((H, W), dtype=torch.float64, device="cuda")
     with pytest.raises(sg.SmokeCudaError):
-        sg.GeometricMultigridSolver()(p, dev(div), sg.OPEN_BOX, sg.OPEN_BOX, 1.0, 1.0, 1.0, precision="fp64")
+        sg.GeometricMultigridSolver()(p, dev(div), sg.OPEN_BOX, sg.OPEN_BOX, 1.0, 1.0, 1.0, precision="fp64", strict=True)
     # the context stays usable after the reported failure
     q = torch.ones(4, device="cuda")
     assert float(q.sum()) == 4.0
