@@ -244,15 +244,17 @@ def run_ours(args):
         return ms, info, launches, clocks
 
     # ---- mixed precision (headline)
-    sim = make(torch.float32, "mixed")
+    only_fp64 = args.only == "fp64"
+    sim = make(torch.float64, "fp64") if only_fp64 else make(torch.float32, "mixed")
     ms, info, launches, clocks = timed(sim, args.steps, args.warmup, sample_clocks=True)
     ms_max = max_over_ranks(ms)
     value = world * cells * args.steps / (ms_max / 1e3)
     relres_ok = info["failures"] == 0 and info["solves"] == args.steps
-    if args.only_mixed:  # profiler runs: the headline timed region only
+    if args.only:  # profiler runs: one timed region only
         if rank == 0:
-            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "ms_per_step": ms_max / args.steps,
-                              "cycles": info["cycles"], "converged": relres_ok, "gpu_launches": int(launches)}))
+            print(json.dumps({"metric": METRIC, "only": args.only, "value": value, "unit": UNIT,
+                              "ms_per_step": ms_max / args.steps, "cycles": info["cycles"], "converged": relres_ok,
+                              "gpu_launches": int(launches)}))
         if world > 1:
             dist.destroy_process_group()
         return 0
@@ -335,7 +337,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only-mixed", action="store_true", help="time the mixed-precision step only (profiling)")
+    ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
+                    help="time one path only, without e2e / roofline / CPU parts (for profiler runs)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
