@@ -192,7 +192,8 @@ def run_ours(args):
         return float(t.item())
 
     def make(dtype, precision):
-        params = sg.GeometricMultigridParams(tol=TOL, max_cycles=40, precision=precision, omega=1.4)
+        params = sg.GeometricMultigridParams(tol=TOL, max_cycles=40, precision=precision, omega=1.4,
+                                             fixed_cycles=args.fixed_cycles)
         return sg.scenes.make_sim(sc, "geometric_multigrid", params, dtype=dtype, device=dev)
 
     solver = sg.get_solver("geometric_multigrid", "cuda")
@@ -337,6 +338,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fixed-cycles", type=int, default=0,
+                    help="profiling: run this many cycles per solve kernel by kernel instead of the graph loop")
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="time one path only, without e2e / roofline / CPU parts (for profiler runs)")
     args = ap.parse_args()
