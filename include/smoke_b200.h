@@ -140,8 +140,10 @@ int sg_emit_scalar(int dtype, int64_t H, int64_t W, void* field, int64_t ld, dou
                    double pos_x, double pos_y, double radius, int approach, void* stream);
 
 /* Plume sources of the benchmark scenes (no reference counterpart; the reference's
- * emitters add, these overwrite). sources: device array of n_sources x 6 doubles
- * (cx, cy, radius, density_value, v_value, noise_amp) in cell units. Cells whose
+ * emitters add, these overwrite). sources: HOST array of n_sources (<= 32) x 6 doubles
+ * (cx, cy, radius, density_value, v_value, noise_amp) in cell units, copied into the
+ * launch parameters (the array may be reused when the call returns); the launch covers
+ * the union of the sources' bounding boxes only. Cells whose
  * centre (i+.5, j+.5) is strictly inside get density; v faces at (i+.5, j) get
  * v_value + noise, u faces at (i, j+.5) get noise; noise is uniform in
  * [-amp, amp), keyed by (seed, step, component, row, column). */

@@ -116,19 +116,25 @@ __device__ __forceinline__ double lerp_ref(T a, T b, double t) {
   return (double)a + (double)d * t;
 }
 
+// floor/ceil are taken with saturating 32-bit conversions (cvt.rmi / cvt.rpi): after the
+// clamp to [0, n-1] they give the same indices as the reference's int(math.floor(x)) for
+// every double, NaN and +-Inf included (both end at an edge index).
 template <typename T>
 __device__ __forceinline__ double sample_ref(const T* __restrict__ f, int64_t ld, int64_t rows, int64_t cols,
                                              double x, double y) {
-  int64_t x0 = (int64_t)floor(x), x1 = (int64_t)ceil(x);
-  int64_t y0 = (int64_t)floor(y), y1 = (int64_t)ceil(y);
-  x0 = clampi(x0, 0, cols - 1);
-  x1 = clampi(x1, 0, cols - 1);
-  y0 = clampi(y0, 0, rows - 1);
-  y1 = clampi(y1, 0, rows - 1);
+  const int nc = (int)cols - 1, nr = (int)rows - 1;
+  int x0 = __double2int_rd(x), x1 = __double2int_ru(x);
+  int y0 = __double2int_rd(y), y1 = __double2int_ru(y);
+  x0 = min(max(x0, 0), nc);
+  x1 = min(max(x1, 0), nc);
+  y0 = min(max(y0, 0), nr);
+  y1 = min(max(y1, 0), nr);
   double tx = x - (double)x0;
   double ty = y - (double)y0;
-  T c00 = f[y0 * ld + x0], c10 = f[y0 * ld + x1];
-  T c01 = f[y1 * ld + x0], c11 = f[y1 * ld + x1];
+  const T* r0 = f + (int64_t)y0 * ld;
+  const T* r1 = f + (int64_t)y1 * ld;
+  T c00 = r0[x0], c10 = r0[x1];
+  T c01 = r1[x0], c11 = r1[x1];
   double c0 = lerp_ref(c00, c10, tx);
   double c1 = lerp_ref(c01, c11, tx);
   return c0 + (c1 - c0) * ty;

@@ -330,6 +330,7 @@ struct TailArgs {
   LevelMask m[kMaxLevels];  // masks (codes in global memory)
   int off_e[kMaxLevels];    // shared-memory offsets (elements of T), row stride = W
   int off_b[kMaxLevels];
+  int off_x;                // restriction scratch: rows x coarse columns of the first level
   T* ge;                    // first tail level in global memory (e in/out, b in)
   const T* gb;
   int64_t gld;
@@ -338,22 +339,115 @@ struct TailArgs {
   int pre, post, wcycle, zero_init;
 };
 
+// 1 / (number of open faces), n in 1..4.
+template <typename T>
+__device__ __forceinline__ T rcp_open(int n) {
+  return n == 4 ? (T)0.25 : (n == 3 ? (T)(1.0 / 3.0) : (n == 2 ? (T)0.5 : (T)1.0));
+}
+
+// Open-face bits of (j, i): analytic levels from the bounds, others from their codes.
+__device__ __forceinline__ uint8_t tail_code(const LevelMask& m, int j, int i) {
+  if (!m.analytic) return m.code[j * m.W + i];
+  return (uint8_t)(C_FLUID | (i > 0 ? C_L : 0) | (i < m.W - 1 ? C_R : 0) | (j > 0 ? C_D : 0) | (j < m.H - 1 ? C_U : 0));
+}
+
+// Half sweep over shared-memory arrays (row stride W); threads laid out 32 x 32.
 template <typename T>
 __device__ void tail_relax(const LevelMask& m, T* e, const T* b, T omega, int color) {
-  int Wh = (m.W + 1) >> 1;
-  int n = m.H * Wh;
-  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
-    int j = idx / Wh;
-    int i = 2 * (idx - j * Wh) + ((j + color) & 1);
-    if (i < m.W) relax_at(j, i, e, (int64_t)m.W, b, (int64_t)m.W, m, omega);
+  const int H = m.H, W = m.W, Wh = (W + 1) >> 1;
+  for (int j = threadIdx.y; j < H; j += blockDim.y) {
+    const int par = (j + color) & 1;
+    for (int k = threadIdx.x; k < Wh; k += blockDim.x) {
+      const int i = 2 * k + par;
+      if (i >= W) continue;
+      const uint8_t c = tail_code(m, j, i);
+      if (!(c & C_FLUID)) continue;
+      const int o = j * W + i;
+      T acc = b[o];
+      int n = 0;
+      if (c & C_L) { acc += e[o - 1]; ++n; }
+      if (c & C_R) { acc += e[o + 1]; ++n; }
+      if (c & C_D) { acc += e[o - W]; ++n; }
+      if (c & C_U) { acc += e[o + W]; ++n; }
+      if (n == 0) continue;
+      const T x = e[o];
+      e[o] = x + omega * (acc * rcp_open<T>(n) - x);
+    }
   }
+  __syncthreads();
+}
+
+// Residual b - A e at (j, i) of a shared-memory level.
+template <typename T>
+__device__ __forceinline__ T tail_res(const LevelMask& m, const T* e, const T* b, int j, int i) {
+  const uint8_t c = tail_code(m, j, i);
+  if (!(c & C_FLUID)) return (T)0;
+  const int W = m.W, o = j * W + i;
+  const T x = e[o];
+  T acc = b[o];
+  if (c & C_L) acc += e[o - 1] - x;
+  if (c & C_R) acc += e[o + 1] - x;
+  if (c & C_D) acc += e[o - W] - x;
+  if (c & C_U) acc += e[o + W] - x;
+  return acc;
+}
+
+// bc = P^T (b - A e), ec = 0. Analytic level pairs use the separable form: rows of the
+// fine level are first restricted along x into the scratch X (H x Wc), then along y.
+template <typename T>
+__device__ void tail_restrict(const LevelMask& m, const T* e, const T* b, const LevelMask& cm, T* bc, T* ec, T* X) {
+  const int H = m.H, W = m.W, Hc = cm.H, Wc = cm.W;
+  if (m.analytic && cm.analytic) {
+    for (int j = threadIdx.y; j < H; j += blockDim.y)
+      for (int I = threadIdx.x; I < Wc; I += blockDim.x) {
+        T acc = (T)0;
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+          const int i = 2 * I - 1 + d;
+          if (i < 0 || i >= W) continue;
+          const T w = (T)w1(i, I, Wc);
+          if (w != (T)0) acc += w * tail_res(m, e, b, j, i);
+        }
+        X[j * Wc + I] = acc;
+      }
+    __syncthreads();
+    for (int J = threadIdx.y; J < Hc; J += blockDim.y)
+      for (int I = threadIdx.x; I < Wc; I += blockDim.x) {
+        T acc = (T)0;
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+          const int j = 2 * J - 1 + d;
+          if (j < 0 || j >= H) continue;
+          const T w = (T)w1(j, J, Hc);
+          if (w != (T)0) acc += w * X[j * Wc + I];
+        }
+        bc[J * Wc + I] = acc;
+        ec[J * Wc + I] = (T)0;
+      }
+  } else {
+    for (int J = threadIdx.y; J < Hc; J += blockDim.y)
+      for (int I = threadIdx.x; I < Wc; I += blockDim.x) {
+        bc[J * Wc + I] = restrict_at(J, I, e, (int64_t)W, b, (int64_t)W, m, cm);
+        ec[J * Wc + I] = (T)0;
+      }
+  }
+  __syncthreads();
+}
+
+// e += P ec on the fluid cells of a shared-memory level.
+template <typename T>
+__device__ void tail_prolong(const LevelMask& m, T* e, const LevelMask& cm, const T* ec) {
+  for (int j = threadIdx.y; j < m.H; j += blockDim.y)
+    for (int i = threadIdx.x; i < m.W; i += blockDim.x)
+      if (m.fluid(j, i)) e[j * m.W + i] += prolong_at(j, i, ec, (int64_t)cm.W, cm);
   __syncthreads();
 }
 
 template <typename T>
 __device__ void tail_coarse_solve(const LevelMask& m, T* e, const T* b, const double* __restrict__ pinv) {
   int n = m.H * m.W;
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  int lane = tid & 31, warp = tid >> 5, nw = (blockDim.x * blockDim.y) >> 5;
   for (int row = warp; row < n; row += nw) {
     double acc = 0.0;
     for (int q = lane; q < n; q += 32) acc += pinv[(int64_t)row * n + q] * (double)b[q];
@@ -379,21 +473,10 @@ __device__ __noinline__ void tail_cycle(const TailArgs<T>& a, T* sm, int k) {
   const LevelMask& cm = a.m[k + 1];
   T* ec = sm + a.off_e[k + 1];
   T* bc = sm + a.off_b[k + 1];
-  int nc = cm.H * cm.W;
-  for (int idx = threadIdx.x; idx < nc; idx += blockDim.x) {
-    int J = idx / cm.W, I = idx - J * cm.W;
-    bc[idx] = restrict_at(J, I, (const T*)e, (int64_t)m.W, (const T*)b, (int64_t)m.W, m, cm);
-    ec[idx] = (T)0;
-  }
-  __syncthreads();
+  tail_restrict(m, (const T*)e, (const T*)b, cm, bc, ec, sm + a.off_x);
   int reps = (a.wcycle && k + 1 < a.n - 1) ? 2 : 1;
   for (int q = 0; q < reps; ++q) tail_cycle(a, sm, k + 1);
-  int nf = m.H * m.W;
-  for (int idx = threadIdx.x; idx < nf; idx += blockDim.x) {
-    int j = idx / m.W, i = idx - j * m.W;
-    if (m.fluid(j, i)) e[idx] += prolong_at(j, i, (const T*)ec, (int64_t)cm.W, cm);
-  }
-  __syncthreads();
+  tail_prolong(m, e, cm, (const T*)ec);
   for (int s = 0; s < a.post; ++s) {
     tail_relax(m, e, b, a.omega, 0);
     tail_relax(m, e, b, a.omega, 1);
@@ -405,20 +488,85 @@ __global__ void __launch_bounds__(kTailThreads) k_gmg_tail(const __grid_constant
   extern __shared__ __align__(16) unsigned char tail_smem[];
   T* sm = reinterpret_cast<T*>(tail_smem);
   const LevelMask& m0 = a.m[0];
-  int n0 = m0.H * m0.W;
   T* e0 = sm + a.off_e[0];
   T* b0 = sm + a.off_b[0];
-  for (int idx = threadIdx.x; idx < n0; idx += blockDim.x) {
-    int j = idx / m0.W, i = idx - j * m0.W;
-    b0[idx] = a.gb[(int64_t)j * a.gld + i];
-    e0[idx] = a.zero_init ? (T)0 : a.ge[(int64_t)j * a.gld + i];
-  }
+  for (int j = threadIdx.y; j < m0.H; j += blockDim.y)
+    for (int i = threadIdx.x; i < m0.W; i += blockDim.x) {
+      b0[j * m0.W + i] = a.gb[(int64_t)j * a.gld + i];
+      e0[j * m0.W + i] = a.zero_init ? (T)0 : a.ge[(int64_t)j * a.gld + i];
+    }
   __syncthreads();
   tail_cycle(a, sm, 0);
-  for (int idx = threadIdx.x; idx < n0; idx += blockDim.x) {
-    int j = idx / m0.W, i = idx - j * m0.W;
-    a.ge[(int64_t)j * a.gld + i] = e0[idx];
+  for (int j = threadIdx.y; j < m0.H; j += blockDim.y)
+    for (int i = threadIdx.x; i < m0.W; i += blockDim.x) a.ge[(int64_t)j * a.gld + i] = e0[j * m0.W + i];
+}
+
+// Tiled bc = P^T (b - A e) for analytic (open-box) level pairs: a 32 x 8 block restricts
+// a 32 x 8 tile of coarse cells; the fine residual of the tile (18 x 66 cells including
+// the window overlap) is computed once into shared memory from e (20 x 68) and b, then
+// restricted along x and y.
+constexpr int kRX = 32, kRY = 8;
+template <typename T>
+__global__ void __launch_bounds__(kRX * kRY) k_gmg_residual_restrict_tiled(const T* __restrict__ e,
+                                                                            const T* __restrict__ b, int64_t ld,
+                                                                            LevelMask fm, T* __restrict__ bc,
+                                                                            int64_t ldc, LevelMask cm) {
+  constexpr int EW = 2 * kRX + 4, EH = 2 * kRY + 4;  // e tile: fine cols 2I0-2 .. 2I0+2kRX+1
+  constexpr int RW = 2 * kRX + 2, RH = 2 * kRY + 2;  // residual tile: fine cols 2I0-1 .. 2I0+2kRX
+  __shared__ T se[EH][EW];
+  __shared__ T sr[RH][RW];
+  __shared__ T sx[RH][kRX];
+  const int H = fm.H, W = fm.W, Hc = cm.H, Wc = cm.W;
+  const int I0 = blockIdx.x * kRX, J0 = blockIdx.y * kRY;
+  const int fj0 = 2 * J0 - 2, fi0 = 2 * I0 - 2;
+  const int tid = threadIdx.y * kRX + threadIdx.x;
+  for (int q = tid; q < EH * EW; q += kRX * kRY) {
+    int r = q / EW, c = q - r * EW;
+    int j = fj0 + r, i = fi0 + c;
+    se[r][c] = (j >= 0 && j < H && i >= 0 && i < W) ? e[(int64_t)j * ld + i] : (T)0;
   }
+  __syncthreads();
+  for (int q = tid; q < RH * RW; q += kRX * kRY) {
+    int r = q / RW, c = q - r * RW;
+    int j = fj0 + 1 + r, i = fi0 + 1 + c;
+    T acc = (T)0;
+    if (j >= 0 && j < H && i >= 0 && i < W) {
+      const T x = se[r + 1][c + 1];
+      acc = b[(int64_t)j * ld + i];
+      if (i > 0) acc += se[r + 1][c] - x;
+      if (i < W - 1) acc += se[r + 1][c + 2] - x;
+      if (j > 0) acc += se[r][c + 1] - x;
+      if (j < H - 1) acc += se[r + 2][c + 1] - x;
+    }
+    sr[r][c] = acc;
+  }
+  __syncthreads();
+  const int I = I0 + threadIdx.x;
+  for (int r = threadIdx.y; r < RH; r += kRY) {
+    T acc = (T)0;
+    if (I < Wc) {
+#pragma unroll
+      for (int d = 0; d < 4; ++d) {
+        const int i = 2 * I - 1 + d;
+        if (i < 0 || i >= W) continue;
+        const T w = (T)w1(i, I, Wc);
+        if (w != (T)0) acc += w * sr[r][2 * threadIdx.x + d];
+      }
+    }
+    sx[r][threadIdx.x] = acc;
+  }
+  __syncthreads();
+  const int J = J0 + threadIdx.y;
+  if (I >= Wc || J >= Hc) return;
+  T acc = (T)0;
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    const int j = 2 * J - 1 + d;
+    if (j < 0 || j >= H) continue;
+    const T w = (T)w1(j, J, Hc);
+    if (w != (T)0) acc += w * sx[2 * threadIdx.y + d][threadIdx.x];
+  }
+  bc[(int64_t)J * ldc + I] = acc;
 }
 
 // ---------------------------------------------------------------- plan
@@ -607,6 +755,7 @@ static int tail_launch(const sg_gmg_plan* p, bool zero_init, cudaStream_t s) {
     off += (int64_t)L.H * L.W;
     off = (off + 3) & ~(int64_t)3;
   }
+  a.off_x = (int)off;
   const Level& L0 = p->levels[p->tail_start];
   a.ge = ws_ptr<T>(p, L0.off_e);
   a.gb = ws_ptr<T>(p, L0.off_b);
@@ -617,7 +766,7 @@ static int tail_launch(const sg_gmg_plan* p, bool zero_init, cudaStream_t s) {
   a.post = p->post;
   a.wcycle = p->cycle;
   a.zero_init = zero_init ? 1 : 0;
-  SG_LAUNCH(k_gmg_tail<T><<<1, kTailThreads, p->tail_smem, s>>>(a));
+  SG_LAUNCH(k_gmg_tail<T><<<1, dim3(32, kTailThreads / 32), p->tail_smem, s>>>(a));
   return SG_OK;
 }
 
@@ -640,8 +789,12 @@ static void cycle(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
     for (int color = 0; color < 2; ++color)
       SG_LAUNCH(k_gmg_rbgs<T><<<gh, block2d(), 0, s>>>(L.H, L.W, e, L.ld, b, m, (T)p->omega, color,
                                                          (zero_init && sw == 0 && color == 0) ? 1 : 0));
-  SG_LAUNCH(k_gmg_residual_restrict<T><<<grid2d(C.W, C.H), block2d(), 0, s>>>(e, b, L.ld, m, ws_ptr<T>(p, C.off_b),
-                                                                               C.ld, cm));
+  if (L.analytic && C.analytic)
+    SG_LAUNCH(k_gmg_residual_restrict_tiled<T><<<dim3((C.W + kRX - 1) / kRX, (C.H + kRY - 1) / kRY), dim3(kRX, kRY),
+                                                 0, s>>>(e, b, L.ld, m, ws_ptr<T>(p, C.off_b), C.ld, cm));
+  else
+    SG_LAUNCH(k_gmg_residual_restrict<T><<<grid2d(C.W, C.H), block2d(), 0, s>>>(e, b, L.ld, m, ws_ptr<T>(p, C.off_b),
+                                                                                 C.ld, cm));
   int nl = (int)p->levels.size();
   int reps = (p->cycle == 1 && k + 1 < nl - 1) ? 2 : 1;
   for (int q = 0; q < reps; ++q) cycle<T>(p, k + 1, q == 0, s);
@@ -873,22 +1026,25 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
     delete p;
     return fail(SG_ERR_ARG, "coarsest operator could not be factorised");
   }
-  // tail: the largest suffix of levels (each <= 128 cells a side) within the shared-memory budget
+  // tail: the largest suffix of levels (each <= 128 cells a side) whose e and b arrays plus
+  // the restriction scratch of its first level (H x ceil(W/2)) fit the shared-memory budget
   size_t cyc = precision == SG_GMG_FP64 ? sizeof(double) : sizeof(float);
-  const int64_t budget = 200 * 1024;
+  const int64_t budget = 220 * 1024;
   int nl = (int)p->levels.size();
-  int64_t acc = 0;
+  int64_t acc = 0;  // elements of e and b below the candidate level
   p->tail_start = nl - 1;
   for (int k = nl - 1; k >= 0; --k) {
     const Level& L = p->levels[k];
-    int64_t need = ((2 * (int64_t)L.H * L.W + 3) & ~(int64_t)3) * (int64_t)cyc;
-    if (std::max(L.H, L.W) > 128 || acc + need > budget) break;
-    acc += need;
+    int64_t arrays = acc + ((2 * (int64_t)L.H * L.W + 3) & ~(int64_t)3);
+    int64_t scratch = (int64_t)L.H * ((L.W + 1) / 2);
+    if (std::max(L.H, L.W) > 128 || (arrays + scratch) * (int64_t)cyc > budget) break;
+    acc = arrays;
     p->tail_start = k;
   }
   acc = 0;
   for (int k = p->tail_start; k < nl; ++k) acc += ((2 * (int64_t)p->levels[k].H * p->levels[k].W + 3) & ~(int64_t)3);
-  p->tail_smem = acc * (int64_t)cyc;
+  const Level& T0 = p->levels[p->tail_start];
+  p->tail_smem = (acc + (int64_t)T0.H * ((T0.W + 1) / 2)) * (int64_t)cyc;
   // workspace layout
   size_t fine = precision == SG_GMG_FP32 ? sizeof(float) : sizeof(double);
   int64_t off = 0;

@@ -311,13 +311,24 @@ __global__ void k_emit(int bw, int bh, int x0, int y0, T* __restrict__ f, int64_
   f[k] = (T)((double)f[k] + value * fo * dt);
 }
 
-// Overwriting disc sources; the last source containing a point wins.
+// Source table passed by value in the launch parameters.
+constexpr int kMaxPlumes = 32;
+struct PlumeTable {
+  int n;
+  int x0, y0;  // origin of the launch box (cells / faces)
+  double row[kMaxPlumes * 6];
+};
+
+// Overwriting disc sources over the union bounding box; the last source containing a
+// point wins.
 template <typename T>
 __global__ void k_plume(int H, int W, T* __restrict__ d, int64_t ldd, T* __restrict__ u, int64_t ldu, T* __restrict__ v,
-                        int64_t ldv, int n, const double* __restrict__ src, uint64_t seed, int64_t step) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
+                        int64_t ldv, const __grid_constant__ PlumeTable tab, uint64_t seed, int64_t step) {
+  int i = tab.x0 + blockIdx.x * blockDim.x + threadIdx.x;
+  int j = tab.y0 + blockIdx.y * blockDim.y + threadIdx.y;
   if (i > W || j > H) return;
+  const double* src = tab.row;
+  int n = tab.n;
   int hit_d = -1, hit_v = -1, hit_u = -1;
   for (int s = 0; s < n; ++s) {
     double cx = src[6 * s], cy = src[6 * s + 1], r = src[6 * s + 2];
@@ -708,11 +719,35 @@ int sg_plume_sources(int dtype, int64_t H, int64_t W, void* density, int64_t ld_
                      int64_t ld_v, int n_sources, const double* sources, uint64_t seed, int64_t step, void* stream) {
   SG_CHECK(check_grid(H, W));
   SG_REQUIRE(density && u && v && ld_d >= W && ld_u >= W + 1 && ld_v >= W, "bad fields");
-  SG_REQUIRE(n_sources >= 0 && (n_sources == 0 || sources), "bad source table");
+  SG_REQUIRE(n_sources >= 0 && n_sources <= kMaxPlumes && (n_sources == 0 || sources),
+             "source table must hold 0..%d rows", kMaxPlumes);
   if (n_sources == 0) return SG_OK;
+  PlumeTable tab;
+  std::memset(&tab, 0, sizeof(tab));
+  tab.n = n_sources;
+  // union of the sources' boxes: every cell centre / face strictly inside a disc lies in
+  // [cx - r - 1, cx + r + 1] x [cy - r - 1, cy + r + 1]
+  double xlo = 1e300, xhi = -1e300, ylo = 1e300, yhi = -1e300;
+  for (int s = 0; s < n_sources; ++s) {
+    const double* q = sources + 6 * s;
+    SG_REQUIRE(std::isfinite(q[0]) && std::isfinite(q[1]) && std::isfinite(q[2]) && q[2] >= 0.0,
+               "source %d: centre and radius must be finite, radius >= 0", s);
+    for (int k = 0; k < 6; ++k) tab.row[6 * s + k] = q[k];
+    xlo = std::min(xlo, q[0] - q[2] - 1.0);
+    xhi = std::max(xhi, q[0] + q[2] + 1.0);
+    ylo = std::min(ylo, q[1] - q[2] - 1.0);
+    yhi = std::max(yhi, q[1] + q[2] + 1.0);
+  }
+  int64_t x0 = std::max<int64_t>(0, (int64_t)std::floor(std::max(xlo, -1.0)));
+  int64_t y0 = std::max<int64_t>(0, (int64_t)std::floor(std::max(ylo, -1.0)));
+  int64_t x1 = std::min<int64_t>(W, (int64_t)std::ceil(std::min(xhi, (double)W + 1.0)));
+  int64_t y1 = std::min<int64_t>(H, (int64_t)std::ceil(std::min(yhi, (double)H + 1.0)));
+  if (x1 < x0 || y1 < y0) return SG_OK;
+  tab.x0 = (int)x0;
+  tab.y0 = (int)y0;
   SG_DISPATCH(dtype, {
-    SG_LAUNCH(k_plume<T><<<grid2d(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
-        (int)H, (int)W, (T*)density, ld_d, (T*)u, ld_u, (T*)v, ld_v, n_sources, sources, seed, step));
+    SG_LAUNCH(k_plume<T><<<grid2d(x1 - x0 + 1, y1 - y0 + 1), block2d(), 0, as_stream(stream)>>>(
+        (int)H, (int)W, (T*)density, ld_d, (T*)u, ld_u, (T*)v, ld_v, tab, seed, step));
   });
   return check_launch("sg_plume_sources");
 }

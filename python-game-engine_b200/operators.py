@@ -10,6 +10,9 @@ the mask instead of reading a plane.
 """
 from __future__ import annotations
 
+import ctypes
+
+import numpy as np
 import torch
 
 from . import _lib as L
@@ -233,17 +236,21 @@ def emit_scalar(field, value, dt, pos_x, pos_y, radius, approach):
 
 
 def plume_sources(density, velocity_u, velocity_v, sources, seed, step):
-    """Overwriting disc sources (benchmark scenes). ``sources``: CUDA float64 tensor (n, 6)."""
+    """Overwriting disc sources (benchmark scenes). ``sources``: host table of shape (n, 6)
+    (numpy array, CPU tensor or nested list) of (cx, cy, r, density, v, noise_amp) rows;
+    it travels in the kernel's launch parameters."""
     dt_code = _same_dtype(density, velocity_u, velocity_v)
     H, W = density.shape
-    if sources.dtype != torch.float64 or not sources.is_cuda or sources.dim() != 2 or sources.shape[1] != 6:
-        raise ValueError("sources must be a CUDA float64 tensor of shape (n, 6)")
-    src = sources.contiguous()
+    if isinstance(sources, torch.Tensor):
+        if sources.is_cuda:
+            raise ValueError("sources must be a host table (it is passed in the launch parameters)")
+        sources = sources.numpy()
+    src = np.ascontiguousarray(np.asarray(sources, dtype=np.float64).reshape(-1, 6))
     d, ldd = L.field(density, "density")
     u, ldu = L.field(velocity_u, "velocity_u")
     v, ldv = L.field(velocity_v, "velocity_v")
-    L.call("sg_plume_sources", dt_code, H, W, d, ldd, u, ldu, v, ldv, src.shape[0], src.data_ptr(), int(seed) & (2**64 - 1),
-           int(step), L.stream_ptr())
+    L.call("sg_plume_sources", dt_code, H, W, d, ldd, u, ldu, v, ldv, src.shape[0],
+           src.ctypes.data_as(ctypes.c_void_p), int(seed) & (2**64 - 1), int(step), L.stream_ptr())
 
 
 def build_masks(solid_mask):

@@ -28,6 +28,7 @@ from __future__ import annotations
 
 import contextlib
 
+import numpy as np
 import torch
 
 from . import _lib as L
@@ -281,9 +282,10 @@ class SmokeSimulation2D:
         self.plumes = list(plumes)
         self._plume_table = None
 
-    def set_plume_table(self, table: torch.Tensor):
-        """Use a caller-owned (n, 6) float64 CUDA table of plume rows (cx, cy, r, density,
-        v, noise) -- e.g. refreshed each step from pinned host memory."""
+    def set_plume_table(self, table):
+        """Use a caller-owned (n, 6) float64 HOST table of plume rows (cx, cy, r, density,
+        v, noise), e.g. refreshed by the caller every step; it is read at each substep and
+        travels to the GPU in the launch parameters."""
         self._plume_table = table
 
     # ------------------------------------------------------------ stepping
@@ -347,8 +349,7 @@ class SmokeSimulation2D:
             emit_channels(e, self.density, self.velocity_u, self.velocity_v, temp, dt)
         if self.plumes or self._plume_table is not None:
             if self._plume_table is None:
-                self._plume_table = torch.tensor([p.row() for p in self.plumes], dtype=torch.float64,
-                                                 device=self.device).reshape(-1, 6)
+                self._plume_table = np.asarray([p.row() for p in self.plumes], dtype=np.float64).reshape(-1, 6)
             ops.plume_sources(self.density, self.velocity_u, self.velocity_v, self._plume_table, self.seed,
                               self.step_index)
 

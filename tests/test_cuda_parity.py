@@ -216,8 +216,7 @@ def test_plume_source_vs_oracle():
         for s in specs:
             s.apply(ed, eu, ev, 17)
         td, tu, tv = dev(dens), dev(u), dev(v)
-        table = torch.tensor([[s.cx, s.cy, s.radius, s.density_value, s.v_value, s.noise_amp] for s in specs],
-                             dtype=torch.float64, device="cuda")
+        table = np.array([[s.cx, s.cy, s.radius, s.density_value, s.v_value, s.noise_amp] for s in specs])
         sg.operators.plume_sources(td, tu, tv, table, 123, 17)
         assert np.array_equal(td.cpu().numpy(), ed)
         assert np.array_equal(tu.cpu().numpy(), eu)
