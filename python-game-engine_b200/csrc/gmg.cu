@@ -226,16 +226,29 @@ __global__ void k_gmg_prolong_add(const T* __restrict__ ec, int64_t ldc, LevelMa
 
 // Fine residual r = bf - A p in the precision of p, stored as the cycle rhs (TO), with
 // per-block sums of r^2.
+// Fine-level kernels run 32 x 8 blocks over 128 x 8 cells: each thread takes 4 cells of a
+// row, 32 apart, so every load instruction is coalesced and 4 are in flight per thread.
+constexpr int kWX = 128;
+inline dim3 grid_wide(int64_t W, int64_t H) {
+  return dim3((unsigned)((W + kWX - 1) / kWX), (unsigned)((H + kBY - 1) / kBY));
+}
+
 template <typename T, typename TO>
 __global__ void k_gmg_fine_residual(int H, int W, const T* __restrict__ p, int64_t ldp, const T* __restrict__ bf,
                                     int64_t ldb, LevelMask m, TO* __restrict__ r, int64_t ldr, double* __restrict__ partial) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int ib = blockIdx.x * kWX + threadIdx.x;
   double sq = 0.0;
-  if (i < W && j < H) {
-    T acc = residual_at(j, i, p, ldp, bf, ldb, m);
-    sq = (double)acc * (double)acc;
-    r[(int64_t)j * ldr + i] = (TO)acc;
+  if (j < H) {
+#pragma unroll
+    for (int q = 0; q < kWX / 32; ++q) {
+      const int i = ib + 32 * q;
+      if (i < W) {
+        T acc = residual_at(j, i, p, ldp, bf, ldb, m);
+        sq += (double)acc * (double)acc;
+        r[(int64_t)j * ldr + i] = (TO)acc;
+      }
+    }
   }
   double s = block_sum(sq);
   if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
@@ -245,16 +258,23 @@ __global__ void k_gmg_fine_residual(int H, int W, const T* __restrict__ p, int64
 template <typename TD, typename TB>
 __global__ void k_gmg_rhs(int H, int W, const TD* __restrict__ div, int64_t ldd, const GmgState* __restrict__ st,
                           LevelMask m, TB* __restrict__ b, int64_t ldb, double* __restrict__ partial) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int ib = blockIdx.x * kWX + threadIdx.x;
+  const double alpha = st->alpha;
   double sq = 0.0;
-  if (i < W && j < H) {
-    TB v = (TB)0;
-    if (m.fluid(j, i)) {
-      v = (TB)(st->alpha * (double)div[(int64_t)j * ldd + i]);
-      sq = (double)v * (double)v;
+  if (j < H) {
+#pragma unroll
+    for (int q = 0; q < kWX / 32; ++q) {
+      const int i = ib + 32 * q;
+      if (i < W) {
+        TB v = (TB)0;
+        if (m.fluid(j, i)) {
+          v = (TB)(alpha * (double)div[(int64_t)j * ldd + i]);
+          sq += (double)v * (double)v;
+        }
+        b[(int64_t)j * ldb + i] = v;
+      }
     }
-    b[(int64_t)j * ldb + i] = v;
   }
   double s = block_sum(sq);
   if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
@@ -263,10 +283,14 @@ __global__ void k_gmg_rhs(int H, int W, const TD* __restrict__ div, int64_t ldd,
 // p += e (fine precision += cycle precision).
 template <typename TP, typename TE>
 __global__ void k_gmg_correct(int H, int W, TP* __restrict__ p, int64_t ldp, const TE* __restrict__ e, int64_t lde) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= W || j >= H) return;
-  p[(int64_t)j * ldp + i] += (TP)e[(int64_t)j * lde + i];
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int ib = blockIdx.x * kWX + threadIdx.x;
+  if (j >= H) return;
+#pragma unroll
+  for (int q = 0; q < kWX / 32; ++q) {
+    const int i = ib + 32 * q;
+    if (i < W) p[(int64_t)j * ldp + i] += (TP)e[(int64_t)j * lde + i];
+  }
 }
 
 __device__ __forceinline__ double sum_partials(const double* __restrict__ partial, int n) {
@@ -322,6 +346,9 @@ __global__ void k_gmg_finalize_rel(const double* __restrict__ partial, int n, Gm
 
 // ---------------------------------------------------------------- single-block tail
 constexpr int kMaxLevels = 16;
+// Levels up to this many cells a side run inside the single-block tail kernel; larger
+// open-box levels use the fused tiled kernels (two launches per level and cycle).
+constexpr int kTailMaxSide = 16;
 constexpr int kTailThreads = 1024;
 
 template <typename T>
@@ -569,6 +596,249 @@ __global__ void __launch_bounds__(kRX * kRY) k_gmg_residual_restrict_tiled(const
   bc[(int64_t)J * ldc + I] = acc;
 }
 
+// ---------------------------------------------------------------- fused tiled level kernels
+// For open-box levels (every cell fluid, every interior face open) one launch runs a whole
+// side of a cycle on a 64 x 32 tile of fine cells held in shared memory:
+//   pre:  SW red-black sweeps, the residual and its full-weighting restriction, reading e
+//         (not at all for a zero initial guess) and b once and writing e and the coarse rhs;
+//   post: bilinear prolongation of the coarse correction plus SW sweeps.
+// The tile carries a halo that shrinks by one ring per half sweep, so the cells it writes
+// see exactly the values a sequence of grid-wide half sweeps would give them. In shared
+// memory the tile is kept in checkerboard-split layout: the cells of each colour of a row
+// are contiguous, so a half sweep streams one colour plane and reads the other without
+// bank conflicts. Smem cell (r, c) is fine cell (j0 + r, i0 + c); its colour is
+// (par0 + r + c) & 1 with par0 = (i0 + j0) & 1 and it lives at plane[colour][r][c >> 1].
+constexpr int kTX = 64, kTY = 32;     // fine cells of a tile
+constexpr int kTBX = 32, kTBY = 8;    // threads of a tile block
+
+template <typename T>
+struct SplitTile {
+  T* e;     // 2 colour planes of EY x EXh
+  T* b;
+  int EXh, EY, par0, i0, j0, H, W;
+  __device__ __forceinline__ int colour(int r, int c) const { return (par0 + r + c) & 1; }
+  __device__ __forceinline__ T* ep(int col) const { return e + col * EY * EXh; }
+  __device__ __forceinline__ T* bp(int col) const { return b + col * EY * EXh; }
+  __device__ __forceinline__ T& E(int r, int c) const { return ep(colour(r, c))[r * EXh + (c >> 1)]; }
+  __device__ __forceinline__ T& B(int r, int c) const { return bp(colour(r, c))[r * EXh + (c >> 1)]; }
+};
+
+// Relax the cells of colour col in smem rows [rlo, rhi), columns [clo, chi) (1 <= clo,
+// chi <= EX - 1, 1 <= rlo, rhi <= EY - 1, so every neighbour is inside the tile).
+template <typename T>
+__device__ __forceinline__ void split_relax(const SplitTile<T>& t, int col, int rlo, int rhi, int clo, int chi, T omega) {
+  T* E = t.ep(col);
+  const T* Bc = t.bp(col);
+  const T* O = t.ep(1 - col);
+  const int EXh = t.EXh;
+  for (int r = rlo + (int)threadIdx.y; r < rhi; r += kTBY) {
+    const int j = t.j0 + r;
+    if (j < 0 || j >= t.H) continue;
+    const int p = (col + t.par0 + r) & 1;  // columns of colour col in this row: c = p + 2k
+    const int klo = (clo - p + 1) >> 1, khi = (chi - p + 1) >> 1;
+    for (int k = klo + (int)threadIdx.x; k < khi; k += kTBX) {
+      const int i = t.i0 + p + 2 * k;
+      if (i < 0 || i >= t.W) continue;
+      const int o = r * EXh + k;
+      T acc = Bc[o];
+      int n = 0;
+      if (i > 0) { acc += O[o + p - 1]; ++n; }
+      if (i < t.W - 1) { acc += O[o + p]; ++n; }
+      if (j > 0) { acc += O[o - EXh]; ++n; }
+      if (j < t.H - 1) { acc += O[o + EXh]; ++n; }
+      if (n == 0) continue;
+      const T x = E[o];
+      E[o] = x + omega * (acc * rcp_open<T>(n) - x);
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void split_load(const SplitTile<T>& t, const T* __restrict__ e, const T* __restrict__ b,
+                                           int64_t ld, int EX, bool load_e) {
+  for (int r = threadIdx.y; r < t.EY; r += kTBY) {
+    const int j = t.j0 + r;
+    const bool jin = j >= 0 && j < t.H;
+    const T* er = e + (int64_t)j * ld;
+    const T* br = b + (int64_t)j * ld;
+    for (int c = threadIdx.x; c < EX; c += kTBX) {
+      const int i = t.i0 + c;
+      const bool in = jin && i >= 0 && i < t.W;
+      t.E(r, c) = (in && load_e) ? er[i] : (T)0;
+      t.B(r, c) = in ? br[i] : (T)0;
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void split_store(const SplitTile<T>& t, T* __restrict__ e, int64_t ld, int halo) {
+  for (int r = halo + threadIdx.y; r < halo + kTY; r += kTBY) {
+    const int j = t.j0 + r;
+    if (j < 0 || j >= t.H) continue;
+    T* er = e + (int64_t)j * ld;
+    for (int c = halo + threadIdx.x; c < halo + kTX; c += kTBX) {
+      const int i = t.i0 + c;
+      if (i >= 0 && i < t.W) er[i] = t.E(r, c);
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T split_residual(const SplitTile<T>& t, int r, int c) {
+  const int j = t.j0 + r, i = t.i0 + c;
+  if (j < 0 || j >= t.H || i < 0 || i >= t.W) return (T)0;
+  const T x = t.E(r, c);
+  T acc = t.B(r, c);
+  if (i > 0) acc += t.E(r, c - 1) - x;
+  if (i < t.W - 1) acc += t.E(r, c + 1) - x;
+  if (j > 0) acc += t.E(r - 1, c) - x;
+  if (j < t.H - 1) acc += t.E(r + 1, c) - x;
+  return acc;
+}
+
+template <int SW>
+struct PreShape {
+  static constexpr int HALO = 2 * SW + 2;  // 2SW half sweeps + residual ring + restriction window
+  static constexpr int EX = kTX + 2 * HALO, EY = kTY + 2 * HALO, EXh = EX / 2;
+  static constexpr int XR = kTY + 2, XC = kTX / 2;
+  template <typename T>
+  static constexpr size_t bytes() { return (size_t)(4 * EY * EXh + XR * XC) * sizeof(T); }
+};
+
+template <int SW>
+struct PostShape {
+  static constexpr int HALO = 2 * SW;
+  static constexpr int EX = kTX + 2 * HALO, EY = kTY + 2 * HALO, EXh = EX / 2;
+  template <typename T>
+  static constexpr size_t bytes() { return (size_t)(4 * EY * EXh) * sizeof(T); }
+};
+
+// pre: SW sweeps + residual + full weighting into bc (coarse tile 32 x 16).
+template <typename T, int SW>
+__global__ void __launch_bounds__(kTBX* kTBY) k_gmg_pre_tiled(T* __restrict__ e, const T* __restrict__ b, int64_t ld,
+                                                               int H, int W, T* __restrict__ bc, int64_t ldc, int Hc,
+                                                               int Wc, T omega, int zero_init) {
+  using S = PreShape<SW>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  T* base = reinterpret_cast<T*>(smem);
+  SplitTile<T> t;
+  t.e = base;
+  t.b = base + 2 * S::EY * S::EXh;
+  T* X = base + 4 * S::EY * S::EXh;
+  t.EXh = S::EXh;
+  t.EY = S::EY;
+  t.i0 = blockIdx.x * kTX - S::HALO;
+  t.j0 = blockIdx.y * kTY - S::HALO;
+  t.par0 = (t.i0 + t.j0) & 1;
+  t.H = H;
+  t.W = W;
+  split_load(t, e, b, ld, S::EX, !zero_init);
+  __syncthreads();
+#pragma unroll
+  for (int hs = 0; hs < 2 * SW; ++hs) {
+    const int ring = S::HALO - 1 - hs;
+    split_relax(t, hs & 1, S::HALO - ring, S::HALO + kTY + ring, S::HALO - ring, S::HALO + kTX + ring, omega);
+    __syncthreads();
+  }
+  // residual on the tile plus one ring, in place of b
+  const int lo = S::HALO - 1;
+  for (int r = lo + threadIdx.y; r < S::HALO + kTY + 1; r += kTBY)
+    for (int c = lo + threadIdx.x; c < S::HALO + kTX + 1; c += kTBX) {
+      T res = split_residual(t, r, c);  // reads e around (r, c) and b at (r, c) only
+      t.B(r, c) = res;
+    }
+  __syncthreads();
+  // restriction along x: X[rr][I'] over fine rows of the tile plus one ring
+  const int Ip = threadIdx.x, I = blockIdx.x * (kTX / 2) + Ip;
+  T wx[4];
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    const int i = 2 * I - 1 + d;
+    wx[d] = (i >= 0 && i < W && I < Wc) ? (T)w1(i, I, Wc) : (T)0;
+  }
+  for (int rr = threadIdx.y; rr < S::XR; rr += kTBY) {
+    T acc = (T)0;
+#pragma unroll
+    for (int d = 0; d < 4; ++d)
+      if (wx[d] != (T)0) acc += wx[d] * t.B(lo + rr, 2 * Ip + lo + d);
+    X[rr * S::XC + Ip] = acc;
+  }
+  __syncthreads();
+  // restriction along y
+  for (int Jp = threadIdx.y; Jp < kTY / 2; Jp += kTBY) {
+    const int J = blockIdx.y * (kTY / 2) + Jp;
+    if (J >= Hc || I >= Wc) continue;
+    T acc = (T)0;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+      const int j = 2 * J - 1 + d;
+      if (j < 0 || j >= H) continue;
+      const T w = (T)w1(j, J, Hc);
+      if (w != (T)0) acc += w * X[(2 * Jp + d) * S::XC + Ip];
+    }
+    bc[(int64_t)J * ldc + I] = acc;
+  }
+  split_store(t, e, ld, S::HALO);
+}
+
+// post: e += P ec, then SW sweeps.
+template <typename T, int SW>
+__global__ void __launch_bounds__(kTBX* kTBY) k_gmg_post_tiled(T* __restrict__ e, const T* __restrict__ b, int64_t ld,
+                                                                int H, int W, const T* __restrict__ ec, int64_t ldc,
+                                                                int Hc, int Wc, T omega) {
+  using S = PostShape<SW>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  T* base = reinterpret_cast<T*>(smem);
+  SplitTile<T> t;
+  t.e = base;
+  t.b = base + 2 * S::EY * S::EXh;
+  t.EXh = S::EXh;
+  t.EY = S::EY;
+  t.i0 = blockIdx.x * kTX - S::HALO;
+  t.j0 = blockIdx.y * kTY - S::HALO;
+  t.par0 = (t.i0 + t.j0) & 1;
+  t.H = H;
+  t.W = W;
+  const T w9 = (T)(9.0 / 16.0), w3 = (T)(3.0 / 16.0), w1_ = (T)(1.0 / 16.0);
+  for (int r = threadIdx.y; r < S::EY; r += kTBY) {
+    const int j = t.j0 + r;
+    const bool jin = j >= 0 && j < H;
+    const int J = j >> 1;
+    int Y = J + ((j & 1) ? 1 : -1);
+    Y = Y < 0 ? 0 : (Y > Hc - 1 ? Hc - 1 : Y);
+    const T* erow = e + (int64_t)j * ld;
+    const T* brow = b + (int64_t)j * ld;
+    const T* c0 = ec + (int64_t)J * ldc;
+    const T* c1 = ec + (int64_t)Y * ldc;
+    for (int c = threadIdx.x; c < S::EX; c += kTBX) {
+      const int i = t.i0 + c;
+      T ev = (T)0, bv = (T)0;
+      if (jin && i >= 0 && i < W) {
+        const int I = i >> 1;
+        int X = I + ((i & 1) ? 1 : -1);
+        X = X < 0 ? 0 : (X > Wc - 1 ? Wc - 1 : X);
+        T acc = (T)0;
+        acc += w9 * c0[I];
+        acc += w3 * c0[X];
+        acc += w3 * c1[I];
+        acc += w1_ * c1[X];
+        ev = erow[i] + acc;
+        bv = brow[i];
+      }
+      t.E(r, c) = ev;
+      t.B(r, c) = bv;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int hs = 0; hs < 2 * SW; ++hs) {
+    const int ring = S::HALO - 1 - hs;
+    split_relax(t, hs & 1, S::HALO - ring, S::HALO + kTY + ring, S::HALO - ring, S::HALO + kTX + ring, omega);
+    __syncthreads();
+  }
+  split_store(t, e, ld, S::HALO);
+}
+
 // ---------------------------------------------------------------- plan
 struct Level {
   int H = 0, W = 0;
@@ -770,11 +1040,72 @@ static int tail_launch(const sg_gmg_plan* p, bool zero_init, cudaStream_t s) {
   return SG_OK;
 }
 
+// The fused tiled kernels serve open-box level pairs with 1..3 sweeps per side.
+static bool fused_level(const sg_gmg_plan* p, int k) {
+  const Level& L = p->levels[k];
+  const Level& C = p->levels[k + 1];
+  return L.analytic && C.analytic && L.H >= 2 && L.W >= 2 && p->pre >= 1 && p->pre <= 3 && p->post >= 1 &&
+         p->post <= 3;
+}
+
+template <typename T, int SW>
+static void launch_pre(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
+  const Level& L = p->levels[k];
+  const Level& C = p->levels[k + 1];
+  dim3 g((L.W + kTX - 1) / kTX, (L.H + kTY - 1) / kTY);
+  SG_LAUNCH(k_gmg_pre_tiled<T, SW><<<g, dim3(kTBX, kTBY), PreShape<SW>::template bytes<T>(), s>>>(
+      ws_ptr<T>(p, L.off_e), ws_ptr<T>(p, L.off_b), L.ld, L.H, L.W, ws_ptr<T>(p, C.off_b), C.ld, C.H, C.W,
+      (T)p->omega, zero_init ? 1 : 0));
+}
+
+template <typename T, int SW>
+static void launch_post(const sg_gmg_plan* p, int k, cudaStream_t s) {
+  const Level& L = p->levels[k];
+  const Level& C = p->levels[k + 1];
+  dim3 g((L.W + kTX - 1) / kTX, (L.H + kTY - 1) / kTY);
+  SG_LAUNCH(k_gmg_post_tiled<T, SW><<<g, dim3(kTBX, kTBY), PostShape<SW>::template bytes<T>(), s>>>(
+      ws_ptr<T>(p, L.off_e), ws_ptr<T>(p, L.off_b), L.ld, L.H, L.W, ws_ptr<T>(p, C.off_e), C.ld, C.H, C.W,
+      (T)p->omega));
+}
+
+template <typename T>
+static int set_tiled_smem_limits() {
+  cudaError_t e = cudaSuccess;
+#define SG_TILED_ATTR(SW)                                                                                          \
+  e = cudaFuncSetAttribute(k_gmg_pre_tiled<T, SW>, cudaFuncAttributeMaxDynamicSharedMemorySize,                    \
+                           (int)PreShape<SW>::template bytes<T>());                                                \
+  if (e != cudaSuccess) return fail(SG_ERR_CUDA, "smem attr: %s", cudaGetErrorString(e));                          \
+  e = cudaFuncSetAttribute(k_gmg_post_tiled<T, SW>, cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
+                           (int)PostShape<SW>::template bytes<T>());                                               \
+  if (e != cudaSuccess) return fail(SG_ERR_CUDA, "smem attr: %s", cudaGetErrorString(e));
+  SG_TILED_ATTR(1)
+  SG_TILED_ATTR(2)
+  SG_TILED_ATTR(3)
+#undef SG_TILED_ATTR
+  return SG_OK;
+}
+
 // One cycle on level k for A_k e_k = b_k; zero_init: start from e_k = 0.
 template <typename T>
 static void cycle(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
   if (k == p->tail_start) {
     tail_launch<T>(p, zero_init, s);
+    return;
+  }
+  const int nl = (int)p->levels.size();
+  if (fused_level(p, k)) {
+    switch (p->pre) {
+      case 1: launch_pre<T, 1>(p, k, zero_init, s); break;
+      case 2: launch_pre<T, 2>(p, k, zero_init, s); break;
+      default: launch_pre<T, 3>(p, k, zero_init, s); break;
+    }
+    int reps = (p->cycle == 1 && k + 1 < nl - 1) ? 2 : 1;
+    for (int q = 0; q < reps; ++q) cycle<T>(p, k + 1, q == 0, s);
+    switch (p->post) {
+      case 1: launch_post<T, 1>(p, k, s); break;
+      case 2: launch_post<T, 2>(p, k, s); break;
+      default: launch_post<T, 3>(p, k, s); break;
+    }
     return;
   }
   const Level& L = p->levels[k];
@@ -795,7 +1126,6 @@ static void cycle(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
   else
     SG_LAUNCH(k_gmg_residual_restrict<T><<<grid2d(C.W, C.H), block2d(), 0, s>>>(e, b, L.ld, m, ws_ptr<T>(p, C.off_b),
                                                                                  C.ld, cm));
-  int nl = (int)p->levels.size();
   int reps = (p->cycle == 1 && k + 1 < nl - 1) ? 2 : 1;
   for (int q = 0; q < reps; ++q) cycle<T>(p, k + 1, q == 0, s);
   SG_LAUNCH(k_gmg_prolong_add<T><<<grid2d(L.W, L.H), block2d(), 0, s>>>(ws_ptr<T>(p, C.off_e), C.ld, cm, e, L.ld, m));
@@ -812,7 +1142,7 @@ static void prologue(const sg_gmg_plan* p, const TP* pp, int64_t ldp, const TD* 
   LevelMask m = level_mask(p, 0);
   double* part = (double*)(p->ws + p->off_partial);
   GmgState* st = state_ptr(p);
-  dim3 g = grid2d(L.W, L.H);
+  dim3 g = grid_wide(L.W, L.H);
   TP* bf = (TP*)(p->ws + p->off_bfine);
   SG_LAUNCH(k_gmg_rhs<TD, TP><<<g, block2d(), 0, s>>>(L.H, L.W, div, ldd, st, m, bf, p->ld_bfine, part));
   SG_LAUNCH(k_gmg_finalize_norm<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st));
@@ -829,7 +1159,7 @@ static void body(const sg_gmg_plan* p, TP* pp, int64_t ldp, cudaGraphConditional
   LevelMask m = level_mask(p, 0);
   double* part = (double*)(p->ws + p->off_partial);
   GmgState* st = state_ptr(p);
-  dim3 g = grid2d(L.W, L.H);
+  dim3 g = grid_wide(L.W, L.H);
   cycle<TC>(p, 0, true, s);
   SG_LAUNCH(k_gmg_correct<TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, pp, ldp, ws_ptr<TC>(p, L.off_e), L.ld));
   SG_LAUNCH(k_gmg_fine_residual<TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, pp, ldp, (const TP*)(p->ws + p->off_bfine),
@@ -1037,7 +1367,7 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
     const Level& L = p->levels[k];
     int64_t arrays = acc + ((2 * (int64_t)L.H * L.W + 3) & ~(int64_t)3);
     int64_t scratch = (int64_t)L.H * ((L.W + 1) / 2);
-    if (std::max(L.H, L.W) > 128 || (arrays + scratch) * (int64_t)cyc > budget) break;
+    if (std::max(L.H, L.W) > kTailMaxSide || (arrays + scratch) * (int64_t)cyc > budget) break;
     acc = arrays;
     p->tail_start = k;
   }
@@ -1063,7 +1393,7 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
   off = align256(off + p->ld_bfine * p->H * (int64_t)fine);
   p->off_pinv = off;
   off = align256(off + (int64_t)p->pinv.size() * 8);
-  dim3 g = grid2d(p->W, p->H);
+  dim3 g = grid_wide(p->W, p->H);
   p->n_partial = (int64_t)g.x * g.y;
   p->off_partial = off;
   off = align256(off + p->n_partial * 8);
@@ -1104,6 +1434,8 @@ int sg_gmg_bind(sg_gmg_plan* plan, void* workspace, void* stream) {
   SG_CUDA_TRY(cudaMemsetAsync(plan->ws + plan->off_state, 0, sizeof(GmgState), s), "sg_gmg_bind state");
   // host vectors must outlive the asynchronous copies
   SG_CUDA_TRY(cudaStreamSynchronize(s), "sg_gmg_bind sync");
+  int rc = plan->precision == SG_GMG_FP64 ? set_tiled_smem_limits<double>() : set_tiled_smem_limits<float>();
+  if (rc != SG_OK) return rc;
   int smem = (int)plan->tail_smem;
   if (plan->precision == SG_GMG_FP64)
     SG_CUDA_TRY(cudaFuncSetAttribute(k_gmg_tail<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
