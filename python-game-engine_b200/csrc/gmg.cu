@@ -597,247 +597,7 @@ __global__ void __launch_bounds__(kRX * kRY) k_gmg_residual_restrict_tiled(const
 }
 
 // ---------------------------------------------------------------- fused tiled level kernels
-// For open-box levels (every cell fluid, every interior face open) one launch runs a whole
-// side of a cycle on a 64 x 32 tile of fine cells held in shared memory:
-//   pre:  SW red-black sweeps, the residual and its full-weighting restriction, reading e
-//         (not at all for a zero initial guess) and b once and writing e and the coarse rhs;
-//   post: bilinear prolongation of the coarse correction plus SW sweeps.
-// The tile carries a halo that shrinks by one ring per half sweep, so the cells it writes
-// see exactly the values a sequence of grid-wide half sweeps would give them. In shared
-// memory the tile is kept in checkerboard-split layout: the cells of each colour of a row
-// are contiguous, so a half sweep streams one colour plane and reads the other without
-// bank conflicts. Smem cell (r, c) is fine cell (j0 + r, i0 + c); its colour is
-// (par0 + r + c) & 1 with par0 = (i0 + j0) & 1 and it lives at plane[colour][r][c >> 1].
-constexpr int kTX = 64, kTY = 32;     // fine cells of a tile
-constexpr int kTBX = 32, kTBY = 8;    // threads of a tile block
-
-template <typename T>
-struct SplitTile {
-  T* e;     // 2 colour planes of EY x EXh
-  T* b;
-  int EXh, EY, par0, i0, j0, H, W;
-  __device__ __forceinline__ int colour(int r, int c) const { return (par0 + r + c) & 1; }
-  __device__ __forceinline__ T* ep(int col) const { return e + col * EY * EXh; }
-  __device__ __forceinline__ T* bp(int col) const { return b + col * EY * EXh; }
-  __device__ __forceinline__ T& E(int r, int c) const { return ep(colour(r, c))[r * EXh + (c >> 1)]; }
-  __device__ __forceinline__ T& B(int r, int c) const { return bp(colour(r, c))[r * EXh + (c >> 1)]; }
-};
-
-// Relax the cells of colour col in smem rows [rlo, rhi), columns [clo, chi) (1 <= clo,
-// chi <= EX - 1, 1 <= rlo, rhi <= EY - 1, so every neighbour is inside the tile).
-template <typename T>
-__device__ __forceinline__ void split_relax(const SplitTile<T>& t, int col, int rlo, int rhi, int clo, int chi, T omega) {
-  T* E = t.ep(col);
-  const T* Bc = t.bp(col);
-  const T* O = t.ep(1 - col);
-  const int EXh = t.EXh;
-  for (int r = rlo + (int)threadIdx.y; r < rhi; r += kTBY) {
-    const int j = t.j0 + r;
-    if (j < 0 || j >= t.H) continue;
-    const int p = (col + t.par0 + r) & 1;  // columns of colour col in this row: c = p + 2k
-    const int klo = (clo - p + 1) >> 1, khi = (chi - p + 1) >> 1;
-    for (int k = klo + (int)threadIdx.x; k < khi; k += kTBX) {
-      const int i = t.i0 + p + 2 * k;
-      if (i < 0 || i >= t.W) continue;
-      const int o = r * EXh + k;
-      T acc = Bc[o];
-      int n = 0;
-      if (i > 0) { acc += O[o + p - 1]; ++n; }
-      if (i < t.W - 1) { acc += O[o + p]; ++n; }
-      if (j > 0) { acc += O[o - EXh]; ++n; }
-      if (j < t.H - 1) { acc += O[o + EXh]; ++n; }
-      if (n == 0) continue;
-      const T x = E[o];
-      E[o] = x + omega * (acc * rcp_open<T>(n) - x);
-    }
-  }
-}
-
-template <typename T>
-__device__ __forceinline__ void split_load(const SplitTile<T>& t, const T* __restrict__ e, const T* __restrict__ b,
-                                           int64_t ld, int EX, bool load_e) {
-  for (int r = threadIdx.y; r < t.EY; r += kTBY) {
-    const int j = t.j0 + r;
-    const bool jin = j >= 0 && j < t.H;
-    const T* er = e + (int64_t)j * ld;
-    const T* br = b + (int64_t)j * ld;
-    for (int c = threadIdx.x; c < EX; c += kTBX) {
-      const int i = t.i0 + c;
-      const bool in = jin && i >= 0 && i < t.W;
-      t.E(r, c) = (in && load_e) ? er[i] : (T)0;
-      t.B(r, c) = in ? br[i] : (T)0;
-    }
-  }
-}
-
-template <typename T>
-__device__ __forceinline__ void split_store(const SplitTile<T>& t, T* __restrict__ e, int64_t ld, int halo) {
-  for (int r = halo + threadIdx.y; r < halo + kTY; r += kTBY) {
-    const int j = t.j0 + r;
-    if (j < 0 || j >= t.H) continue;
-    T* er = e + (int64_t)j * ld;
-    for (int c = halo + threadIdx.x; c < halo + kTX; c += kTBX) {
-      const int i = t.i0 + c;
-      if (i >= 0 && i < t.W) er[i] = t.E(r, c);
-    }
-  }
-}
-
-template <typename T>
-__device__ __forceinline__ T split_residual(const SplitTile<T>& t, int r, int c) {
-  const int j = t.j0 + r, i = t.i0 + c;
-  if (j < 0 || j >= t.H || i < 0 || i >= t.W) return (T)0;
-  const T x = t.E(r, c);
-  T acc = t.B(r, c);
-  if (i > 0) acc += t.E(r, c - 1) - x;
-  if (i < t.W - 1) acc += t.E(r, c + 1) - x;
-  if (j > 0) acc += t.E(r - 1, c) - x;
-  if (j < t.H - 1) acc += t.E(r + 1, c) - x;
-  return acc;
-}
-
-template <int SW>
-struct PreShape {
-  static constexpr int HALO = 2 * SW + 2;  // 2SW half sweeps + residual ring + restriction window
-  static constexpr int EX = kTX + 2 * HALO, EY = kTY + 2 * HALO, EXh = EX / 2;
-  static constexpr int XR = kTY + 2, XC = kTX / 2;
-  template <typename T>
-  static constexpr size_t bytes() { return (size_t)(4 * EY * EXh + XR * XC) * sizeof(T); }
-};
-
-template <int SW>
-struct PostShape {
-  static constexpr int HALO = 2 * SW;
-  static constexpr int EX = kTX + 2 * HALO, EY = kTY + 2 * HALO, EXh = EX / 2;
-  template <typename T>
-  static constexpr size_t bytes() { return (size_t)(4 * EY * EXh) * sizeof(T); }
-};
-
-// pre: SW sweeps + residual + full weighting into bc (coarse tile 32 x 16).
-template <typename T, int SW>
-__global__ void __launch_bounds__(kTBX* kTBY) k_gmg_pre_tiled(T* __restrict__ e, const T* __restrict__ b, int64_t ld,
-                                                               int H, int W, T* __restrict__ bc, int64_t ldc, int Hc,
-                                                               int Wc, T omega, int zero_init) {
-  using S = PreShape<SW>;
-  extern __shared__ __align__(16) unsigned char smem[];
-  T* base = reinterpret_cast<T*>(smem);
-  SplitTile<T> t;
-  t.e = base;
-  t.b = base + 2 * S::EY * S::EXh;
-  T* X = base + 4 * S::EY * S::EXh;
-  t.EXh = S::EXh;
-  t.EY = S::EY;
-  t.i0 = blockIdx.x * kTX - S::HALO;
-  t.j0 = blockIdx.y * kTY - S::HALO;
-  t.par0 = (t.i0 + t.j0) & 1;
-  t.H = H;
-  t.W = W;
-  split_load(t, e, b, ld, S::EX, !zero_init);
-  __syncthreads();
-#pragma unroll
-  for (int hs = 0; hs < 2 * SW; ++hs) {
-    const int ring = S::HALO - 1 - hs;
-    split_relax(t, hs & 1, S::HALO - ring, S::HALO + kTY + ring, S::HALO - ring, S::HALO + kTX + ring, omega);
-    __syncthreads();
-  }
-  // residual on the tile plus one ring, in place of b
-  const int lo = S::HALO - 1;
-  for (int r = lo + threadIdx.y; r < S::HALO + kTY + 1; r += kTBY)
-    for (int c = lo + threadIdx.x; c < S::HALO + kTX + 1; c += kTBX) {
-      T res = split_residual(t, r, c);  // reads e around (r, c) and b at (r, c) only
-      t.B(r, c) = res;
-    }
-  __syncthreads();
-  // restriction along x: X[rr][I'] over fine rows of the tile plus one ring
-  const int Ip = threadIdx.x, I = blockIdx.x * (kTX / 2) + Ip;
-  T wx[4];
-#pragma unroll
-  for (int d = 0; d < 4; ++d) {
-    const int i = 2 * I - 1 + d;
-    wx[d] = (i >= 0 && i < W && I < Wc) ? (T)w1(i, I, Wc) : (T)0;
-  }
-  for (int rr = threadIdx.y; rr < S::XR; rr += kTBY) {
-    T acc = (T)0;
-#pragma unroll
-    for (int d = 0; d < 4; ++d)
-      if (wx[d] != (T)0) acc += wx[d] * t.B(lo + rr, 2 * Ip + lo + d);
-    X[rr * S::XC + Ip] = acc;
-  }
-  __syncthreads();
-  // restriction along y
-  for (int Jp = threadIdx.y; Jp < kTY / 2; Jp += kTBY) {
-    const int J = blockIdx.y * (kTY / 2) + Jp;
-    if (J >= Hc || I >= Wc) continue;
-    T acc = (T)0;
-#pragma unroll
-    for (int d = 0; d < 4; ++d) {
-      const int j = 2 * J - 1 + d;
-      if (j < 0 || j >= H) continue;
-      const T w = (T)w1(j, J, Hc);
-      if (w != (T)0) acc += w * X[(2 * Jp + d) * S::XC + Ip];
-    }
-    bc[(int64_t)J * ldc + I] = acc;
-  }
-  split_store(t, e, ld, S::HALO);
-}
-
-// post: e += P ec, then SW sweeps.
-template <typename T, int SW>
-__global__ void __launch_bounds__(kTBX* kTBY) k_gmg_post_tiled(T* __restrict__ e, const T* __restrict__ b, int64_t ld,
-                                                                int H, int W, const T* __restrict__ ec, int64_t ldc,
-                                                                int Hc, int Wc, T omega) {
-  using S = PostShape<SW>;
-  extern __shared__ __align__(16) unsigned char smem[];
-  T* base = reinterpret_cast<T*>(smem);
-  SplitTile<T> t;
-  t.e = base;
-  t.b = base + 2 * S::EY * S::EXh;
-  t.EXh = S::EXh;
-  t.EY = S::EY;
-  t.i0 = blockIdx.x * kTX - S::HALO;
-  t.j0 = blockIdx.y * kTY - S::HALO;
-  t.par0 = (t.i0 + t.j0) & 1;
-  t.H = H;
-  t.W = W;
-  const T w9 = (T)(9.0 / 16.0), w3 = (T)(3.0 / 16.0), w1_ = (T)(1.0 / 16.0);
-  for (int r = threadIdx.y; r < S::EY; r += kTBY) {
-    const int j = t.j0 + r;
-    const bool jin = j >= 0 && j < H;
-    const int J = j >> 1;
-    int Y = J + ((j & 1) ? 1 : -1);
-    Y = Y < 0 ? 0 : (Y > Hc - 1 ? Hc - 1 : Y);
-    const T* erow = e + (int64_t)j * ld;
-    const T* brow = b + (int64_t)j * ld;
-    const T* c0 = ec + (int64_t)J * ldc;
-    const T* c1 = ec + (int64_t)Y * ldc;
-    for (int c = threadIdx.x; c < S::EX; c += kTBX) {
-      const int i = t.i0 + c;
-      T ev = (T)0, bv = (T)0;
-      if (jin && i >= 0 && i < W) {
-        const int I = i >> 1;
-        int X = I + ((i & 1) ? 1 : -1);
-        X = X < 0 ? 0 : (X > Wc - 1 ? Wc - 1 : X);
-        T acc = (T)0;
-        acc += w9 * c0[I];
-        acc += w3 * c0[X];
-        acc += w3 * c1[I];
-        acc += w1_ * c1[X];
-        ev = erow[i] + acc;
-        bv = brow[i];
-      }
-      t.E(r, c) = ev;
-      t.B(r, c) = bv;
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int hs = 0; hs < 2 * SW; ++hs) {
-    const int ring = S::HALO - 1 - hs;
-    split_relax(t, hs & 1, S::HALO - ring, S::HALO + kTY + ring, S::HALO - ring, S::HALO + kTX + ring, omega);
-    __syncthreads();
-  }
-  split_store(t, e, ld, S::HALO);
-}
+#include "gmg_tiled.cuh"
 
 // ---------------------------------------------------------------- plan
 struct Level {
@@ -845,7 +605,8 @@ struct Level {
   int64_t ld = 0;              // row stride of the real arrays
   int analytic = 0;            // every cell fluid and every interior face open
   std::vector<uint8_t> code;   // H * W codes (host), empty when analytic
-  int64_t off_e = 0, off_b = 0, off_code = 0;
+  int fused = 0;               // this level and the next run the fused tiled kernels
+  int64_t off_e = 0, off_e2 = 0, off_b = 0, off_code = 0;  // e2: second e buffer (fused levels)
 };
 
 }  // namespace sg
@@ -1041,21 +802,17 @@ static int tail_launch(const sg_gmg_plan* p, bool zero_init, cudaStream_t s) {
 }
 
 // The fused tiled kernels serve open-box level pairs with 1..3 sweeps per side.
-static bool fused_level(const sg_gmg_plan* p, int k) {
-  const Level& L = p->levels[k];
-  const Level& C = p->levels[k + 1];
-  return L.analytic && C.analytic && L.H >= 2 && L.W >= 2 && p->pre >= 1 && p->pre <= 3 && p->post >= 1 &&
-         p->post <= 3;
-}
+static bool fused_level(const sg_gmg_plan* p, int k) { return p->levels[k].fused != 0; }
 
 template <typename T, int SW>
 static void launch_pre(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
   const Level& L = p->levels[k];
   const Level& C = p->levels[k + 1];
   dim3 g((L.W + kTX - 1) / kTX, (L.H + kTY - 1) / kTY);
+  // reads E0 (nothing for a zero initial guess), writes E1
   SG_LAUNCH(k_gmg_pre_tiled<T, SW><<<g, dim3(kTBX, kTBY), PreShape<SW>::template bytes<T>(), s>>>(
-      ws_ptr<T>(p, L.off_e), ws_ptr<T>(p, L.off_b), L.ld, L.H, L.W, ws_ptr<T>(p, C.off_b), C.ld, C.H, C.W,
-      (T)p->omega, zero_init ? 1 : 0));
+      zero_init ? nullptr : ws_ptr<T>(p, L.off_e), ws_ptr<T>(p, L.off_e2), ws_ptr<T>(p, L.off_b), L.ld, L.H, L.W,
+      ws_ptr<T>(p, C.off_b), C.ld, C.H, C.W, (T)p->omega));
 }
 
 template <typename T, int SW>
@@ -1063,9 +820,10 @@ static void launch_post(const sg_gmg_plan* p, int k, cudaStream_t s) {
   const Level& L = p->levels[k];
   const Level& C = p->levels[k + 1];
   dim3 g((L.W + kTX - 1) / kTX, (L.H + kTY - 1) / kTY);
+  // reads E1 and the coarse correction (the coarse level's E0), writes E0
   SG_LAUNCH(k_gmg_post_tiled<T, SW><<<g, dim3(kTBX, kTBY), PostShape<SW>::template bytes<T>(), s>>>(
-      ws_ptr<T>(p, L.off_e), ws_ptr<T>(p, L.off_b), L.ld, L.H, L.W, ws_ptr<T>(p, C.off_e), C.ld, C.H, C.W,
-      (T)p->omega));
+      ws_ptr<T>(p, L.off_e2), ws_ptr<T>(p, L.off_e), ws_ptr<T>(p, L.off_b), L.ld, L.H, L.W, ws_ptr<T>(p, C.off_e),
+      C.ld, C.H, C.W, (T)p->omega));
 }
 
 template <typename T>
@@ -1378,11 +1136,21 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
   // workspace layout
   size_t fine = precision == SG_GMG_FP32 ? sizeof(float) : sizeof(double);
   int64_t off = 0;
+  for (size_t k = 0; k + 1 < p->levels.size(); ++k) {
+    const Level& L = p->levels[k];
+    const Level& C = p->levels[k + 1];
+    p->levels[k].fused = (L.analytic && C.analytic && L.H >= 2 && L.W >= 2 && pre_sweeps >= 1 && pre_sweeps <= 3 &&
+                          post_sweeps >= 1 && post_sweeps <= 3)
+                             ? 1
+                             : 0;
+  }
   for (auto& L : p->levels) {
     L.ld = ((int64_t)L.W + 31) / 32 * 32;
     int64_t n = L.ld * L.H;
     L.off_e = off;
     off = align256(off + n * (int64_t)cyc);
+    L.off_e2 = off;
+    if (L.fused) off = align256(off + n * (int64_t)cyc);
     L.off_b = off;
     off = align256(off + n * (int64_t)cyc);
     L.off_code = off;
