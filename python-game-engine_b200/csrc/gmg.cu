@@ -804,41 +804,67 @@ static int tail_launch(const sg_gmg_plan* p, bool zero_init, cudaStream_t s) {
 // The fused tiled kernels serve open-box level pairs with 1..3 sweeps per side.
 static bool fused_level(const sg_gmg_plan* p, int k) { return p->levels[k].fused != 0; }
 
-template <typename T, int SW>
-static void launch_pre(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
+// Large tiles while a level fills the GPU with them (two blocks per SM), small tiles below:
+// a small level is latency-bound, and more blocks with less serial work each finish sooner.
+static bool small_tiles(const Level& L) {
+  const int64_t large_blocks = (int64_t)((L.W + kTX - 1) / kTX) * ((L.H + kTY - 1) / kTY);
+  return large_blocks < 2 * 148;
+}
+
+template <typename T, int SW, int TX, int TY>
+static void launch_pre_t(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
   const Level& L = p->levels[k];
   const Level& C = p->levels[k + 1];
-  dim3 g((L.W + kTX - 1) / kTX, (L.H + kTY - 1) / kTY);
+  dim3 g((L.W + TX - 1) / TX, (L.H + TY - 1) / TY);
   // reads E0 (nothing for a zero initial guess), writes E1
-  SG_LAUNCH(k_gmg_pre_tiled<T, SW><<<g, dim3(kTBX, kTBY), PreShape<SW>::template bytes<T>(), s>>>(
+  SG_LAUNCH(k_gmg_pre_tiled<T, SW, TX, TY><<<g, dim3(kTBX, kTBY), PreShape<SW, TX, TY>::template bytes<T>(), s>>>(
       zero_init ? nullptr : ws_ptr<T>(p, L.off_e), ws_ptr<T>(p, L.off_e2), ws_ptr<T>(p, L.off_b), L.ld, L.H, L.W,
       ws_ptr<T>(p, C.off_b), C.ld, C.H, C.W, (T)p->omega));
 }
 
-template <typename T, int SW>
-static void launch_post(const sg_gmg_plan* p, int k, cudaStream_t s) {
+template <typename T, int SW, int TX, int TY>
+static void launch_post_t(const sg_gmg_plan* p, int k, cudaStream_t s) {
   const Level& L = p->levels[k];
   const Level& C = p->levels[k + 1];
-  dim3 g((L.W + kTX - 1) / kTX, (L.H + kTY - 1) / kTY);
+  dim3 g((L.W + TX - 1) / TX, (L.H + TY - 1) / TY);
   // reads E1 and the coarse correction (the coarse level's E0), writes E0
-  SG_LAUNCH(k_gmg_post_tiled<T, SW><<<g, dim3(kTBX, kTBY), PostShape<SW>::template bytes<T>(), s>>>(
+  SG_LAUNCH(k_gmg_post_tiled<T, SW, TX, TY><<<g, dim3(kTBX, kTBY), PostShape<SW, TX, TY>::template bytes<T>(), s>>>(
       ws_ptr<T>(p, L.off_e2), ws_ptr<T>(p, L.off_e), ws_ptr<T>(p, L.off_b), L.ld, L.H, L.W, ws_ptr<T>(p, C.off_e),
       C.ld, C.H, C.W, (T)p->omega));
+}
+
+template <typename T, int SW>
+static void launch_pre(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
+  if (small_tiles(p->levels[k]))
+    launch_pre_t<T, SW, kSX, kSY>(p, k, zero_init, s);
+  else
+    launch_pre_t<T, SW, kTX, kTY>(p, k, zero_init, s);
+}
+
+template <typename T, int SW>
+static void launch_post(const sg_gmg_plan* p, int k, cudaStream_t s) {
+  if (small_tiles(p->levels[k]))
+    launch_post_t<T, SW, kSX, kSY>(p, k, s);
+  else
+    launch_post_t<T, SW, kTX, kTY>(p, k, s);
 }
 
 template <typename T>
 static int set_tiled_smem_limits() {
   cudaError_t e = cudaSuccess;
-#define SG_TILED_ATTR(SW)                                                                                          \
-  e = cudaFuncSetAttribute(k_gmg_pre_tiled<T, SW>, cudaFuncAttributeMaxDynamicSharedMemorySize,                    \
-                           (int)PreShape<SW>::template bytes<T>());                                                \
+#define SG_TILED_ATTR(SW, TX, TY)                                                                                  \
+  e = cudaFuncSetAttribute(k_gmg_pre_tiled<T, SW, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,            \
+                           (int)PreShape<SW, TX, TY>::template bytes<T>());                                        \
   if (e != cudaSuccess) return fail(SG_ERR_CUDA, "smem attr: %s", cudaGetErrorString(e));                          \
-  e = cudaFuncSetAttribute(k_gmg_post_tiled<T, SW>, cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
-                           (int)PostShape<SW>::template bytes<T>());                                               \
+  e = cudaFuncSetAttribute(k_gmg_post_tiled<T, SW, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,           \
+                           (int)PostShape<SW, TX, TY>::template bytes<T>());                                       \
   if (e != cudaSuccess) return fail(SG_ERR_CUDA, "smem attr: %s", cudaGetErrorString(e));
-  SG_TILED_ATTR(1)
-  SG_TILED_ATTR(2)
-  SG_TILED_ATTR(3)
+  SG_TILED_ATTR(1, kTX, kTY)
+  SG_TILED_ATTR(2, kTX, kTY)
+  SG_TILED_ATTR(3, kTX, kTY)
+  SG_TILED_ATTR(1, kSX, kSY)
+  SG_TILED_ATTR(2, kSX, kSY)
+  SG_TILED_ATTR(3, kSX, kSY)
 #undef SG_TILED_ATTR
   return SG_OK;
 }

@@ -2,7 +2,8 @@
 // namespace sg; uses w1 and rcp_open from there).
 //
 // For open-box levels (every cell fluid, every interior face open) one launch runs a whole
-// side of a cycle on a 64 x 32 tile of fine cells held in shared memory:
+// side of a cycle on a tile of fine cells held in shared memory (64 x 32 on large levels,
+// 16 x 16 on levels too small to fill the GPU with large tiles):
 //   pre:  SW red-black sweeps, the residual and its full-weighting restriction; reads e
 //         (not at all for a zero initial guess) and b once, writes e and the coarse rhs;
 //   post: bilinear prolongation of the coarse correction plus SW sweeps.
@@ -17,7 +18,8 @@
 // all but the outermost) take a path without bounds checks (every cell has 4 neighbours).
 #pragma once
 
-constexpr int kTX = 64, kTY = 32;   // fine cells of a tile
+constexpr int kTX = 64, kTY = 32;   // fine cells of a large-level tile
+constexpr int kSX = 16, kSY = 16;   // fine cells of a small-level tile (more blocks per level)
 constexpr int kTBX = 32, kTBY = 8;  // threads of a tile block
 constexpr int kTThreads = kTBX * kTBY;
 
@@ -36,11 +38,11 @@ struct SplitTile {
 __device__ __forceinline__ int tile_tid() { return threadIdx.y * kTBX + threadIdx.x; }
 
 // Relax the cells of colour col in the tile grown by RING rings (smem rows/cols
-// [HALO - RING, HALO + kT* + RING)); every neighbour is inside the loaded tile.
-template <typename T, bool INTERIOR, int HALO, int RING, int EXh>
+// [HALO - RING, HALO + TY|TX + RING)); every neighbour is inside the loaded tile.
+template <typename T, bool INTERIOR, int HALO, int RING, int EXh, int TX, int TY>
 __device__ __forceinline__ void relax_ring(const SplitTile<T>& t, int col, T omega) {
-  constexpr int RLO = HALO - RING, NR = kTY + 2 * RING;
-  constexpr int CLO = HALO - RING, CHI = HALO + kTX + RING;
+  constexpr int RLO = HALO - RING, NR = TY + 2 * RING;
+  constexpr int CLO = HALO - RING, CHI = HALO + TX + RING;
   constexpr int KW = (CHI - CLO + 1) / 2;  // cells of one colour per row, upper bound
   constexpr int N = NR * KW;
   T* E = t.ep(col);
@@ -74,12 +76,12 @@ __device__ __forceinline__ void relax_ring(const SplitTile<T>& t, int col, T ome
 }
 
 // Half sweeps HS .. NHS-1 (colour = HS & 1, ring HALO - 1 - HS).
-template <typename T, bool INTERIOR, int HALO, int EXh, int HS, int NHS>
+template <typename T, bool INTERIOR, int HALO, int EXh, int TX, int TY, int HS, int NHS>
 __device__ __forceinline__ void relax_all(const SplitTile<T>& t, T omega) {
   if constexpr (HS < NHS) {
-    relax_ring<T, INTERIOR, HALO, HALO - 1 - HS, EXh>(t, HS & 1, omega);
+    relax_ring<T, INTERIOR, HALO, HALO - 1 - HS, EXh, TX, TY>(t, HS & 1, omega);
     __syncthreads();
-    relax_all<T, INTERIOR, HALO, EXh, HS + 1, NHS>(t, omega);
+    relax_all<T, INTERIOR, HALO, EXh, TX, TY, HS + 1, NHS>(t, omega);
   }
 }
 
@@ -96,10 +98,10 @@ __device__ __forceinline__ void tile_load(const SplitTile<T>& t, const T* __rest
   }
 }
 
-template <typename T, bool INTERIOR, int HALO>
+template <typename T, bool INTERIOR, int HALO, int TX, int TY>
 __device__ __forceinline__ void tile_store(const SplitTile<T>& t, T* __restrict__ e, int64_t ld) {
-  for (int f = tile_tid(); f < kTX * kTY; f += kTThreads) {
-    const int rr = f / kTX, cc = f - rr * kTX;
+  for (int f = tile_tid(); f < TX * TY; f += kTThreads) {
+    const int rr = f / TX, cc = f - rr * TX;
     const int j = t.j0 + HALO + rr, i = t.i0 + HALO + cc;
     if (INTERIOR || (j < t.H && i < t.W)) e[(int64_t)j * ld + i] = t.E(HALO + rr, HALO + cc);
   }
@@ -119,24 +121,24 @@ __device__ __forceinline__ T tile_residual(const SplitTile<T>& t, int r, int c) 
   return acc;
 }
 
-template <int SW>
+template <int SW, int TX, int TY>
 struct PreShape {
   static constexpr int HALO = 2 * SW + 2;  // 2SW half sweeps + residual ring + restriction window
-  static constexpr int EX = kTX + 2 * HALO, EY = kTY + 2 * HALO, EXh = EX / 2;
-  static constexpr int XR = kTY + 2, XC = kTX / 2;
+  static constexpr int EX = TX + 2 * HALO, EY = TY + 2 * HALO, EXh = EX / 2;
+  static constexpr int XR = TY + 2, XC = TX / 2;
   template <typename T>
   static constexpr size_t bytes() { return (size_t)(4 * EY * EXh + XR * XC) * sizeof(T); }
 };
 
-template <int SW>
+template <int SW, int TX, int TY>
 struct PostShape {
   static constexpr int HALO = 2 * SW;
-  static constexpr int EX = kTX + 2 * HALO, EY = kTY + 2 * HALO, EXh = EX / 2;
+  static constexpr int EX = TX + 2 * HALO, EY = TY + 2 * HALO, EXh = EX / 2;
   template <typename T>
   static constexpr size_t bytes() { return (size_t)(4 * EY * EXh) * sizeof(T); }
 };
 
-template <typename T, int SW>
+template <typename T, int TX, int TY>
 __device__ __forceinline__ SplitTile<T> make_tile(unsigned char* smem, int halo, int EXh, int EY, int H, int W) {
   SplitTile<T> t;
   T* base = reinterpret_cast<T*>(smem);
@@ -144,24 +146,24 @@ __device__ __forceinline__ SplitTile<T> make_tile(unsigned char* smem, int halo,
   t.b = base + 2 * EY * EXh;
   t.EXh = EXh;
   t.EY = EY;
-  t.i0 = blockIdx.x * kTX - halo;
-  t.j0 = blockIdx.y * kTY - halo;
+  t.i0 = blockIdx.x * TX - halo;
+  t.j0 = blockIdx.y * TY - halo;
   t.par0 = (t.i0 + t.j0) & 1;
   t.H = H;
   t.W = W;
   return t;
 }
 
-template <typename T, int SW, bool INTERIOR>
+template <typename T, int SW, int TX, int TY, bool INTERIOR>
 __device__ __forceinline__ void pre_body(const SplitTile<T>& t, const T* __restrict__ e_in, T* __restrict__ e_out,
                                          const T* __restrict__ b, int64_t ld, T* __restrict__ bc, int64_t ldc, int Hc,
                                          int Wc, T omega, T* X) {
-  using S = PreShape<SW>;
+  using S = PreShape<SW, TX, TY>;
   tile_load<T, INTERIOR, S::EX, S::EY>(t, e_in, b, ld);
   __syncthreads();
-  relax_all<T, INTERIOR, S::HALO, S::EXh, 0, 2 * SW>(t, omega);
+  relax_all<T, INTERIOR, S::HALO, S::EXh, TX, TY, 0, 2 * SW>(t, omega);
   // residual on the tile plus one ring, in place of b (each cell reads only its own b)
-  constexpr int RW = kTX + 2, RH = kTY + 2, LO = S::HALO - 1;
+  constexpr int RW = TX + 2, RH = TY + 2, LO = S::HALO - 1;
   for (int f = tile_tid(); f < RW * RH; f += kTThreads) {
     const int rr = f / RW, cc = f - rr * RW;
     const T res = tile_residual<T, INTERIOR>(t, LO + rr, LO + cc);
@@ -169,25 +171,27 @@ __device__ __forceinline__ void pre_body(const SplitTile<T>& t, const T* __restr
   }
   __syncthreads();
   // full weighting along x: X[rr][I'] over fine rows of the tile plus one ring
-  const int Ip = threadIdx.x, I = blockIdx.x * (kTX / 2) + Ip;
   const int H = t.H, W = t.W;
-  T wx[4];
-#pragma unroll
-  for (int d = 0; d < 4; ++d) {
-    const int i = 2 * I - 1 + d;
-    wx[d] = (i >= 0 && i < W && I < Wc) ? (T)w1(i, I, Wc) : (T)0;
-  }
-  for (int rr = threadIdx.y; rr < S::XR; rr += kTBY) {
+  for (int f = tile_tid(); f < S::XR * S::XC; f += kTThreads) {
+    const int rr = f / S::XC, Ip = f - rr * S::XC;
+    const int I = blockIdx.x * S::XC + Ip;
     T acc = (T)0;
+    if (I < Wc) {
 #pragma unroll
-    for (int d = 0; d < 4; ++d)
-      if (wx[d] != (T)0) acc += wx[d] * t.B(LO + rr, 2 * Ip + LO + d);
-    X[rr * S::XC + Ip] = acc;
+      for (int d = 0; d < 4; ++d) {
+        const int i = 2 * I - 1 + d;
+        if (i < 0 || i >= W) continue;
+        const T w = (T)w1(i, I, Wc);
+        if (w != (T)0) acc += w * t.B(LO + rr, 2 * Ip + LO + d);
+      }
+    }
+    X[f] = acc;
   }
   __syncthreads();
   // along y
-  for (int Jp = threadIdx.y; Jp < kTY / 2; Jp += kTBY) {
-    const int J = blockIdx.y * (kTY / 2) + Jp;
+  for (int f = tile_tid(); f < (TY / 2) * S::XC; f += kTThreads) {
+    const int Jp = f / S::XC, Ip = f - Jp * S::XC;
+    const int J = blockIdx.y * (TY / 2) + Jp, I = blockIdx.x * S::XC + Ip;
     if (J >= Hc || I >= Wc) continue;
     T acc = (T)0;
 #pragma unroll
@@ -199,31 +203,31 @@ __device__ __forceinline__ void pre_body(const SplitTile<T>& t, const T* __restr
     }
     bc[(int64_t)J * ldc + I] = acc;
   }
-  tile_store<T, INTERIOR, S::HALO>(t, e_out, ld);
+  tile_store<T, INTERIOR, S::HALO, TX, TY>(t, e_out, ld);
 }
 
 // pre: SW sweeps from e_in (NULL: zero initial guess) + residual + full weighting into
-// bc (coarse tile 32 x 16); the smoothed tile goes to e_out.
-template <typename T, int SW>
+// bc (coarse tile TX/2 x TY/2); the smoothed tile goes to e_out.
+template <typename T, int SW, int TX, int TY>
 __global__ void __launch_bounds__(kTThreads) k_gmg_pre_tiled(const T* __restrict__ e_in, T* __restrict__ e_out,
                                                              const T* __restrict__ b, int64_t ld, int H, int W,
                                                              T* __restrict__ bc, int64_t ldc, int Hc, int Wc, T omega) {
-  using S = PreShape<SW>;
+  using S = PreShape<SW, TX, TY>;
   extern __shared__ __align__(16) unsigned char smem[];
-  SplitTile<T> t = make_tile<T, SW>(smem, S::HALO, S::EXh, S::EY, H, W);
+  SplitTile<T> t = make_tile<T, TX, TY>(smem, S::HALO, S::EXh, S::EY, H, W);
   T* X = reinterpret_cast<T*>(smem) + 4 * S::EY * S::EXh;
   const bool interior = t.i0 >= 0 && t.i0 + S::EX <= W && t.j0 >= 0 && t.j0 + S::EY <= H;
   if (interior)
-    pre_body<T, SW, true>(t, e_in, e_out, b, ld, bc, ldc, Hc, Wc, omega, X);
+    pre_body<T, SW, TX, TY, true>(t, e_in, e_out, b, ld, bc, ldc, Hc, Wc, omega, X);
   else
-    pre_body<T, SW, false>(t, e_in, e_out, b, ld, bc, ldc, Hc, Wc, omega, X);
+    pre_body<T, SW, TX, TY, false>(t, e_in, e_out, b, ld, bc, ldc, Hc, Wc, omega, X);
 }
 
-template <typename T, int SW, bool INTERIOR>
+template <typename T, int SW, int TX, int TY, bool INTERIOR>
 __device__ __forceinline__ void post_body(const SplitTile<T>& t, const T* __restrict__ e_in, T* __restrict__ e_out,
                                           const T* __restrict__ b, int64_t ld, const T* __restrict__ ec, int64_t ldc,
                                           int Hc, int Wc, T omega) {
-  using S = PostShape<SW>;
+  using S = PostShape<SW, TX, TY>;
   const T w9 = (T)(9.0 / 16.0), w3 = (T)(3.0 / 16.0), wd = (T)(1.0 / 16.0);
   for (int f = tile_tid(); f < S::EX * S::EY; f += kTThreads) {
     const int r = f / S::EX, c = f - r * S::EX;
@@ -249,22 +253,22 @@ __device__ __forceinline__ void post_body(const SplitTile<T>& t, const T* __rest
     t.B(r, c) = bv;
   }
   __syncthreads();
-  relax_all<T, INTERIOR, S::HALO, S::EXh, 0, 2 * SW>(t, omega);
-  tile_store<T, INTERIOR, S::HALO>(t, e_out, ld);
+  relax_all<T, INTERIOR, S::HALO, S::EXh, TX, TY, 0, 2 * SW>(t, omega);
+  tile_store<T, INTERIOR, S::HALO, TX, TY>(t, e_out, ld);
 }
 
 // post: e_out = smoothed (e_in + P ec).
-template <typename T, int SW>
+template <typename T, int SW, int TX, int TY>
 __global__ void __launch_bounds__(kTThreads) k_gmg_post_tiled(const T* __restrict__ e_in, T* __restrict__ e_out,
                                                               const T* __restrict__ b, int64_t ld, int H, int W,
                                                               const T* __restrict__ ec, int64_t ldc, int Hc, int Wc,
                                                               T omega) {
-  using S = PostShape<SW>;
+  using S = PostShape<SW, TX, TY>;
   extern __shared__ __align__(16) unsigned char smem[];
-  SplitTile<T> t = make_tile<T, SW>(smem, S::HALO, S::EXh, S::EY, H, W);
+  SplitTile<T> t = make_tile<T, TX, TY>(smem, S::HALO, S::EXh, S::EY, H, W);
   const bool interior = t.i0 >= 0 && t.i0 + S::EX <= W && t.j0 >= 0 && t.j0 + S::EY <= H;
   if (interior)
-    post_body<T, SW, true>(t, e_in, e_out, b, ld, ec, ldc, Hc, Wc, omega);
+    post_body<T, SW, TX, TY, true>(t, e_in, e_out, b, ld, ec, ldc, Hc, Wc, omega);
   else
-    post_body<T, SW, false>(t, e_in, e_out, b, ld, ec, ldc, Hc, Wc, omega);
+    post_body<T, SW, TX, TY, false>(t, e_in, e_out, b, ld, ec, ldc, Hc, Wc, omega);
 }
