@@ -598,6 +598,7 @@ __global__ void __launch_bounds__(kRX * kRY) k_gmg_residual_restrict_tiled(const
 
 // ---------------------------------------------------------------- fused tiled level kernels
 #include "gmg_tiled.cuh"
+#include "gmg_regtile.cuh"
 
 // ---------------------------------------------------------------- plan
 struct Level {
@@ -834,11 +835,36 @@ static void launch_post_t(const sg_gmg_plan* p, int k, cudaStream_t s) {
 }
 
 template <typename T, int SW>
+static void launch_pre_reg(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
+  constexpr int RPT = RegShape<T>::RPT, NW = RegShape<T>::NWARP;
+  using S = RegPre<T, SW, RPT, NW>;
+  const Level& L = p->levels[k];
+  const Level& C = p->levels[k + 1];
+  dim3 g((L.W + S::TXO - 1) / S::TXO, (L.H + S::TYO - 1) / S::TYO);
+  SG_LAUNCH(k_gmg_pre_reg<T, SW, RPT, NW><<<g, 32 * NW, 0, s>>>(
+      zero_init ? nullptr : ws_ptr<T>(p, L.off_e), ws_ptr<T>(p, L.off_e2), ws_ptr<T>(p, L.off_b), L.ld, L.H, L.W,
+      ws_ptr<T>(p, C.off_b), C.ld, C.H, C.W, (T)p->omega));
+}
+
+template <typename T, int SW>
+static void launch_post_reg(const sg_gmg_plan* p, int k, cudaStream_t s) {
+  constexpr int RPT = RegShape<T>::RPT, NW = RegShape<T>::NWARP;
+  using S = RegPost<T, SW, RPT, NW>;
+  const Level& L = p->levels[k];
+  const Level& C = p->levels[k + 1];
+  dim3 g((L.W + S::TXO - 1) / S::TXO, (L.H + S::TYO - 1) / S::TYO);
+  SG_LAUNCH(k_gmg_post_reg<T, SW, RPT, NW><<<g, 32 * NW, 0, s>>>(
+      ws_ptr<T>(p, L.off_e2), ws_ptr<T>(p, L.off_e), ws_ptr<T>(p, L.off_b), L.ld, L.H, L.W, ws_ptr<T>(p, C.off_e),
+      C.ld, C.H, C.W, (T)p->omega));
+}
+
+// Large levels: register tiles; small levels: 16 x 16 shared-memory tiles.
+template <typename T, int SW>
 static void launch_pre(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
   if (small_tiles(p->levels[k]))
     launch_pre_t<T, SW, kSX, kSY>(p, k, zero_init, s);
   else
-    launch_pre_t<T, SW, kTX, kTY>(p, k, zero_init, s);
+    launch_pre_reg<T, SW>(p, k, zero_init, s);
 }
 
 template <typename T, int SW>
@@ -846,7 +872,7 @@ static void launch_post(const sg_gmg_plan* p, int k, cudaStream_t s) {
   if (small_tiles(p->levels[k]))
     launch_post_t<T, SW, kSX, kSY>(p, k, s);
   else
-    launch_post_t<T, SW, kTX, kTY>(p, k, s);
+    launch_post_reg<T, SW>(p, k, s);
 }
 
 template <typename T>

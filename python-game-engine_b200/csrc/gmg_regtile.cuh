@@ -1,0 +1,391 @@
+// Register-tiled level kernels of the convergent multigrid for large open-box levels
+// (included by gmg.cu inside namespace sg; uses w1 and rcp_open from there).
+//
+// Same two launches per level and cycle as the shared-memory tiles (pre: sweeps + residual
+// + full weighting; post: prolongation + sweeps), but the cells stay in registers:
+//   - a block is NWARP warps stacked vertically over a 64-column tile; lane l owns columns
+//     i0 + 2l, i0 + 2l + 1 and warp w owns rows j0 + w RPT .. j0 + w RPT + RPT - 1;
+//   - horizontal neighbours come from the adjacent lane by warp shuffles, vertical ones from
+//     the thread's own registers, except the first and last row of a warp, which are
+//     exchanged through shared memory once per half sweep (one barrier, double-buffered);
+//   - the tile origin (i0, j0) is even, so the colour of a register cell, (r + q) & 1, is
+//     known at compile time and every half sweep is straight-line code.
+// The tile carries a halo (pre: 2 SW + 2 cells, post: 2 SW) that absorbs the wrong values
+// grown from its edge, one cell per half sweep, so every cell a block writes holds exactly
+// what grid-wide half sweeps give. Blocks read e from one buffer and write another (pre:
+// E0 or nothing -> E1, post: E1 -> E0), so no block reads cells another one is writing.
+// Tiles whose cells all lie inside the grid take a path without bounds checks; on the
+// others, cells outside the grid hold 0 and are never updated, so the relaxation sum is
+// unchanged and only the neighbour count (and the residual's terms) need the bounds.
+#pragma once
+
+constexpr int kRW = 64;  // tile columns: 32 lanes x 2
+
+template <typename T>
+struct Pair;
+template <>
+struct Pair<float> {
+  using V = float2;
+};
+template <>
+struct Pair<double> {
+  using V = double2;
+};
+
+template <typename T>
+__device__ __forceinline__ T shfl_up1(T v) {
+  return __shfl_up_sync(0xffffffffu, v, 1);
+}
+template <typename T>
+__device__ __forceinline__ T shfl_down1(T v) {
+  return __shfl_down_sync(0xffffffffu, v, 1);
+}
+
+// Shared-memory exchange of the first and last row of each warp (double-buffered).
+template <typename T, int NWARP>
+struct RegXchg {
+  typename Pair<T>::V top[2][NWARP][32];
+  typename Pair<T>::V bot[2][NWARP][32];
+  T xtop[NWARP][32];
+  T xbot[NWARP][32];
+};
+
+// Publish the warp's edge rows into buffer buf, wait, and fetch the neighbouring warps'
+// edges: above = row w RPT - 1 (last row of warp w - 1), below = row (w + 1) RPT (first row
+// of warp w + 1). The outermost warps get their own rows back (halo cells, never used).
+template <typename T, int RPT, int NWARP>
+__device__ __forceinline__ void exchange_rows(RegXchg<T, NWARP>& x, int buf, const T (&e)[RPT][2], int w, int lane,
+                                              T (&above)[2], T (&below)[2]) {
+  using V = typename Pair<T>::V;
+  V t, bo;
+  t.x = e[0][0];
+  t.y = e[0][1];
+  bo.x = e[RPT - 1][0];
+  bo.y = e[RPT - 1][1];
+  x.top[buf][w][lane] = t;
+  x.bot[buf][w][lane] = bo;
+  __syncthreads();
+  const V a = x.bot[buf][w > 0 ? w - 1 : w][lane];
+  const V b = x.top[buf][w < NWARP - 1 ? w + 1 : w][lane];
+  above[0] = a.x;
+  above[1] = a.y;
+  below[0] = b.x;
+  below[1] = b.y;
+}
+
+// One half sweep of colour COL over the thread's cells. Row r, column q has colour
+// (r + q) & 1. BOUNDED: tile touches the grid edge; (j, i) of the thread's first cell.
+template <typename T, int RPT, int COL, bool BOUNDED>
+__device__ __forceinline__ void reg_half_sweep(T (&e)[RPT][2], const T (&b)[RPT][2], const T (&above)[2],
+                                               const T (&below)[2], T omega, int j, int i, int H, int W) {
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) {
+    const int q = (COL + r) & 1;
+    // the neighbour in the other lane: q = 0 needs column 2l - 1 (lane l - 1's column 1),
+    // q = 1 needs column 2l + 2 (lane l + 1's column 0)
+    const T far = q == 0 ? shfl_up1(e[r][1]) : shfl_down1(e[r][0]);
+    const T left = q == 0 ? far : e[r][0];
+    const T right = q == 0 ? e[r][1] : far;
+    const T up = r > 0 ? e[r > 0 ? r - 1 : 0][q] : above[q];
+    const T down = r < RPT - 1 ? e[r < RPT - 1 ? r + 1 : 0][q] : below[q];
+    const T acc = b[r][q] + left + right + up + down;
+    const T x = e[r][q];
+    if (!BOUNDED) {
+      e[r][q] = x + omega * (acc * (T)0.25 - x);
+    } else {
+      const int jj = j + r, ii = i + q;
+      if (jj >= 0 && jj < H && ii >= 0 && ii < W) {
+        const int n = (ii > 0) + (ii < W - 1) + (jj > 0) + (jj < H - 1);
+        if (n > 0) e[r][q] = x + omega * (acc * rcp_open<T>(n) - x);
+      }
+    }
+  }
+}
+
+template <typename T, int RPT, int NWARP, int NHS, int HS, bool BOUNDED>
+__device__ __forceinline__ void reg_sweeps(RegXchg<T, NWARP>& x, T (&e)[RPT][2], const T (&b)[RPT][2], T omega,
+                                           int w, int lane, int j, int i, int H, int W) {
+  if constexpr (HS < NHS) {
+    T above[2], below[2];
+    exchange_rows<T, RPT, NWARP>(x, HS & 1, e, w, lane, above, below);
+    reg_half_sweep<T, RPT, HS & 1, BOUNDED>(e, b, above, below, omega, j, i, H, W);
+    reg_sweeps<T, RPT, NWARP, NHS, HS + 1, BOUNDED>(x, e, b, omega, w, lane, j, i, H, W);
+  }
+}
+
+// Load RPT x 2 cells at (j, i) (i even) from a level array; cells outside the grid get 0.
+template <typename T, int RPT, bool BOUNDED>
+__device__ __forceinline__ void reg_load(T (&v)[RPT][2], const T* __restrict__ a, int64_t ld, int j, int i, int H,
+                                         int W) {
+  using V = typename Pair<T>::V;
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) {
+    const int jj = j + r;
+    if (!BOUNDED) {
+      const V t = *reinterpret_cast<const V*>(a + (int64_t)jj * ld + i);
+      v[r][0] = t.x;
+      v[r][1] = t.y;
+    } else {
+      const bool row = jj >= 0 && jj < H;
+      v[r][0] = (row && i >= 0 && i < W) ? a[(int64_t)jj * ld + i] : (T)0;
+      v[r][1] = (row && i + 1 >= 0 && i + 1 < W) ? a[(int64_t)jj * ld + i + 1] : (T)0;
+    }
+  }
+}
+
+// Store the owned cells (rows [r_lo, r_hi) of the thread's RPT, both columns when owned).
+template <typename T, int RPT, bool BOUNDED>
+__device__ __forceinline__ void reg_store(const T (&v)[RPT][2], T* __restrict__ a, int64_t ld, int j, int i, int H,
+                                          int W, bool cols_owned, int r_lo, int r_hi) {
+  using V = typename Pair<T>::V;
+  if (!cols_owned) return;
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) {
+    if (r < r_lo || r >= r_hi) continue;
+    const int jj = j + r;
+    if (!BOUNDED) {
+      V t;
+      t.x = v[r][0];
+      t.y = v[r][1];
+      *reinterpret_cast<V*>(a + (int64_t)jj * ld + i) = t;
+    } else {
+      if (jj >= H) continue;
+      if (i < W) a[(int64_t)jj * ld + i] = v[r][0];
+      if (i + 1 < W) a[(int64_t)jj * ld + i + 1] = v[r][1];
+    }
+  }
+}
+
+template <typename T, int SW, int RPT, int NWARP>
+struct RegPre {
+  static constexpr int HALO = 2 * SW + 2;
+  static constexpr int TXO = kRW - 2 * HALO;          // owned columns
+  static constexpr int TYO = NWARP * RPT - 2 * HALO;  // owned rows
+  static_assert(RPT % 2 == 0 && TYO > 0 && TXO > 0, "bad register tile");
+};
+
+template <typename T, int SW, int RPT, int NWARP>
+struct RegPost {
+  static constexpr int HALO = 2 * SW;
+  static constexpr int TXO = kRW - 2 * HALO;
+  static constexpr int TYO = NWARP * RPT - 2 * HALO;
+  static_assert(RPT % 2 == 0 && TYO > 0 && TXO > 0, "bad register tile");
+};
+
+template <typename T, int SW, int RPT, int NWARP, bool BOUNDED>
+__device__ __forceinline__ void reg_pre_body(RegXchg<T, NWARP>& x, const T* __restrict__ e_in, T* __restrict__ e_out,
+                                             const T* __restrict__ bsrc, int64_t ld, int H, int W, T* __restrict__ bc,
+                                             int64_t ldc, int Hc, int Wc, T omega, int i0, int j0) {
+  using S = RegPre<T, SW, RPT, NWARP>;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = i0 + 2 * lane, j = j0 + w * RPT;
+  T e[RPT][2], b[RPT][2];
+  reg_load<T, RPT, BOUNDED>(b, bsrc, ld, j, i, H, W);
+  if (e_in) {
+    reg_load<T, RPT, BOUNDED>(e, e_in, ld, j, i, H, W);
+  } else {
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) e[r][0] = e[r][1] = (T)0;
+  }
+  reg_sweeps<T, RPT, NWARP, 2 * SW, 0, BOUNDED>(x, e, b, omega, w, lane, j, i, H, W);
+  // residual b - A e in place of b
+  T above[2], below[2];
+  exchange_rows<T, RPT, NWARP>(x, (2 * SW) & 1, e, w, lane, above, below);
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) {
+    const T l1 = shfl_up1(e[r][1]);
+    const T r0 = shfl_down1(e[r][0]);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const T xv = e[r][q];
+      const T left = q == 0 ? l1 : e[r][0];
+      const T right = q == 0 ? e[r][1] : r0;
+      const T up = r > 0 ? e[r > 0 ? r - 1 : 0][q] : above[q];
+      const T down = r < RPT - 1 ? e[r < RPT - 1 ? r + 1 : 0][q] : below[q];
+      if (!BOUNDED) {
+        b[r][q] = b[r][q] + (left - xv) + (right - xv) + (up - xv) + (down - xv);
+      } else {
+        const int jj = j + r, ii = i + q;
+        T acc = (T)0;
+        if (jj >= 0 && jj < H && ii >= 0 && ii < W) {
+          acc = b[r][q];
+          if (ii > 0) acc += left - xv;
+          if (ii < W - 1) acc += right - xv;
+          if (jj > 0) acc += up - xv;
+          if (jj < H - 1) acc += down - xv;
+        }
+        b[r][q] = acc;
+      }
+    }
+  }
+  // full weighting along x: coarse column I = i0 / 2 + lane from fine columns 2I - 1 .. 2I + 2
+  const int I = (i0 >> 1) + lane;
+  T wx0 = (T)0.25, wx1 = (T)0.75, wx2 = (T)0.75, wx3 = (T)0.25;
+  if (BOUNDED) {
+    wx0 = (2 * I - 1 >= 0 && 2 * I - 1 < W) ? (T)w1(2 * I - 1, I, Wc) : (T)0;
+    wx1 = (2 * I < W) ? (T)w1(2 * I, I, Wc) : (T)0;
+    wx2 = (2 * I + 1 < W) ? (T)w1(2 * I + 1, I, Wc) : (T)0;
+    wx3 = (2 * I + 2 < W) ? (T)w1(2 * I + 2, I, Wc) : (T)0;
+  }
+  T X[RPT];
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) {
+    const T rl = shfl_up1(b[r][1]);
+    const T rr = shfl_down1(b[r][0]);
+    T acc = (T)0;
+    acc += wx0 * rl;
+    acc += wx1 * b[r][0];
+    acc += wx2 * b[r][1];
+    acc += wx3 * rr;
+    X[r] = acc;
+  }
+  x.xtop[w][lane] = X[0];
+  x.xbot[w][lane] = X[RPT - 1];
+  __syncthreads();
+  const T xa = x.xbot[w > 0 ? w - 1 : w][lane];
+  const T xb = x.xtop[w < NWARP - 1 ? w + 1 : w][lane];
+  // along y: coarse row J = j / 2 + m from X rows 2m - 1 .. 2m + 2
+  const bool cols_owned = 2 * lane >= S::HALO && 2 * lane < S::HALO + S::TXO && I < Wc;
+  if (cols_owned) {
+#pragma unroll
+    for (int m = 0; m < RPT / 2; ++m) {
+      const int rt = w * RPT + 2 * m;  // tile row of fine row 2J
+      if (rt < S::HALO || rt >= S::HALO + S::TYO) continue;
+      const int J = (j >> 1) + m;
+      if (J >= Hc) continue;
+      const T x0 = m > 0 ? X[m > 0 ? 2 * m - 1 : 0] : xa;
+      const T x3 = 2 * m + 2 < RPT ? X[2 * m + 2 < RPT ? 2 * m + 2 : 0] : xb;
+      T wy0 = (T)0.25, wy1 = (T)0.75, wy2 = (T)0.75, wy3 = (T)0.25;
+      if (BOUNDED) {
+        wy0 = (2 * J - 1 >= 0 && 2 * J - 1 < H) ? (T)w1(2 * J - 1, J, Hc) : (T)0;
+        wy1 = (2 * J < H) ? (T)w1(2 * J, J, Hc) : (T)0;
+        wy2 = (2 * J + 1 < H) ? (T)w1(2 * J + 1, J, Hc) : (T)0;
+        wy3 = (2 * J + 2 < H) ? (T)w1(2 * J + 2, J, Hc) : (T)0;
+      }
+      T acc = (T)0;
+      acc += wy0 * x0;
+      acc += wy1 * X[2 * m];
+      acc += wy2 * X[2 * m + 1];
+      acc += wy3 * x3;
+      bc[(int64_t)J * ldc + I] = acc;
+    }
+  }
+  const int r_lo = S::HALO - w * RPT, r_hi = S::HALO + S::TYO - w * RPT;
+  reg_store<T, RPT, BOUNDED>(e, e_out, ld, j, i, H, W, 2 * lane >= S::HALO && 2 * lane < S::HALO + S::TXO, r_lo,
+                             r_hi);
+}
+
+// pre: SW sweeps from e_in (NULL: zero initial guess), residual and its full weighting
+// into bc; the smoothed cells go to e_out.
+template <typename T, int SW, int RPT, int NWARP>
+__global__ void __launch_bounds__(32 * NWARP) k_gmg_pre_reg(const T* __restrict__ e_in, T* __restrict__ e_out,
+                                                           const T* __restrict__ b, int64_t ld, int H, int W,
+                                                           T* __restrict__ bc, int64_t ldc, int Hc, int Wc, T omega) {
+  using S = RegPre<T, SW, RPT, NWARP>;
+  __shared__ RegXchg<T, NWARP> x;
+  const int i0 = blockIdx.x * S::TXO - S::HALO;
+  const int j0 = blockIdx.y * S::TYO - S::HALO;
+  const bool inside = i0 >= 0 && i0 + kRW <= W && j0 >= 0 && j0 + NWARP * RPT <= H;
+  if (inside)
+    reg_pre_body<T, SW, RPT, NWARP, false>(x, e_in, e_out, b, ld, H, W, bc, ldc, Hc, Wc, omega, i0, j0);
+  else
+    reg_pre_body<T, SW, RPT, NWARP, true>(x, e_in, e_out, b, ld, H, W, bc, ldc, Hc, Wc, omega, i0, j0);
+}
+
+template <typename T, int SW, int RPT, int NWARP, bool BOUNDED>
+__device__ __forceinline__ void reg_post_body(RegXchg<T, NWARP>& x, const T* __restrict__ e_in, T* __restrict__ e_out,
+                                              const T* __restrict__ bsrc, int64_t ld, int H, int W,
+                                              const T* __restrict__ ec, int64_t ldc, int Hc, int Wc, T omega, int i0,
+                                              int j0) {
+  using S = RegPost<T, SW, RPT, NWARP>;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = i0 + 2 * lane, j = j0 + w * RPT;
+  T e[RPT][2], b[RPT][2];
+  reg_load<T, RPT, BOUNDED>(b, bsrc, ld, j, i, H, W);
+  reg_load<T, RPT, BOUNDED>(e, e_in, ld, j, i, H, W);
+  // bilinear prolongation: fine (j, i) from coarse (J, I), (J, X), (Y, I), (Y, X) with
+  // X = I -+ 1 for even / odd i and Y = J -+ 1 for even / odd j, both clamped to the level.
+  // Every tile cell needs its exact start value (the sweeps only absorb wrong neighbours),
+  // so the edge lanes load their outer coarse column instead of shuffling it in; with I
+  // clamped on every lane, the shuffled neighbours are the clamped ones as well.
+  const T w9 = (T)(9.0 / 16.0), w3 = (T)(3.0 / 16.0), wd = (T)(1.0 / 16.0);
+  const int I = (i0 >> 1) + lane;
+  const int Ic = I < 0 ? 0 : (I > Wc - 1 ? Wc - 1 : I);
+  const int Iedge = lane == 0 ? (I - 1 < 0 ? 0 : (I - 1 > Wc - 1 ? Wc - 1 : I - 1))
+                              : (I + 1 < 0 ? 0 : (I + 1 > Wc - 1 ? Wc - 1 : I + 1));
+  const bool edge = lane == 0 || lane == 31;
+  const int Jb = j >> 1;  // coarse row of the thread's first fine row (j even)
+  auto fetch = [&](int J, T& cl, T& cm, T& cr) {
+    const int Jc = J < 0 ? 0 : (J > Hc - 1 ? Hc - 1 : J);
+    const T* row = ec + (int64_t)Jc * ldc;
+    const T v = row[Ic];
+    const T ve = edge ? row[Iedge] : (T)0;
+    const T lv = shfl_up1(v), rv = shfl_down1(v);
+    cl = lane == 0 ? ve : lv;
+    cm = v;
+    cr = lane == 31 ? ve : rv;
+  };
+  T pl, pm, pr, cl, cm, cr;  // coarse rows Jb + m - 1 and Jb + m at columns I - 1, I, I + 1
+  fetch(Jb - 1, pl, pm, pr);
+  fetch(Jb, cl, cm, cr);
+#pragma unroll
+  for (int m = 0; m < RPT / 2; ++m) {
+    T nl, nm, nr;
+    fetch(Jb + m + 1, nl, nm, nr);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = 2 * m + h;
+      // fine row 2J (even): Y = J - 1; fine row 2J + 1 (odd): Y = J + 1
+      const T yl = h == 0 ? pl : nl, ym = h == 0 ? pm : nm, yr = h == 0 ? pr : nr;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        T acc = (T)0;
+        acc += w9 * cm;
+        acc += w3 * (q == 0 ? cl : cr);
+        acc += w3 * ym;
+        acc += wd * (q == 0 ? yl : yr);
+        if (!BOUNDED || (j + r >= 0 && j + r < H && i + q >= 0 && i + q < W)) e[r][q] = e[r][q] + acc;
+      }
+    }
+    pl = cl;
+    pm = cm;
+    pr = cr;
+    cl = nl;
+    cm = nm;
+    cr = nr;
+  }
+  reg_sweeps<T, RPT, NWARP, 2 * SW, 0, BOUNDED>(x, e, b, omega, w, lane, j, i, H, W);
+  const int r_lo = S::HALO - w * RPT, r_hi = S::HALO + S::TYO - w * RPT;
+  reg_store<T, RPT, BOUNDED>(e, e_out, ld, j, i, H, W, 2 * lane >= S::HALO && 2 * lane < S::HALO + S::TXO, r_lo,
+                             r_hi);
+}
+
+// post: e_out = smoothed (e_in + P ec).
+template <typename T, int SW, int RPT, int NWARP>
+__global__ void __launch_bounds__(32 * NWARP) k_gmg_post_reg(const T* __restrict__ e_in, T* __restrict__ e_out,
+                                                            const T* __restrict__ b, int64_t ld, int H, int W,
+                                                            const T* __restrict__ ec, int64_t ldc, int Hc, int Wc,
+                                                            T omega) {
+  using S = RegPost<T, SW, RPT, NWARP>;
+  __shared__ RegXchg<T, NWARP> x;
+  const int i0 = blockIdx.x * S::TXO - S::HALO;
+  const int j0 = blockIdx.y * S::TYO - S::HALO;
+  const bool inside = i0 >= 0 && i0 + kRW <= W && j0 >= 0 && j0 + NWARP * RPT <= H;
+  if (inside)
+    reg_post_body<T, SW, RPT, NWARP, false>(x, e_in, e_out, b, ld, H, W, ec, ldc, Hc, Wc, omega, i0, j0);
+  else
+    reg_post_body<T, SW, RPT, NWARP, true>(x, e_in, e_out, b, ld, H, W, ec, ldc, Hc, Wc, omega, i0, j0);
+}
+
+// Rows per thread and warps per block of the register tiles: FP32 keeps 12 rows of e and b
+// per thread (about 70 registers, three blocks per SM), FP64 keeps 8 (two blocks per SM).
+template <typename T>
+struct RegShape;
+template <>
+struct RegShape<float> {
+  static constexpr int RPT = 12, NWARP = 8;
+};
+template <>
+struct RegShape<double> {
+  static constexpr int RPT = 8, NWARP = 8;
+};

@@ -73,12 +73,15 @@ def _problem(H, W, obstacles, seed):
     return fmu, fmv, fl, div
 
 
-@pytest.mark.parametrize("shape,obstacles,cycle", [((64, 64), False, "V"), ((96, 80), True, "V"), ((37, 50), True, "V"),
-                                                  ((256, 256), False, "V"), ((300, 260), True, "V"),
-                                                  ((200, 176), False, "W"), ((96, 80), True, "W")])
-def test_gmg_one_cycle_vs_oracle(shape, obstacles, cycle):
-    """Grids up to ~100^2 run wholly in the single-block kernel; larger ones also use the
-    grid-wide smoother / fused restriction / prolongation kernels."""
+@pytest.mark.parametrize("shape,obstacles,cycle,precision", [
+    ((64, 64), False, "V", "fp64"), ((96, 80), True, "V", "fp64"), ((37, 50), True, "V", "fp64"),
+    ((256, 256), False, "V", "fp64"), ((300, 260), True, "V", "fp64"), ((200, 176), False, "W", "fp64"),
+    ((96, 80), True, "W", "fp64"), ((1100, 1300), False, "V", "fp64"), ((1201, 1025), False, "V", "fp64"),
+    ((1100, 1300), False, "W", "fp32"), ((1201, 1025), False, "V", "fp32")])
+def test_gmg_one_cycle_vs_oracle(shape, obstacles, cycle, precision):
+    """Levels <= 16^2 run in the single-block tail kernel, open-box levels in the tiled level
+    kernels (register tiles on levels large enough to fill the GPU, 16 x 16 shared-memory
+    tiles below), levels with obstacles in the grid-wide kernels."""
     H, W = shape
     fmu, fmv, fl, div = _problem(H, W, obstacles, 1)
     alpha = -0.7
@@ -87,11 +90,14 @@ def test_gmg_one_cycle_vs_oracle(shape, obstacles, cycle):
     g.vcycle(0, pe, alpha * div)
     solver = sg.GeometricMultigridSolver()
     masks = (sg.OPEN_BOX, sg.OPEN_BOX) if not obstacles else (dev(fmu), dev(fmv))
-    p = torch.zeros((H, W), dtype=torch.float64, device="cuda")
+    dtype = torch.float64 if precision == "fp64" else torch.float32
+    p = torch.zeros((H, W), dtype=dtype, device="cuda")
     # cell_size, rho, dt chosen so that alpha = -(h^2) rho / dt = -0.7
-    solver(p, dev(div), masks[0], masks[1], 0.7, 1.0, 1.0, precision="fp64", fixed_cycles=1, cycle=cycle)
-    got = p.cpu().numpy()
-    assert np.max(np.abs(got - pe)) <= 1e-10 * np.max(np.abs(pe))
+    solver(p, dev(div.astype(np.float64 if precision == "fp64" else np.float32)), masks[0], masks[1], 0.7, 1.0, 1.0,
+           precision=precision, fixed_cycles=1, cycle=cycle)
+    got = p.double().cpu().numpy()
+    tol = 1e-10 if precision == "fp64" else 2e-5
+    assert np.max(np.abs(got - pe)) <= tol * np.max(np.abs(pe))
 
 
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 1e-8), ("fp32", 1e-5)])
