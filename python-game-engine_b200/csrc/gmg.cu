@@ -235,7 +235,8 @@ inline dim3 grid_wide(int64_t W, int64_t H) {
 
 template <typename T, typename TO>
 __global__ void k_gmg_fine_residual(int H, int W, const T* __restrict__ p, int64_t ldp, const T* __restrict__ bf,
-                                    int64_t ldb, LevelMask m, TO* __restrict__ r, int64_t ldr, double* __restrict__ partial) {
+                                    int64_t ldb, LevelMask m, TO* __restrict__ r, int64_t ldr, T* __restrict__ rfull,
+                                    double* __restrict__ partial) {
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int ib = blockIdx.x * kWX + threadIdx.x;
   double sq = 0.0;
@@ -247,6 +248,7 @@ __global__ void k_gmg_fine_residual(int H, int W, const T* __restrict__ p, int64
         T acc = residual_at(j, i, p, ldp, bf, ldb, m);
         sq += (double)acc * (double)acc;
         r[(int64_t)j * ldr + i] = (TO)acc;
+        if (rfull) rfull[(int64_t)j * ldr + i] = acc;
       }
     }
   }
@@ -598,6 +600,7 @@ __global__ void __launch_bounds__(kRX * kRY) k_gmg_residual_restrict_tiled(const
 
 // ---------------------------------------------------------------- fused tiled level kernels
 #include "gmg_tiled.cuh"
+#include "gmg_tail_open.cuh"
 #include "gmg_regtile.cuh"
 
 // ---------------------------------------------------------------- plan
@@ -618,10 +621,16 @@ struct sg_gmg_plan {
   std::vector<sg::Level> levels;
   std::vector<double> pinv;  // coarsest pseudo-inverse, n x n
   int tail_start = 0;        // first level handled by the single-block tail kernel
+  int tail_open = 0;         // every tail level is an open box (k_gmg_tail_open)
   int64_t tail_smem = 0;     // its dynamic shared memory (bytes)
   int64_t off_pinv = 0, off_bfine = 0, off_partial = 0, off_state = 0, bytes = 0;
   int64_t ld_bfine = 0;
   int64_t n_partial = 0;
+  // fused fine level (register tiles): post-smoothing, correction and residual in one
+  // kernel; the cycle rhs alternates between levels[0].off_b and off_b2, and off_r64 holds
+  // the residual in the precision of p when that differs from the cycle precision
+  int fused_ir = 0;
+  int64_t off_b2 = 0, off_r64 = 0;
   char* ws = nullptr;        // bound device workspace
   // cached solve graph
   cudaStream_t capture_stream = nullptr;
@@ -771,8 +780,70 @@ static T* ws_ptr(const sg_gmg_plan* p, int64_t off) {
 
 static GmgState* state_ptr(const sg_gmg_plan* p) { return (GmgState*)(p->ws + p->off_state); }
 
+// Shared-memory layout of the open-box tail (elements of T): every level's e planes first
+// (zeroed at start), then the b planes, then the restriction and residual scratch.
+struct OpenTailLayout {
+  int off_e[kMaxLevels], off_b[kMaxLevels], e_total, off_x, off_r, total;
+};
+
+static OpenTailLayout open_tail_layout(const std::vector<Level>& levels, int start) {
+  OpenTailLayout t;
+  std::memset(&t, 0, sizeof(t));
+  int n = (int)levels.size() - start;
+  int off = 0;
+  for (int q = 0; q < n; ++q) {
+    const Level& L = levels[start + q];
+    const int wh = (L.W + 1) / 2;
+    t.off_e[q] = off;
+    off += 2 * (L.H + 2) * (wh + 2);
+  }
+  t.e_total = off;
+  for (int q = 0; q < n; ++q) {
+    const Level& L = levels[start + q];
+    t.off_b[q] = off;
+    off += 2 * L.H * ((L.W + 1) / 2);
+  }
+  t.off_x = off;
+  off += levels[start].H * ((levels[start].W + 1) / 2);
+  t.off_r = off;
+  off += levels[start].H * levels[start].W;
+  t.total = off;
+  return t;
+}
+
+template <typename T>
+static int tail_open_launch(const sg_gmg_plan* p, bool zero_init, cudaStream_t s) {
+  OpenTailArgs<T> a;
+  std::memset(&a, 0, sizeof(a));
+  int nl = (int)p->levels.size();
+  a.n = nl - p->tail_start;
+  OpenTailLayout t = open_tail_layout(p->levels, p->tail_start);
+  for (int q = 0; q < a.n; ++q) {
+    a.H[q] = p->levels[p->tail_start + q].H;
+    a.W[q] = p->levels[p->tail_start + q].W;
+    a.off_e[q] = t.off_e[q];
+    a.off_b[q] = t.off_b[q];
+  }
+  a.e_total = t.e_total;
+  a.off_x = t.off_x;
+  a.off_r = t.off_r;
+  const Level& L0 = p->levels[p->tail_start];
+  a.ge = ws_ptr<T>(p, L0.off_e);
+  a.gb = ws_ptr<T>(p, L0.off_b);
+  a.gld = L0.ld;
+  a.pinv = (const double*)(p->ws + p->off_pinv);
+  a.omega = (T)p->omega;
+  a.pre = p->pre;
+  a.post = p->post;
+  a.wcycle = p->cycle;
+  a.zero_init = zero_init ? 1 : 0;
+  SG_LAUNCH(k_gmg_tail_open<T><<<1, dim3(32, kOpenTailThreads / 32), p->tail_smem, s>>>(a));
+  return SG_OK;
+}
+
 template <typename T>
 static int tail_launch(const sg_gmg_plan* p, bool zero_init, cudaStream_t s) {
+  if (p->tail_open) return tail_open_launch<T>(p, zero_init, s);
   TailArgs<T> a;
   std::memset(&a, 0, sizeof(a));
   int nl = (int)p->levels.size();
@@ -835,27 +906,48 @@ static void launch_post_t(const sg_gmg_plan* p, int k, cudaStream_t s) {
 }
 
 template <typename T, int SW>
-static void launch_pre_reg(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
-  constexpr int RPT = RegShape<T>::RPT, NW = RegShape<T>::NWARP;
+static void launch_pre_reg(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s, const T* b_alt = nullptr) {
+  constexpr int RPT = RegShape<T>::RPT, NW = RegShape<T>::NWARP, MB = RegShape<T>::MINB;
   using S = RegPre<T, SW, RPT, NW>;
   const Level& L = p->levels[k];
   const Level& C = p->levels[k + 1];
   dim3 g((L.W + S::TXO - 1) / S::TXO, (L.H + S::TYO - 1) / S::TYO);
-  SG_LAUNCH(k_gmg_pre_reg<T, SW, RPT, NW><<<g, 32 * NW, 0, s>>>(
-      zero_init ? nullptr : ws_ptr<T>(p, L.off_e), ws_ptr<T>(p, L.off_e2), ws_ptr<T>(p, L.off_b), L.ld, L.H, L.W,
-      ws_ptr<T>(p, C.off_b), C.ld, C.H, C.W, (T)p->omega));
+  SG_LAUNCH(k_gmg_pre_reg<T, SW, RPT, NW, MB><<<g, 32 * NW, 0, s>>>(
+      zero_init ? nullptr : ws_ptr<T>(p, L.off_e), ws_ptr<T>(p, L.off_e2), ws_ptr<T>(p, L.off_b), b_alt,
+      state_ptr(p), L.ld, L.H, L.W, ws_ptr<T>(p, C.off_b), C.ld, C.H, C.W, (T)p->omega));
 }
 
 template <typename T, int SW>
 static void launch_post_reg(const sg_gmg_plan* p, int k, cudaStream_t s) {
-  constexpr int RPT = RegShape<T>::RPT, NW = RegShape<T>::NWARP;
+  constexpr int RPT = RegShape<T>::RPT, NW = RegShape<T>::NWARP, MB = RegShape<T>::MINB;
   using S = RegPost<T, SW, RPT, NW>;
   const Level& L = p->levels[k];
   const Level& C = p->levels[k + 1];
   dim3 g((L.W + S::TXO - 1) / S::TXO, (L.H + S::TYO - 1) / S::TYO);
-  SG_LAUNCH(k_gmg_post_reg<T, SW, RPT, NW><<<g, 32 * NW, 0, s>>>(
+  SG_LAUNCH(k_gmg_post_reg<T, SW, RPT, NW, MB><<<g, 32 * NW, 0, s>>>(
       ws_ptr<T>(p, L.off_e2), ws_ptr<T>(p, L.off_e), ws_ptr<T>(p, L.off_b), L.ld, L.H, L.W, ws_ptr<T>(p, C.off_e),
       C.ld, C.H, C.W, (T)p->omega));
+}
+
+// Grid of the fused fine-level post kernel (also the number of its partial sums).
+template <typename TC>
+static dim3 post_final_grid(const sg_gmg_plan* p) {
+  constexpr int RPT = RegShape<TC>::RPT, NW = RegShape<TC>::NWARP;
+  const int sw = p->post < 1 ? 1 : (p->post > 3 ? 3 : p->post);
+  const int halo = 2 * sw + 2, txo = kRW - 2 * halo, tyo = NW * RPT - 2 * halo;
+  const Level& L = p->levels[0];
+  return dim3((L.W + txo - 1) / txo, (L.H + tyo - 1) / tyo);
+}
+
+template <typename TC, typename TP, int SW>
+static void launch_post_final(const sg_gmg_plan* p, TP* pp, int64_t ldp, cudaStream_t s) {
+  constexpr int RPT = RegShape<TC>::RPT, NW = RegShape<TC>::NWARP, MB = RegShape<TC>::MINB_FINAL;
+  const Level& L = p->levels[0];
+  const Level& C = p->levels[1];
+  TP* r64 = p->off_r64 ? (TP*)(p->ws + p->off_r64) : nullptr;
+  SG_LAUNCH(k_gmg_post_final_reg<TC, TP, SW, RPT, NW, MB><<<post_final_grid<TC>(p), 32 * NW, 0, s>>>(
+      ws_ptr<TC>(p, L.off_e2), ws_ptr<TC>(p, L.off_b), ws_ptr<TC>(p, p->off_b2), state_ptr(p), L.ld, L.H, L.W,
+      ws_ptr<TC>(p, C.off_e), C.ld, C.H, C.W, (TC)p->omega, pp, ldp, r64, (double*)(p->ws + p->off_partial)));
 }
 
 // Large levels: register tiles; small levels: 16 x 16 shared-memory tiles.
@@ -957,7 +1049,9 @@ static void prologue(const sg_gmg_plan* p, const TP* pp, int64_t ldp, const TD* 
   SG_LAUNCH(k_gmg_rhs<TD, TP><<<g, block2d(), 0, s>>>(L.H, L.W, div, ldd, st, m, bf, p->ld_bfine, part));
   SG_LAUNCH(k_gmg_finalize_norm<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st));
   SG_LAUNCH(k_gmg_fine_residual<TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, pp, ldp, bf, p->ld_bfine, m,
-                                                                   ws_ptr<TC>(p, L.off_b), L.ld, part));
+                                                                   ws_ptr<TC>(p, L.off_b), L.ld,
+                                                                   p->off_r64 ? (TP*)(p->ws + p->off_r64) : nullptr,
+                                                                   part));
   SG_LAUNCH(k_gmg_finalize_rel<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st, h, use_handle, 0));
 }
 
@@ -969,11 +1063,32 @@ static void body(const sg_gmg_plan* p, TP* pp, int64_t ldp, cudaGraphConditional
   LevelMask m = level_mask(p, 0);
   double* part = (double*)(p->ws + p->off_partial);
   GmgState* st = state_ptr(p);
+  if (p->fused_ir) {
+    // pre (rhs by cycle parity) -> coarse levels -> post + correction + next residual
+    const TC* b_alt = ws_ptr<TC>(p, p->off_b2);
+    switch (p->pre) {
+      case 1: launch_pre_reg<TC, 1>(p, 0, true, s, b_alt); break;
+      case 2: launch_pre_reg<TC, 2>(p, 0, true, s, b_alt); break;
+      default: launch_pre_reg<TC, 3>(p, 0, true, s, b_alt); break;
+    }
+    const int nl = (int)p->levels.size();
+    int reps = (p->cycle == 1 && 1 < nl - 1) ? 2 : 1;
+    for (int q = 0; q < reps; ++q) cycle<TC>(p, 1, q == 0, s);
+    switch (p->post) {
+      case 1: launch_post_final<TC, TP, 1>(p, pp, ldp, s); break;
+      case 2: launch_post_final<TC, TP, 2>(p, pp, ldp, s); break;
+      default: launch_post_final<TC, TP, 3>(p, pp, ldp, s); break;
+    }
+    dim3 gf = post_final_grid<TC>(p);
+    SG_LAUNCH(k_gmg_finalize_rel<<<1, 1024, 0, s>>>(part, (int)(gf.x * gf.y), st, h, use_handle, 1));
+    return;
+  }
   dim3 g = grid_wide(L.W, L.H);
   cycle<TC>(p, 0, true, s);
   SG_LAUNCH(k_gmg_correct<TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, pp, ldp, ws_ptr<TC>(p, L.off_e), L.ld));
   SG_LAUNCH(k_gmg_fine_residual<TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, pp, ldp, (const TP*)(p->ws + p->off_bfine),
-                                                                   p->ld_bfine, m, ws_ptr<TC>(p, L.off_b), L.ld, part));
+                                                                   p->ld_bfine, m, ws_ptr<TC>(p, L.off_b), L.ld,
+                                                                   (TP*)nullptr, part));
   SG_LAUNCH(k_gmg_finalize_rel<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st, h, use_handle, 1));
 }
 
@@ -1166,25 +1281,33 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
     delete p;
     return fail(SG_ERR_ARG, "coarsest operator could not be factorised");
   }
-  // tail: the largest suffix of levels (each <= 128 cells a side) whose e and b arrays plus
-  // the restriction scratch of its first level (H x ceil(W/2)) fit the shared-memory budget
+  // tail: the largest suffix of levels that fits one block's shared memory: open boxes up
+  // to kOpenTailMaxSide cells a side (k_gmg_tail_open), otherwise up to kTailMaxSide
+  // (k_gmg_tail, codes from global memory); e and b of every level plus the scratch of
+  // the first one
   size_t cyc = precision == SG_GMG_FP64 ? sizeof(double) : sizeof(float);
   const int64_t budget = 220 * 1024;
   int nl = (int)p->levels.size();
-  int64_t acc = 0;  // elements of e and b below the candidate level
+  auto generic_elems = [&](int start) {
+    int64_t acc = 0;
+    for (int k = start; k < nl; ++k) acc += ((2 * (int64_t)p->levels[k].H * p->levels[k].W + 3) & ~(int64_t)3);
+    return acc + (int64_t)p->levels[start].H * ((p->levels[start].W + 1) / 2);
+  };
   p->tail_start = nl - 1;
+  bool open_suffix = true;
   for (int k = nl - 1; k >= 0; --k) {
     const Level& L = p->levels[k];
-    int64_t arrays = acc + ((2 * (int64_t)L.H * L.W + 3) & ~(int64_t)3);
-    int64_t scratch = (int64_t)L.H * ((L.W + 1) / 2);
-    if (std::max(L.H, L.W) > kTailMaxSide || (arrays + scratch) * (int64_t)cyc > budget) break;
-    acc = arrays;
+    const bool open = open_suffix && L.analytic;
+    const int side = std::max(L.H, L.W);
+    const int64_t elems = open ? (int64_t)open_tail_layout(p->levels, k).total : generic_elems(k);
+    if (side > (open ? kOpenTailMaxSide : kTailMaxSide) || elems * (int64_t)cyc > budget) break;
+    open_suffix = open;
     p->tail_start = k;
   }
-  acc = 0;
-  for (int k = p->tail_start; k < nl; ++k) acc += ((2 * (int64_t)p->levels[k].H * p->levels[k].W + 3) & ~(int64_t)3);
-  const Level& T0 = p->levels[p->tail_start];
-  p->tail_smem = (acc + (int64_t)T0.H * ((T0.W + 1) / 2)) * (int64_t)cyc;
+  p->tail_open = open_suffix ? 1 : 0;
+  p->tail_smem = (p->tail_open ? (int64_t)open_tail_layout(p->levels, p->tail_start).total
+                               : generic_elems(p->tail_start)) *
+                 (int64_t)cyc;
   // workspace layout
   size_t fine = precision == SG_GMG_FP32 ? sizeof(float) : sizeof(double);
   int64_t off = 0;
@@ -1211,10 +1334,23 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
   p->ld_bfine = p->levels[0].ld;
   p->off_bfine = off;
   off = align256(off + p->ld_bfine * p->H * (int64_t)fine);
+  p->fused_ir = (p->levels.size() >= 2 && p->tail_start >= 1 && p->levels[0].fused && !small_tiles(p->levels[0])) ? 1 : 0;
+  if (p->fused_ir) {
+    p->off_b2 = off;
+    off = align256(off + p->levels[0].ld * p->H * (int64_t)cyc);
+    if (precision == SG_GMG_MIXED) {
+      p->off_r64 = off;
+      off = align256(off + p->levels[0].ld * p->H * (int64_t)fine);
+    }
+  }
   p->off_pinv = off;
   off = align256(off + (int64_t)p->pinv.size() * 8);
   dim3 g = grid_wide(p->W, p->H);
   p->n_partial = (int64_t)g.x * g.y;
+  if (p->fused_ir) {
+    dim3 gf = precision == SG_GMG_FP64 ? post_final_grid<double>(p) : post_final_grid<float>(p);
+    p->n_partial = std::max(p->n_partial, (int64_t)gf.x * gf.y);
+  }
   p->off_partial = off;
   off = align256(off + p->n_partial * 8);
   p->off_state = off;
@@ -1257,10 +1393,15 @@ int sg_gmg_bind(sg_gmg_plan* plan, void* workspace, void* stream) {
   int rc = plan->precision == SG_GMG_FP64 ? set_tiled_smem_limits<double>() : set_tiled_smem_limits<float>();
   if (rc != SG_OK) return rc;
   int smem = (int)plan->tail_smem;
-  if (plan->precision == SG_GMG_FP64)
+  if (plan->precision == SG_GMG_FP64) {
     SG_CUDA_TRY(cudaFuncSetAttribute(k_gmg_tail<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
-  else
+    SG_CUDA_TRY(cudaFuncSetAttribute(k_gmg_tail_open<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                "smem attr");
+  } else {
     SG_CUDA_TRY(cudaFuncSetAttribute(k_gmg_tail<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
+    SG_CUDA_TRY(cudaFuncSetAttribute(k_gmg_tail_open<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                "smem attr");
+  }
   return SG_OK;
 }
 

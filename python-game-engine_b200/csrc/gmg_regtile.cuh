@@ -277,12 +277,16 @@ __device__ __forceinline__ void reg_pre_body(RegXchg<T, NWARP>& x, const T* __re
 
 // pre: SW sweeps from e_in (NULL: zero initial guess), residual and its full weighting
 // into bc; the smoothed cells go to e_out.
-template <typename T, int SW, int RPT, int NWARP>
-__global__ void __launch_bounds__(32 * NWARP) k_gmg_pre_reg(const T* __restrict__ e_in, T* __restrict__ e_out,
-                                                           const T* __restrict__ b, int64_t ld, int H, int W,
+// b_alt (fine level of a fused solve only): the rhs alternates between b and b_alt from
+// cycle to cycle (b on even cycles), as k_gmg_post_final_reg writes the next one.
+template <typename T, int SW, int RPT, int NWARP, int MINB>
+__global__ void __launch_bounds__(32 * NWARP, MINB) k_gmg_pre_reg(const T* __restrict__ e_in, T* __restrict__ e_out,
+                                                           const T* __restrict__ b, const T* __restrict__ b_alt,
+                                                           const GmgState* __restrict__ st, int64_t ld, int H, int W,
                                                            T* __restrict__ bc, int64_t ldc, int Hc, int Wc, T omega) {
   using S = RegPre<T, SW, RPT, NWARP>;
   __shared__ RegXchg<T, NWARP> x;
+  if (b_alt && (st->cycles & 1)) b = b_alt;
   const int i0 = blockIdx.x * S::TXO - S::HALO;
   const int j0 = blockIdx.y * S::TYO - S::HALO;
   const bool inside = i0 >= 0 && i0 + kRW <= W && j0 >= 0 && j0 + NWARP * RPT <= H;
@@ -292,15 +296,14 @@ __global__ void __launch_bounds__(32 * NWARP) k_gmg_pre_reg(const T* __restrict_
     reg_pre_body<T, SW, RPT, NWARP, true>(x, e_in, e_out, b, ld, H, W, bc, ldc, Hc, Wc, omega, i0, j0);
 }
 
+// e = e_in + P ec on the thread's cells, then SW sweeps (e and b stay in registers).
 template <typename T, int SW, int RPT, int NWARP, bool BOUNDED>
-__device__ __forceinline__ void reg_post_body(RegXchg<T, NWARP>& x, const T* __restrict__ e_in, T* __restrict__ e_out,
-                                              const T* __restrict__ bsrc, int64_t ld, int H, int W,
-                                              const T* __restrict__ ec, int64_t ldc, int Hc, int Wc, T omega, int i0,
-                                              int j0) {
-  using S = RegPost<T, SW, RPT, NWARP>;
+__device__ __forceinline__ void reg_prolong_smooth(RegXchg<T, NWARP>& x, T (&e)[RPT][2], T (&b)[RPT][2],
+                                                   const T* __restrict__ e_in, const T* __restrict__ bsrc, int64_t ld,
+                                                   int H, int W, const T* __restrict__ ec, int64_t ldc, int Hc, int Wc,
+                                                   T omega, int i0, int j0) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int i = i0 + 2 * lane, j = j0 + w * RPT;
-  T e[RPT][2], b[RPT][2];
   reg_load<T, RPT, BOUNDED>(b, bsrc, ld, j, i, H, W);
   reg_load<T, RPT, BOUNDED>(e, e_in, ld, j, i, H, W);
   // bilinear prolongation: fine (j, i) from coarse (J, I), (J, X), (Y, I), (Y, X) with
@@ -355,14 +358,26 @@ __device__ __forceinline__ void reg_post_body(RegXchg<T, NWARP>& x, const T* __r
     cr = nr;
   }
   reg_sweeps<T, RPT, NWARP, 2 * SW, 0, BOUNDED>(x, e, b, omega, w, lane, j, i, H, W);
+}
+
+template <typename T, int SW, int RPT, int NWARP, bool BOUNDED>
+__device__ __forceinline__ void reg_post_body(RegXchg<T, NWARP>& x, const T* __restrict__ e_in, T* __restrict__ e_out,
+                                              const T* __restrict__ bsrc, int64_t ld, int H, int W,
+                                              const T* __restrict__ ec, int64_t ldc, int Hc, int Wc, T omega, int i0,
+                                              int j0) {
+  using S = RegPost<T, SW, RPT, NWARP>;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = i0 + 2 * lane, j = j0 + w * RPT;
+  T e[RPT][2], b[RPT][2];
+  reg_prolong_smooth<T, SW, RPT, NWARP, BOUNDED>(x, e, b, e_in, bsrc, ld, H, W, ec, ldc, Hc, Wc, omega, i0, j0);
   const int r_lo = S::HALO - w * RPT, r_hi = S::HALO + S::TYO - w * RPT;
   reg_store<T, RPT, BOUNDED>(e, e_out, ld, j, i, H, W, 2 * lane >= S::HALO && 2 * lane < S::HALO + S::TXO, r_lo,
                              r_hi);
 }
 
 // post: e_out = smoothed (e_in + P ec).
-template <typename T, int SW, int RPT, int NWARP>
-__global__ void __launch_bounds__(32 * NWARP) k_gmg_post_reg(const T* __restrict__ e_in, T* __restrict__ e_out,
+template <typename T, int SW, int RPT, int NWARP, int MINB>
+__global__ void __launch_bounds__(32 * NWARP, MINB) k_gmg_post_reg(const T* __restrict__ e_in, T* __restrict__ e_out,
                                                             const T* __restrict__ b, int64_t ld, int H, int W,
                                                             const T* __restrict__ ec, int64_t ldc, int Hc, int Wc,
                                                             T omega) {
@@ -377,15 +392,160 @@ __global__ void __launch_bounds__(32 * NWARP) k_gmg_post_reg(const T* __restrict
     reg_post_body<T, SW, RPT, NWARP, true>(x, e_in, e_out, b, ld, H, W, ec, ldc, Hc, Wc, omega, i0, j0);
 }
 
-// Rows per thread and warps per block of the register tiles: FP32 keeps 12 rows of e and b
-// per thread (about 70 registers, three blocks per SM), FP64 keeps 8 (two blocks per SM).
+__device__ __forceinline__ void prefetch_l2(const void* ptr) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+}
+
+// Fine level of a fused solve: post-smoothing, the correction p += e and the next residual
+// in one pass. The residual follows r_new = r - A e (A p = sum over open faces of
+// p - p_nb), which equals bf - A (p + e) up to rounding; every cell it writes needs e on
+// its four neighbours only, so the tile halo is 2 SW + 2 (as for the pre kernel) and p is
+// read and written on owned cells alone. The cycle rhs alternates between b0 and b1 by the
+// parity of the cycle count (read from b0 on even cycles, next one written to the other).
+// r64: the residual in the precision of p when it differs from the cycle's (mixed
+// precision); otherwise the cycle rhs itself is the residual. Per-block sums of r^2 go to
+// partial[] for k_gmg_finalize_rel.
+template <typename TC, typename TP, int SW, int RPT, int NWARP, bool BOUNDED>
+__device__ __forceinline__ void reg_post_final_body(RegXchg<TC, NWARP>& x, const TC* __restrict__ e_in,
+                                                    const TC* __restrict__ bsrc, TC* __restrict__ bdst, int64_t ld,
+                                                    int H, int W, const TC* __restrict__ ec, int64_t ldc, int Hc,
+                                                    int Wc, TC omega, TP* __restrict__ p, int64_t ldp,
+                                                    TP* __restrict__ r64, int i0, int j0, double& sq) {
+  using S = RegPre<TC, SW, RPT, NWARP>;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = i0 + 2 * lane, j = j0 + w * RPT;
+  const bool cols_owned = 2 * lane >= S::HALO && 2 * lane < S::HALO + S::TXO && (!BOUNDED || i < W);
+  const int r_lo = S::HALO - w * RPT, r_hi = S::HALO + S::TYO - w * RPT;
+  // p and r64 are only needed after the sweeps: start bringing the owned rows into L2 now
+  if (cols_owned) {
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+      if (r < r_lo || r >= r_hi || (BOUNDED && j + r >= H)) continue;
+      prefetch_l2(p + (int64_t)(j + r) * ldp + i);
+      if (r64) prefetch_l2(r64 + (int64_t)(j + r) * ld + i);
+    }
+  }
+  TC e[RPT][2], b[RPT][2];
+  reg_prolong_smooth<TC, SW, RPT, NWARP, BOUNDED>(x, e, b, e_in, bsrc, ld, H, W, ec, ldc, Hc, Wc, omega, i0, j0);
+  TC above[2], below[2];
+  exchange_rows<TC, RPT, NWARP>(x, (2 * SW) & 1, e, w, lane, above, below);
+  using VC = typename Pair<TC>::V;
+  using VP = typename Pair<TP>::V;
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) {
+    const TC l1 = shfl_up1(e[r][1]);
+    const TC r0 = shfl_down1(e[r][0]);
+    if (r < r_lo || r >= r_hi || !cols_owned) continue;
+    const int jj = j + r;
+    if (BOUNDED && jj >= H) continue;
+    const int64_t o = (int64_t)jj * ld + i;
+    TP acc[2];
+    if (r64 && !BOUNDED) {
+      const VP t = *reinterpret_cast<const VP*>(r64 + o);
+      acc[0] = t.x;
+      acc[1] = t.y;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 2; ++q) acc[q] = r64 ? ((!BOUNDED || i + q < W) ? r64[o + q] : (TP)0) : (TP)b[r][q];
+    }
+    TP xv[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int ii = i + q;
+      xv[q] = (TP)e[r][q];
+      const TP left = (TP)(q == 0 ? l1 : e[r][0]);
+      const TP right = (TP)(q == 0 ? e[r][1] : r0);
+      const TP up = (TP)(r > 0 ? e[r > 0 ? r - 1 : 0][q] : above[q]);
+      const TP down = (TP)(r < RPT - 1 ? e[r < RPT - 1 ? r + 1 : 0][q] : below[q]);
+      if (!BOUNDED) {
+        acc[q] += left - xv[q];
+        acc[q] += right - xv[q];
+        acc[q] += up - xv[q];
+        acc[q] += down - xv[q];
+      } else {
+        if (ii > 0) acc[q] += left - xv[q];
+        if (ii < W - 1) acc[q] += right - xv[q];
+        if (jj > 0) acc[q] += up - xv[q];
+        if (jj < H - 1) acc[q] += down - xv[q];
+      }
+    }
+    TP* pc = p + (int64_t)jj * ldp + i;
+    if (!BOUNDED) {
+      pc[0] = pc[0] + xv[0];
+      pc[1] = pc[1] + xv[1];
+      if (r64) {
+        VP t;
+        t.x = acc[0];
+        t.y = acc[1];
+        *reinterpret_cast<VP*>(r64 + o) = t;
+      }
+      VC c;
+      c.x = (TC)acc[0];
+      c.y = (TC)acc[1];
+      *reinterpret_cast<VC*>(bdst + o) = c;
+      sq += (double)acc[0] * (double)acc[0];
+      sq += (double)acc[1] * (double)acc[1];
+    } else {
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        if (i + q >= W) continue;
+        pc[q] = pc[q] + xv[q];
+        if (r64) r64[o + q] = acc[q];
+        bdst[o + q] = (TC)acc[q];
+        sq += (double)acc[q] * (double)acc[q];
+      }
+    }
+  }
+}
+
+template <typename TC, typename TP, int SW, int RPT, int NWARP, int MINB>
+__global__ void __launch_bounds__(32 * NWARP, MINB)
+    k_gmg_post_final_reg(const TC* __restrict__ e_in, TC* __restrict__ b0, TC* __restrict__ b1,
+                         const GmgState* __restrict__ st, int64_t ld, int H, int W, const TC* __restrict__ ec,
+                         int64_t ldc, int Hc, int Wc, TC omega, TP* __restrict__ p, int64_t ldp, TP* __restrict__ r64,
+                         double* __restrict__ partial) {
+  using S = RegPre<TC, SW, RPT, NWARP>;
+  __shared__ RegXchg<TC, NWARP> x;
+  const bool odd = st->cycles & 1;
+  const TC* bsrc = odd ? b1 : b0;
+  TC* bdst = odd ? b0 : b1;
+  const int i0 = blockIdx.x * S::TXO - S::HALO;
+  const int j0 = blockIdx.y * S::TYO - S::HALO;
+  const bool inside = i0 >= 0 && i0 + kRW <= W && j0 >= 0 && j0 + NWARP * RPT <= H;
+  double sq = 0.0;
+  if (inside)
+    reg_post_final_body<TC, TP, SW, RPT, NWARP, false>(x, e_in, bsrc, bdst, ld, H, W, ec, ldc, Hc, Wc, omega, p, ldp,
+                                                      r64, i0, j0, sq);
+  else
+    reg_post_final_body<TC, TP, SW, RPT, NWARP, true>(x, e_in, bsrc, bdst, ld, H, W, ec, ldc, Hc, Wc, omega, p, ldp,
+                                                     r64, i0, j0, sq);
+  const double s = block_sum(sq);
+  if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
+}
+
+// Rows per thread, warps per block and minimum resident blocks per SM of the register
+// tiles (the last caps the registers a thread may use); MINB_FINAL for the fused fine-level
+// post kernel.
+#ifndef SG_REG_F32_RPT
+#define SG_REG_F32_RPT 8
+#define SG_REG_F32_NWARP 8
+#define SG_REG_F32_MINB 4
+#endif
+#ifndef SG_REG_F64_RPT
+#define SG_REG_F64_RPT 4
+#define SG_REG_F64_NWARP 8
+#define SG_REG_F64_MINB 4
+#endif
+#ifndef SG_REG_FINAL_MINB
+#define SG_REG_FINAL_MINB 4
+#endif
+template <int R, int N, int M>
+struct RegShapeOf {
+  static constexpr int RPT = R, NWARP = N, MINB = M, MINB_FINAL = SG_REG_FINAL_MINB;
+};
 template <typename T>
 struct RegShape;
 template <>
-struct RegShape<float> {
-  static constexpr int RPT = 12, NWARP = 8;
-};
+struct RegShape<float> : RegShapeOf<SG_REG_F32_RPT, SG_REG_F32_NWARP, SG_REG_F32_MINB> {};
 template <>
-struct RegShape<double> {
-  static constexpr int RPT = 8, NWARP = 8;
-};
+struct RegShape<double> : RegShapeOf<SG_REG_F64_RPT, SG_REG_F64_NWARP, SG_REG_F64_MINB> {};

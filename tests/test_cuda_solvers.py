@@ -77,11 +77,12 @@ def _problem(H, W, obstacles, seed):
     ((64, 64), False, "V", "fp64"), ((96, 80), True, "V", "fp64"), ((37, 50), True, "V", "fp64"),
     ((256, 256), False, "V", "fp64"), ((300, 260), True, "V", "fp64"), ((200, 176), False, "W", "fp64"),
     ((96, 80), True, "W", "fp64"), ((1100, 1300), False, "V", "fp64"), ((1201, 1025), False, "V", "fp64"),
-    ((1100, 1300), False, "W", "fp32"), ((1201, 1025), False, "V", "fp32")])
+    ((1100, 1300), False, "W", "fp32"), ((1201, 1025), False, "V", "fp32"), ((1100, 1300), False, "V", "mixed")])
 def test_gmg_one_cycle_vs_oracle(shape, obstacles, cycle, precision):
-    """Levels <= 16^2 run in the single-block tail kernel, open-box levels in the tiled level
-    kernels (register tiles on levels large enough to fill the GPU, 16 x 16 shared-memory
-    tiles below), levels with obstacles in the grid-wide kernels."""
+    """Coarse levels run in a single-block tail kernel, open-box levels in the tiled level
+    kernels (register tiles on levels large enough to fill the GPU, the fine one fused with
+    the correction and residual; 16 x 16 shared-memory tiles below), levels with obstacles
+    in the grid-wide kernels."""
     H, W = shape
     fmu, fmv, fl, div = _problem(H, W, obstacles, 1)
     alpha = -0.7
@@ -90,8 +91,7 @@ def test_gmg_one_cycle_vs_oracle(shape, obstacles, cycle, precision):
     g.vcycle(0, pe, alpha * div)
     solver = sg.GeometricMultigridSolver()
     masks = (sg.OPEN_BOX, sg.OPEN_BOX) if not obstacles else (dev(fmu), dev(fmv))
-    dtype = torch.float64 if precision == "fp64" else torch.float32
-    p = torch.zeros((H, W), dtype=dtype, device="cuda")
+    p = torch.zeros((H, W), dtype=torch.float32 if precision == "fp32" else torch.float64, device="cuda")
     # cell_size, rho, dt chosen so that alpha = -(h^2) rho / dt = -0.7
     solver(p, dev(div.astype(np.float64 if precision == "fp64" else np.float32)), masks[0], masks[1], 0.7, 1.0, 1.0,
            precision=precision, fixed_cycles=1, cycle=cycle)
@@ -124,6 +124,37 @@ def test_gmg_reaches_tolerance(precision, tol, obstacles):
     # relative (about 1.3e4 * tol at 128^2); the bounds below sit well inside that
     bound = {"fp64": 1e-6, "mixed": 1e-4, "fp32": 5e-2}[precision]
     assert np.max(np.abs(a - b)) <= bound * np.max(np.abs(b))
+
+
+def _true_relres(p, b):
+    """||b - A p|| / ||b|| on an open box, A p = sum over open faces of p - p_nb (float64)."""
+    r = b.copy()
+    r[:, 1:] += p[:, :-1] - p[:, 1:]
+    r[:, :-1] += p[:, 1:] - p[:, :-1]
+    r[1:, :] += p[:-1, :] - p[1:, :]
+    r[:-1, :] += p[1:, :] - p[:-1, :]
+    return np.linalg.norm(r) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 1e-8), ("fp32", 1e-4)])
+def test_gmg_large_grid_reported_residual_is_true(precision, tol):
+    """On grids large enough for the fused fine-level kernel the residual is carried from
+    cycle to cycle (r - A e) rather than recomputed; the relative residual the solver reports
+    must still be the true one of the returned pressure, and the solve must get there."""
+    H, W = 1100, 1300
+    _, _, _, div = _problem(H, W, False, 4)
+    solver = sg.GeometricMultigridSolver()
+    p = torch.zeros((H, W), dtype=torch.float32 if precision == "fp32" else torch.float64, device="cuda")
+    d = dev(div.astype(np.float64 if precision == "fp64" else np.float32))
+    solver(p, d, sg.OPEN_BOX, sg.OPEN_BOX, 1.0, 1.0 / H, 0.5 / H, tol=tol, max_cycles=40, precision=precision,
+           strict=True)
+    assert solver.converged and solver.last_relres <= tol
+    alpha = O.alpha_coeff(1.0 / H, 1.0, 0.5 / H)
+    b = alpha * d.double().cpu().numpy()
+    true = _true_relres(p.double().cpu().numpy(), b)
+    # the reported value tracks the true one to rounding (FP32: to the rounding of p itself)
+    slack = {"fp64": 1e-3, "mixed": 1e-3, "fp32": 0.5}[precision]
+    assert abs(true - solver.last_relres) <= slack * tol + 1e-13
 
 
 def test_gmg_fixed_cycles_residual_history():
