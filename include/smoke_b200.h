@@ -280,6 +280,15 @@ int sg_gmg_level_shape(const sg_gmg_plan* plan, int level, int* H, int* W);
 /* Run `sweeps` smoother sweeps on one level's workspace buffers (whatever they hold);
  * a building block exposed for timing the smoother in isolation. */
 int sg_gmg_smooth_async(sg_gmg_plan* plan, int level, int sweeps, void* stream);
+/* 1 when the plan's fine level runs the fused register-tiled kernels (open box, large
+ * enough to fill the GPU): pre-smoothing + restriction in one launch, post-smoothing +
+ * correction of p + next residual in another. */
+int sg_gmg_fine_fused(const sg_gmg_plan* plan);
+/* One launch of a fused fine-level kernel on the bound workspace, whatever it holds
+ * (which = 0: pre kernel; 1: post kernel, which adds its correction to p, ld_p >= W, in the
+ * plan's fine precision). Exposed for timing the solver's dominant kernels in isolation;
+ * the solve itself runs them inside its graph. No counterpart in the reference. */
+int sg_gmg_fine_kernel_async(sg_gmg_plan* plan, int which, void* p, int64_t ld_p, void* stream);
 
 #ifdef __cplusplus
 }

@@ -65,6 +65,8 @@ SIGNATURES = {
     "sg_gmg_tail_start": [P],
     "sg_gmg_level_shape": [P, I, PI, PI],
     "sg_gmg_smooth_async": [P, I, I, P],
+    "sg_gmg_fine_fused": [P],
+    "sg_gmg_fine_kernel_async": [P, I, P, I64, P],
     "sg_version": [],
     "sg_last_error": [],
     "sg_launch_count": [],

@@ -1529,4 +1529,40 @@ int sg_gmg_smooth_async(sg_gmg_plan* plan, int level, int sweeps, void* stream) 
   return check_launch("sg_gmg_smooth_async");
 }
 
+int sg_gmg_fine_fused(const sg_gmg_plan* plan) { return plan ? plan->fused_ir : 0; }
+
+int sg_gmg_fine_kernel_async(sg_gmg_plan* plan, int which, void* p, int64_t ld_p, void* stream) {
+  SG_REQUIRE(plan && plan->ws, "plan not bound to a workspace");
+  SG_REQUIRE(plan->fused_ir, "the fine level of this plan does not run the fused kernels");
+  SG_REQUIRE(which == 0 || which == 1, "which must be 0 (pre) or 1 (post)");
+  SG_REQUIRE(which == 0 || (p && ld_p >= plan->W), "post kernel needs the pressure array");
+  cudaStream_t s = as_stream(stream);
+  auto pre = [&](auto tag) {
+    using TC = decltype(tag);
+    const TC* b_alt = ws_ptr<TC>(plan, plan->off_b2);
+    switch (plan->pre) {
+      case 1: launch_pre_reg<TC, 1>(plan, 0, true, s, b_alt); break;
+      case 2: launch_pre_reg<TC, 2>(plan, 0, true, s, b_alt); break;
+      default: launch_pre_reg<TC, 3>(plan, 0, true, s, b_alt); break;
+    }
+  };
+  auto post = [&](auto tc, auto tp) {
+    using TC = decltype(tc);
+    using TP = decltype(tp);
+    switch (plan->post) {
+      case 1: launch_post_final<TC, TP, 1>(plan, (TP*)p, ld_p, s); break;
+      case 2: launch_post_final<TC, TP, 2>(plan, (TP*)p, ld_p, s); break;
+      default: launch_post_final<TC, TP, 3>(plan, (TP*)p, ld_p, s); break;
+    }
+  };
+  if (plan->precision == SG_GMG_FP64) {
+    if (which == 0) pre(0.0); else post(0.0, 0.0);
+  } else if (plan->precision == SG_GMG_MIXED) {
+    if (which == 0) pre(0.0f); else post(0.0f, 0.0);
+  } else {
+    if (which == 0) pre(0.0f); else post(0.0f, 0.0f);
+  }
+  return check_launch("sg_gmg_fine_kernel_async");
+}
+
 }  // extern "C"

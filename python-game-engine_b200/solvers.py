@@ -285,6 +285,16 @@ class GMGPlan:
     def tail_start(self):
         return L.load().sg_gmg_tail_start(self.handle)
 
+    def fine_fused(self):
+        """True when the fine level runs the fused register-tiled pre/post kernels."""
+        return bool(L.load().sg_gmg_fine_fused(self.handle))
+
+    def fine_kernel_async(self, which, pressure=None):
+        """Launch the fused fine-level pre (0) or post (1) kernel once on the workspace as it
+        stands (for timing the dominant kernels alone; the post kernel adds to `pressure`)."""
+        p, ldp = L.field(pressure, "pressure") if pressure is not None else (None, 0)
+        L.call("sg_gmg_fine_kernel_async", self.handle, int(which), p, ldp, L.stream_ptr())
+
     def cycles_async(self, pressure, divergence, alpha, n_cycles, relres_out):
         p, ldp = L.field(pressure, "pressure")
         d, ldd = L.field(divergence, "divergence")
