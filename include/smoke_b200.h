@@ -290,6 +290,54 @@ int sg_gmg_fine_fused(const sg_gmg_plan* plan);
  * the solve itself runs them inside its graph. No counterpart in the reference. */
 int sg_gmg_fine_kernel_async(sg_gmg_plan* plan, int which, void* p, int64_t ld_p, void* stream);
 
+/* ---------------------------------------------------------------- adjoint (gradients)
+ * Reverse-mode kernels of the smoke step with a per-step control force, for gradients of a
+ * loss on the final state; the reference has no differentiation, so none of these has a
+ * counterpart there. Fields have the MAC shapes of the forward operators; every lam_* output
+ * is ACCUMULATED (+=) unless stated, so the caller zeroes it first. */
+
+/* Forward control: u[j][i] += dt fu[j][i] (i < W), v[j][i] += dt fv[j][i] (j < H); fu, fv
+ * are H x W. */
+int sg_add_control(int dtype, int64_t H, int64_t W, void* u, int64_t ld_u, void* v, int64_t ld_v, const void* fu,
+                   int64_t ld_fu, const void* fv, int64_t ld_fv, double dt, void* stream);
+
+/* Workspace bytes of sg_adjoint_advect_scalar (gather = 1: the deterministic form). */
+int64_t sg_adjoint_advect_scalar_workspace(int dtype, int64_t H, int64_t W, int gather);
+/* Adjoint of sg_advect_scalar (cell-centred field advected by (u, v), then x dissipation):
+ * lam_src += transpose(interpolation) lam_out (gather = 0: atomicAdd scatter; 1:
+ * deterministic gather over the stored backtrace stencils), and lam_u / lam_v += the
+ * velocity part. `src` is the field that was advected. */
+int sg_adjoint_advect_scalar(int dtype, int64_t H, int64_t W, const void* lam_out, int64_t ld_lo, const void* src,
+                             int64_t ld_src, const void* u, int64_t ld_u, const void* v, int64_t ld_v, int mask_mode,
+                             const uint8_t* is_fluid, int64_t ld_fluid, double dt, double cell_size,
+                             double dissipation, void* lam_src, int64_t ld_ls, void* lam_u, int64_t ld_lu, void* lam_v,
+                             int64_t ld_lv, int gather, void* workspace, int64_t workspace_bytes, void* stream);
+/* Adjoint of sg_advect_velocity: (lam_u, lam_v) += adjoint w.r.t. the old (u, v) of the
+ * advected faces' adjoints (lam_u_new, lam_v_new); atomicAdd scatter. */
+int sg_adjoint_advect_velocity(int dtype, int64_t H, int64_t W, const void* lam_u_new, int64_t ld_lun,
+                               const void* lam_v_new, int64_t ld_lvn, const void* u, int64_t ld_u, const void* v,
+                               int64_t ld_v, int mask_mode, const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv,
+                               int64_t ld_fmv, double dt, double cell_size, void* lam_u, int64_t ld_lu, void* lam_v,
+                               int64_t ld_lv, void* stream);
+/* Adjoint of the density buoyancy term of sg_apply_forces (lam_d += ...) and of
+ * sg_add_control (grad_fu = dt lam_u[:, :W], grad_fv = dt lam_v[:H, :], written, either may
+ * be NULL). */
+int sg_adjoint_forces(int dtype, int64_t H, int64_t W, const void* lam_u, int64_t ld_lu, const void* lam_v,
+                      int64_t ld_lv, void* lam_d, int64_t ld_ld, void* grad_fu, int64_t ld_gu, void* grad_fv,
+                      int64_t ld_gv, double dt, double gravity, double density_coefficient, void* stream);
+/* Adjoint of sg_project: lam_u_out / lam_v_out = the identity part (written), lam_p =
+ * -s G^T lam (written), s = dt / (rho h). The pressure's adjoint then goes through the same
+ * Poisson solve (lam_div = solve(lam_p)) and sg_adjoint_divergence. */
+int sg_adjoint_project(int dtype, int64_t H, int64_t W, const void* lam_u, int64_t ld_lu, const void* lam_v,
+                       int64_t ld_lv, void* lam_u_out, int64_t ld_lou, void* lam_v_out, int64_t ld_lov, void* lam_p,
+                       int64_t ld_lp, int mask_mode, const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv,
+                       int64_t ld_fmv, int solid_mode, const uint8_t* solid, int64_t ld_s, double fluid_density,
+                       double cell_size, double dt, void* stream);
+/* Adjoint of sg_compute_divergence: (lam_u, lam_v) += D^T lam_div. */
+int sg_adjoint_divergence(int dtype, int64_t H, int64_t W, const void* lam_div, int64_t ld_ld, void* lam_u,
+                          int64_t ld_lu, void* lam_v, int64_t ld_lv, int mask_mode, const uint8_t* fmu, int64_t ld_fmu,
+                          const uint8_t* fmv, int64_t ld_fmv, double cell_size, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -67,6 +67,16 @@ SIGNATURES = {
     "sg_gmg_smooth_async": [P, I, I, P],
     "sg_gmg_fine_fused": [P],
     "sg_gmg_fine_kernel_async": [P, I, P, I64, P],
+    "sg_add_control": [I, I64, I64, P, I64, P, I64, P, I64, P, I64, D, P],
+    "sg_adjoint_advect_scalar_workspace": [I, I64, I64, I],
+    "sg_adjoint_advect_scalar": [I, I64, I64, P, I64, P, I64, P, I64, P, I64, I, P, I64, D, D, D, P, I64, P, I64, P,
+                                 I64, I, P, I64, P],
+    "sg_adjoint_advect_velocity": [I, I64, I64, P, I64, P, I64, P, I64, P, I64, I, P, I64, P, I64, D, D, P, I64, P,
+                                   I64, P],
+    "sg_adjoint_forces": [I, I64, I64, P, I64, P, I64, P, I64, P, I64, P, I64, D, D, D, P],
+    "sg_adjoint_project": [I, I64, I64, P, I64, P, I64, P, I64, P, I64, P, I64, I, P, I64, P, I64, I, P, I64, D, D,
+                           D, P],
+    "sg_adjoint_divergence": [I, I64, I64, P, I64, P, I64, P, I64, I, P, I64, P, I64, D, P],
     "sg_version": [],
     "sg_last_error": [],
     "sg_launch_count": [],
@@ -77,6 +87,7 @@ _RESTYPE = {
     "sg_gmg_plan_destroy": None,
     "sg_gmg_workspace_bytes": ctypes.c_int64,
     "sg_launch_count": ctypes.c_uint64,
+    "sg_adjoint_advect_scalar_workspace": ctypes.c_int64,
 }
 
 _lib = None

@@ -33,6 +33,12 @@ unsigned long long launch_count();
     if (!(cond)) return ::sg::fail(SG_ERR_ARG, __VA_ARGS__); \
   } while (0)
 
+#define SG_CHECK(x)            \
+  do {                         \
+    int _rc = (x);             \
+    if (_rc != SG_OK) return _rc; \
+  } while (0)
+
 #define SG_DISPATCH(dtype, ...)                                     \
   do {                                                              \
     if ((dtype) == SG_F32) {                                        \
@@ -86,6 +92,13 @@ struct Masks {
     return u(j, i) || u(j, i + 1) || v(j, i) || v(j + 1, i);
   }
 };
+
+// Solid cell test of boundaries.py:7-39 (plane: value 1; ring: the outermost cells).
+__device__ __forceinline__ bool solid_at(int mode, const uint8_t* s, int64_t ld, int H, int W, int j, int i) {
+  if (mode == SG_MASK_PLANES) return s[(int64_t)j * ld + i] == 1;
+  if (mode == SG_MASK_RING) return j == 0 || j == H - 1 || i == 0 || i == W - 1;
+  return false;
+}
 
 inline Masks make_masks(int mode, int64_t H, int64_t W, const uint8_t* fmu, int64_t ldu, const uint8_t* fmv,
                         int64_t ldv, const uint8_t* fl, int64_t ldf) {

@@ -239,12 +239,6 @@ __global__ void k_residual(int H, int W, const T* __restrict__ p, int64_t ldp, c
 }
 
 // ------------------------------------------------------------------ projection
-__device__ __forceinline__ bool solid_at(int mode, const uint8_t* s, int64_t ld, int H, int W, int j, int i) {
-  if (mode == SG_MASK_PLANES) return s[(int64_t)j * ld + i] == 1;
-  if (mode == SG_MASK_RING) return j == 0 || j == H - 1 || i == 0 || i == W - 1;
-  return false;
-}
-
 // pressure_gradient.py:4-37 then, if solid_mode != SG_MASK_NONE, boundaries.py:7-39.
 template <typename T>
 __global__ void k_project(int H, int W, T* __restrict__ u, int64_t ldu, T* __restrict__ v, int64_t ldv,
@@ -482,12 +476,6 @@ static int check_mask_mode(int mode, const void* a, const void* b) {
   if (mode == SG_MASK_OPEN || mode == SG_MASK_RING) return SG_OK;
   return fail(SG_ERR_ARG, "bad mask mode %d", mode);
 }
-
-#define SG_CHECK(x)            \
-  do {                         \
-    int _rc = (x);             \
-    if (_rc != SG_OK) return _rc; \
-  } while (0)
 
 // Ping-pong buffer of sg_jacobi_solve_noalloc: a fixed array in device memory, so the
 // entry point allocates nothing. Host code cannot use the name as a device address;
