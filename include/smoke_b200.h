@@ -338,6 +338,45 @@ int sg_adjoint_divergence(int dtype, int64_t H, int64_t W, const void* lam_div, 
                           int64_t ld_lu, void* lam_v, int64_t ld_lv, int mask_mode, const uint8_t* fmu, int64_t ld_fmu,
                           const uint8_t* fmv, int64_t ld_fmv, double cell_size, void* stream);
 
+/* ---------------------------------------------------------------- batched scenes
+ * Many independent default scenes (open box, solid ring, one overwriting plume, float32)
+ * of uneven sizes stepped together: one persistent launch per operator over a tile work
+ * list, the multigrid solve to a per-scene relative-residual tolerance, the whole step
+ * captured in a CUDA graph. The reference steps one scene per SmokeSimulation2D; these
+ * entries have no counterpart there. */
+typedef struct sg_batch sg_batch;
+
+/* n_scenes scenes of H[s] x W[s] cells; params: 10 doubles per scene (cell size, dt,
+ * fluid density, gravity, density buoyancy coefficient, plume cx, cy, radius (cells),
+ * plume density, plume v). Host only. */
+int sg_batch_create(sg_batch** out, int n_scenes, const int* H, const int* W, const double* params, double tol,
+                    int max_cycles, uint64_t seed);
+void sg_batch_destroy(sg_batch* batch);
+/* Device workspace the batch needs (fields, hierarchy, work lists, state). */
+int64_t sg_batch_workspace_bytes(const sg_batch* batch);
+/* Bind a zero-filled state in `workspace` (256-byte aligned) and build the step graphs. */
+int sg_batch_bind(sg_batch* batch, void* workspace, int64_t bytes, void* stream);
+/* Tile shape (index into sg_batch_tile_shape), smoother sweeps per side, cycle 0 V / 1 W. */
+int sg_batch_configure(sg_batch* batch, int tile, int sweeps, int wcycle);
+int sg_batch_tile_shape(int tile, int* tx, int* ty);
+/* Advance every scene by n_steps steps (graph launches on `stream`). */
+int sg_batch_step(sg_batch* batch, int n_steps, void* stream);
+/* Byte offsets into the workspace of scene s's current density (H x W), u (H x (W+1)),
+ * v ((H+1) x W) and pressure (H x W), float32, row stride = row length. */
+int sg_batch_layout(const sg_batch* batch, int scene, int64_t* off_density, int64_t* off_u, int64_t* off_v,
+                    int64_t* off_pressure);
+/* Which of the two field buffers holds the current state (0 / 1). */
+int sg_batch_current(const sg_batch* batch);
+int sg_batch_graph_nodes(const sg_batch* batch, int* step_nodes, int* cycle_nodes);
+/* Per-scene outcome of the last solve (host arrays, any may be NULL); synchronises. */
+int sg_batch_stats(sg_batch* batch, int* cycles, double* relres, long long* total_cycles, void* stream);
+/* Scratch bytes the autotuner needs for its snapshot of the state. */
+int64_t sg_batch_snapshot_bytes(const sg_batch* batch);
+/* Time `steps` steps of every (tile, sweeps in 1..2, V/W) candidate from the current state
+ * (restored each time), configure the fastest whose scenes all converged. */
+int sg_batch_autotune(sg_batch* batch, int steps, void* scratch, int64_t scratch_bytes, void* stream, int* tile,
+                      int* sweeps, int* wcycle, double* ms_per_step);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,7 +9,7 @@ include/smoke_b200.h); there is no CPU fallback.
 The package directory name is not a Python identifier; import it with
 ``importlib.import_module("python-game-engine_b200")``.
 """
-from . import _lib, adjoint, scenes
+from . import _lib, adjoint, batch, scenes
 from .config import Backend, GridConfig, OperatorBackendConfig, PressureSolverConfig, SimulationConfig
 from .operators import OPEN_BOX, RING_BOX, AnalyticMask, register_operators
 from .params import (DEFAULT_SOLVER_PARAMS, SOLVER_PARAM_TYPES, GaussSeidelParams, GeometricMultigridParams,

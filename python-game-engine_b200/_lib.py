@@ -77,6 +77,19 @@ SIGNATURES = {
     "sg_adjoint_project": [I, I64, I64, P, I64, P, I64, P, I64, P, I64, P, I64, I, P, I64, P, I64, I, P, I64, D, D,
                            D, P],
     "sg_adjoint_divergence": [I, I64, I64, P, I64, P, I64, P, I64, I, P, I64, P, I64, D, P],
+    "sg_batch_create": [P, I, P, P, P, D, I, U64],
+    "sg_batch_destroy": [P],
+    "sg_batch_workspace_bytes": [P],
+    "sg_batch_bind": [P, P, I64, P],
+    "sg_batch_configure": [P, I, I, I],
+    "sg_batch_tile_shape": [I, PI, PI],
+    "sg_batch_step": [P, I, P],
+    "sg_batch_layout": [P, I, P, P, P, P],
+    "sg_batch_current": [P],
+    "sg_batch_graph_nodes": [P, PI, PI],
+    "sg_batch_stats": [P, P, P, P, P],
+    "sg_batch_snapshot_bytes": [P],
+    "sg_batch_autotune": [P, I, P, I64, P, PI, PI, PI, PD],
     "sg_version": [],
     "sg_last_error": [],
     "sg_launch_count": [],
@@ -88,6 +101,9 @@ _RESTYPE = {
     "sg_gmg_workspace_bytes": ctypes.c_int64,
     "sg_launch_count": ctypes.c_uint64,
     "sg_adjoint_advect_scalar_workspace": ctypes.c_int64,
+    "sg_batch_destroy": None,
+    "sg_batch_workspace_bytes": ctypes.c_int64,
+    "sg_batch_snapshot_bytes": ctypes.c_int64,
 }
 
 _lib = None

@@ -41,11 +41,12 @@ __device__ __forceinline__ Stencil stencil_ref(int64_t rows, int64_t cols, doubl
   return s;
 }
 
+// The sample's value, rounded as sample_ref rounds it (corner differences in T).
 template <typename T>
 __device__ __forceinline__ double stencil_value(const T* __restrict__ f, int64_t ld, const Stencil& s) {
-  const double c00 = (double)f[(int64_t)s.y0 * ld + s.x0], c10 = (double)f[(int64_t)s.y0 * ld + s.x1];
-  const double c01 = (double)f[(int64_t)s.y1 * ld + s.x0], c11 = (double)f[(int64_t)s.y1 * ld + s.x1];
-  const double c0 = c00 + (c10 - c00) * s.tx, c1 = c01 + (c11 - c01) * s.tx;
+  const T c00 = f[(int64_t)s.y0 * ld + s.x0], c10 = f[(int64_t)s.y0 * ld + s.x1];
+  const T c01 = f[(int64_t)s.y1 * ld + s.x0], c11 = f[(int64_t)s.y1 * ld + s.x1];
+  const double c0 = lerp_ref(c00, c10, s.tx), c1 = lerp_ref(c01, c11, s.tx);
   return c0 + (c1 - c0) * s.ty;
 }
 
@@ -53,11 +54,11 @@ __device__ __forceinline__ double stencil_value(const T* __restrict__ f, int64_t
 template <typename T>
 __device__ __forceinline__ void stencil_grad(const T* __restrict__ f, int64_t ld, const Stencil& s, double& gx,
                                              double& gy) {
-  const double c00 = (double)f[(int64_t)s.y0 * ld + s.x0], c10 = (double)f[(int64_t)s.y0 * ld + s.x1];
-  const double c01 = (double)f[(int64_t)s.y1 * ld + s.x0], c11 = (double)f[(int64_t)s.y1 * ld + s.x1];
-  gx = (c10 - c00) * (1.0 - s.ty) + (c11 - c01) * s.ty;
-  const double c0 = c00 + (c10 - c00) * s.tx, c1 = c01 + (c11 - c01) * s.tx;
-  gy = c1 - c0;
+  const T c00 = f[(int64_t)s.y0 * ld + s.x0], c10 = f[(int64_t)s.y0 * ld + s.x1];
+  const T c01 = f[(int64_t)s.y1 * ld + s.x0], c11 = f[(int64_t)s.y1 * ld + s.x1];
+  const T d0 = c10 - c00, d1 = c11 - c01;
+  gx = (double)d0 * (1.0 - s.ty) + (double)d1 * s.ty;
+  gy = lerp_ref(c01, c11, s.tx) - lerp_ref(c00, c10, s.tx);
 }
 
 // lam_f[corners] += lam * weights (the transpose of one sample).

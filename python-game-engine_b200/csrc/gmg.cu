@@ -763,6 +763,17 @@ static bool coarsest_pinv(const std::vector<uint8_t>& code, int H, int W, std::v
   return true;
 }
 
+// Pseudo-inverse of the open-box operator on an H x W grid (every cell fluid, every
+// interior face open); used by the batched solver for its scenes' coarsest levels.
+bool open_box_pinv(int H, int W, std::vector<double>& out) {
+  std::vector<uint8_t> fl((size_t)H * W, 1), fu((size_t)H * (W + 1), 0), fv((size_t)(H + 1) * W, 0);
+  for (int j = 0; j < H; ++j)
+    for (int i = 1; i < W; ++i) fu[(size_t)j * (W + 1) + i] = 1;
+  for (int j = 1; j < H; ++j)
+    for (int i = 0; i < W; ++i) fv[(size_t)j * W + i] = 1;
+  return coarsest_pinv(pack_codes(fl, fu, fv, H, W), H, W, out);
+}
+
 static LevelMask level_mask(const sg_gmg_plan* p, int k) {
   const Level& L = p->levels[k];
   LevelMask m;

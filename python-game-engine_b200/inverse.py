@@ -51,7 +51,7 @@ def fd_check(n, steps, n_entries, eps=1e-6, seed=11):
              "strong": [tuple(int(x) for x in strong[rng.integers(0, len(strong))]) for _ in range(n_entries)]}
     out = {"entries_per_set": n_entries, "eps": eps, "loss": loss0, "grad_max": gmax}
     for name, idx in picks.items():
-        rel, worst = [], None
+        rel, resolved, worst = [], [], None
         for k in idx:
             fp, fm = force.clone(), force.clone()
             fp[k] += eps
@@ -61,10 +61,14 @@ def fd_check(n, steps, n_entries, eps=1e-6, seed=11):
             an = float(g[k])
             r = abs(fd - an) / max(abs(fd), abs(an), 1e-30)
             rel.append(r)
+            if max(abs(fd), abs(an)) >= 1e-3 * gmax:
+                resolved.append(r)
             if worst is None or r > worst[0]:
                 worst = (r, fd, an)
         out[name] = {"max_rel_err": max(rel), "median_rel_err": float(np.median(rel)),
-                     "worst": {"fd": worst[1], "adjoint": worst[2]}}
+                     "worst": {"fd": worst[1], "adjoint": worst[2]},
+                     "entries_above_1e-3_of_max": len(resolved),
+                     "max_rel_err_above_1e-3_of_max": max(resolved) if resolved else None}
     return out
 
 
