@@ -367,6 +367,8 @@ int sg_batch_layout(const sg_batch* batch, int scene, int64_t* off_density, int6
                     int64_t* off_pressure);
 /* Which of the two field buffers holds the current state (0 / 1). */
 int sg_batch_current(const sg_batch* batch);
+/* Cycle-loop iterations (one per cycle of all scenes together) since bind; synchronises. */
+int sg_batch_loops(sg_batch* batch, long long* loops, void* stream);
 int sg_batch_graph_nodes(const sg_batch* batch, int* step_nodes, int* cycle_nodes);
 /* Per-scene outcome of the last solve (host arrays, any may be NULL); synchronises. */
 int sg_batch_stats(sg_batch* batch, int* cycles, double* relres, long long* total_cycles, void* stream);

@@ -86,6 +86,7 @@ SIGNATURES = {
     "sg_batch_step": [P, I, P],
     "sg_batch_layout": [P, I, P, P, P, P],
     "sg_batch_current": [P],
+    "sg_batch_loops": [P, P, P],
     "sg_batch_graph_nodes": [P, PI, PI],
     "sg_batch_stats": [P, P, P, P, P],
     "sg_batch_snapshot_bytes": [P],

@@ -94,6 +94,12 @@ class BatchedSmoke:
                t.ctypes.data_as(ctypes.c_void_p), L.stream_ptr())
         return c, r, t
 
+    def loops(self):
+        """Cycle-loop iterations (all scenes together) run since bind."""
+        n = ctypes.c_longlong(0)
+        L.call("sg_batch_loops", self.handle, ctypes.byref(n), L.stream_ptr())
+        return n.value
+
     def graph_nodes(self):
         a, b = ctypes.c_int(0), ctypes.c_int(0)
         L.call("sg_batch_graph_nodes", self.handle, ctypes.byref(a), ctypes.byref(b))

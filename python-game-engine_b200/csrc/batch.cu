@@ -72,6 +72,7 @@ struct BPools {
 struct BCtl {
   double tol;
   int max_cycles, n_scenes, any, steps;
+  long long loops;  // cycle-loop iterations run since bind (all scenes together)
 };
 
 __device__ __forceinline__ Masks open_masks(int H, int W) {
@@ -463,6 +464,7 @@ __global__ void k_b_after_cycle(BPools P, BCtl* ctl, cudaGraphConditionalHandle 
   any = __syncthreads_or(any);
   if (threadIdx.x == 0) {
     ctl->any = any;
+    ctl->loops += 1;
     if (use_handle) cudaGraphSetConditional(h, any ? 1u : 0u);
   }
 }
@@ -946,6 +948,15 @@ int sg_batch_step(sg_batch* b, int n_steps, void* stream) {
 }
 
 int sg_batch_current(const sg_batch* b) { return b ? b->cur : -1; }
+
+// Cycle-loop iterations (one per cycle of all scenes together) run since bind; synchronises.
+int sg_batch_loops(sg_batch* b, long long* loops, void* stream) {
+  SG_REQUIRE(b && b->ws && loops, "batch not bound");
+  cudaStream_t s = as_stream(stream);
+  SG_BTRY(cudaMemcpyAsync(loops, &ctl_ptr(b)->loops, sizeof(long long), cudaMemcpyDeviceToHost, s), "loops");
+  SG_BTRY(cudaStreamSynchronize(s), "loops");
+  return SG_OK;
+}
 
 int sg_batch_graph_nodes(const sg_batch* b, int* step_nodes, int* cycle_nodes) {
   SG_REQUIRE(b && step_nodes && cycle_nodes, "null pointer");

@@ -35,12 +35,13 @@ def _final_density(model, force):
     return d
 
 
-def fd_check(n, steps, n_entries, eps=1e-6, seed=11):
+def fd_check(n, steps, n_entries, eps=(1e-6, 1e-4), seed=11):
     """Central differences of the loss on `n_entries` control entries drawn uniformly and on
-    as many drawn from the entries whose adjoint gradient is at least 1 % of the largest.
-    The difference L(f + eps) - L(f - eps) is summed cell by cell as
-    (d+ - d-) (d+ + d- - 2 target), the same number without the cancellation of two
-    losses of ~1e3 (which would bury gradients below ~1e-6)."""
+    as many drawn from the entries whose adjoint gradient is at least 1 % of the largest,
+    for each step size in `eps`. The difference L(f + e) - L(f - e) is summed cell by cell
+    as (d+ - d-) (d+ + d- - 2 target), the same number without the cancellation of two
+    losses of ~1e3. What remains at e = 1e-6 is the rounding of the FP64 rollouts, which
+    the pressure solves amplify by their condition number (~3e4 at 256^2)."""
     model, force, target = A.inverse_problem(n=n, steps=steps, dtype=torch.float64, precision="fp64",
                                              fixed_cycles=30, exact_forces=True, adjoint_advection="gather")
     loss0, g = A.loss_and_grad(model, force, target)
@@ -49,26 +50,27 @@ def fd_check(n, steps, n_entries, eps=1e-6, seed=11):
     strong = torch.nonzero(g.abs() >= 0.01 * gmax).cpu().numpy()
     picks = {"uniform": [tuple(int(rng.integers(0, s)) for s in force.shape) for _ in range(n_entries)],
              "strong": [tuple(int(x) for x in strong[rng.integers(0, len(strong))]) for _ in range(n_entries)]}
-    out = {"entries_per_set": n_entries, "eps": eps, "loss": loss0, "grad_max": gmax}
-    for name, idx in picks.items():
-        rel, resolved, worst = [], [], None
-        for k in idx:
-            fp, fm = force.clone(), force.clone()
-            fp[k] += eps
-            fm[k] -= eps
-            dp, dm = _final_density(model, fp), _final_density(model, fm)
-            fd = float(((dp - dm) * (dp + dm - 2 * target)).sum()) / (2 * eps)
-            an = float(g[k])
-            r = abs(fd - an) / max(abs(fd), abs(an), 1e-30)
-            rel.append(r)
-            if max(abs(fd), abs(an)) >= 1e-3 * gmax:
-                resolved.append(r)
-            if worst is None or r > worst[0]:
-                worst = (r, fd, an)
-        out[name] = {"max_rel_err": max(rel), "median_rel_err": float(np.median(rel)),
-                     "worst": {"fd": worst[1], "adjoint": worst[2]},
-                     "entries_above_1e-3_of_max": len(resolved),
-                     "max_rel_err_above_1e-3_of_max": max(resolved) if resolved else None}
+    out = {"entries_per_set": n_entries, "loss": loss0, "grad_max": gmax}
+    for e in eps:
+        for name, idx in picks.items():
+            rel, resolved, worst = [], [], None
+            for k in idx:
+                fp, fm = force.clone(), force.clone()
+                fp[k] += e
+                fm[k] -= e
+                dp, dm = _final_density(model, fp), _final_density(model, fm)
+                fd = float(((dp - dm) * (dp + dm - 2 * target)).sum()) / (2 * e)
+                an = float(g[k])
+                r = abs(fd - an) / max(abs(fd), abs(an), 1e-30)
+                rel.append(r)
+                if max(abs(fd), abs(an)) >= 1e-3 * gmax:
+                    resolved.append(r)
+                if worst is None or r > worst[0]:
+                    worst = (r, fd, an)
+            out[f"eps={e:g} {name}"] = {
+                "max_rel_err": max(rel), "median_rel_err": float(np.median(rel)),
+                "worst": {"fd": worst[1], "adjoint": worst[2]}, "entries_above_1e-3_of_max": len(resolved),
+                "max_rel_err_above_1e-3_of_max": max(resolved) if resolved else None}
     return out
 
 
