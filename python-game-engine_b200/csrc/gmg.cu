@@ -324,10 +324,7 @@ __global__ void k_gmg_finalize_norm(const double* __restrict__ partial, int n, G
 
 // Relative residual after the prologue (body = 0) or a cycle (body = 1); decides whether
 // the WHILE node runs another cycle (when use_handle) and records the status.
-__global__ void k_gmg_finalize_rel(const double* __restrict__ partial, int n, GmgState* st, cudaGraphConditionalHandle h,
-                                   int use_handle, int body) {
-  double s = sum_partials(partial, n);
-  if (threadIdx.x != 0) return;
+__device__ void finalize_rel_state(double s, GmgState* st, cudaGraphConditionalHandle h, int use_handle, int body) {
   double nb = st->bnorm;
   double rel = sqrt(s);
   if (!(nb == nb) || isinf(nb)) rel = nb + rel;  // a non-finite ||b|| makes the ratio non-finite
@@ -344,6 +341,12 @@ __global__ void k_gmg_finalize_rel(const double* __restrict__ partial, int n, Gm
   st->status = status;
   if (status >= 2) st->failures += 1;
   if (use_handle) cudaGraphSetConditional(h, status == 0 ? 1u : 0u);
+}
+
+__global__ void k_gmg_finalize_rel(const double* __restrict__ partial, int n, GmgState* st, cudaGraphConditionalHandle h,
+                                   int use_handle, int body) {
+  double s = sum_partials(partial, n);
+  if (threadIdx.x == 0) finalize_rel_state(s, st, h, use_handle, body);
 }
 
 // ---------------------------------------------------------------- single-block tail
@@ -943,7 +946,7 @@ static void launch_post_reg(const sg_gmg_plan* p, int k, cudaStream_t s) {
 // Grid of the fused fine-level post kernel (also the number of its partial sums).
 template <typename TC>
 static dim3 post_final_grid(const sg_gmg_plan* p) {
-  constexpr int RPT = RegShape<TC>::RPT, NW = RegShape<TC>::NWARP;
+  constexpr int RPT = RegShape<TC>::RPT_FINAL, NW = RegShape<TC>::NWARP_FINAL;
   const int sw = p->post < 1 ? 1 : (p->post > 3 ? 3 : p->post);
   const int halo = 2 * sw + 2, txo = kRW - 2 * halo, tyo = NW * RPT - 2 * halo;
   const Level& L = p->levels[0];
@@ -952,7 +955,7 @@ static dim3 post_final_grid(const sg_gmg_plan* p) {
 
 template <typename TC, typename TP, int SW>
 static void launch_post_final(const sg_gmg_plan* p, TP* pp, int64_t ldp, cudaStream_t s) {
-  constexpr int RPT = RegShape<TC>::RPT, NW = RegShape<TC>::NWARP, MB = RegShape<TC>::MINB_FINAL;
+  constexpr int RPT = RegShape<TC>::RPT_FINAL, NW = RegShape<TC>::NWARP_FINAL, MB = RegShape<TC>::MINB_FINAL;
   const Level& L = p->levels[0];
   const Level& C = p->levels[1];
   TP* r64 = p->off_r64 ? (TP*)(p->ws + p->off_r64) : nullptr;

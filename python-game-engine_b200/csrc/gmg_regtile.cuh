@@ -539,13 +539,26 @@ __global__ void __launch_bounds__(32 * NWARP, MINB)
 #ifndef SG_REG_FINAL_MINB
 #define SG_REG_FINAL_MINB 4
 #endif
-template <int R, int N, int M>
+// the fused fine-level post kernel's rows per thread and warps (measured: 6 x 8 for FP32
+// cycles, the level kernels' 4 x 8 for FP64)
+#ifndef SG_REG_FINAL_F32_RPT
+#define SG_REG_FINAL_F32_RPT 6
+#define SG_REG_FINAL_F32_NWARP 8
+#endif
+#ifndef SG_REG_FINAL_F64_RPT
+#define SG_REG_FINAL_F64_RPT SG_REG_F64_RPT
+#define SG_REG_FINAL_F64_NWARP SG_REG_F64_NWARP
+#endif
+template <int R, int N, int M, int RF, int NF>
 struct RegShapeOf {
   static constexpr int RPT = R, NWARP = N, MINB = M, MINB_FINAL = SG_REG_FINAL_MINB;
+  static constexpr int RPT_FINAL = RF, NWARP_FINAL = NF;
 };
 template <typename T>
 struct RegShape;
 template <>
-struct RegShape<float> : RegShapeOf<SG_REG_F32_RPT, SG_REG_F32_NWARP, SG_REG_F32_MINB> {};
+struct RegShape<float> : RegShapeOf<SG_REG_F32_RPT, SG_REG_F32_NWARP, SG_REG_F32_MINB, SG_REG_FINAL_F32_RPT,
+                                    SG_REG_FINAL_F32_NWARP> {};
 template <>
-struct RegShape<double> : RegShapeOf<SG_REG_F64_RPT, SG_REG_F64_NWARP, SG_REG_F64_MINB> {};
+struct RegShape<double> : RegShapeOf<SG_REG_F64_RPT, SG_REG_F64_NWARP, SG_REG_F64_MINB, SG_REG_FINAL_F64_RPT,
+                                     SG_REG_FINAL_F64_NWARP> {};

@@ -3,8 +3,9 @@
 //
 // When every level from the tail's first one down to the coarsest is an open box, one
 // block of 1024 threads runs the whole rest of the cycle in shared memory: the levels up
-// to 64 cells a side cost a few barriers each here, against two grid launches apiece in
-// the tiled kernels. Each level keeps
+// to 16 cells a side (measured best on B200: at 32^2 and 64^2 one SM's issue rate makes
+// the block slower than two 16 x 16-tiled launches per level) cost a few barriers each
+// here. Each level keeps
 //   e: two colour planes of (H + 2) x (Wh + 2) (Wh = ceil(W / 2)), cell (j, i) of colour
 //      c = (i + j) & 1 at plane c, row j + 1, column (i >> 1) + 1; the ring and the
 //      slot past an odd row end stay 0, so out-of-grid neighbours read 0;
@@ -15,7 +16,10 @@
 // with a bit mask recording which W-cycle levels already made their first coarse visit.
 #pragma once
 
-constexpr int kOpenTailMaxSide = 64;
+#ifndef SG_OPEN_TAIL_MAX_SIDE
+#define SG_OPEN_TAIL_MAX_SIDE 16
+#endif
+constexpr int kOpenTailMaxSide = SG_OPEN_TAIL_MAX_SIDE;
 #ifndef SG_OPEN_TAIL_THREADS
 #define SG_OPEN_TAIL_THREADS 1024
 #endif
