@@ -253,6 +253,11 @@ int sg_gmg_bind(sg_gmg_plan* plan, void* workspace, void* stream);
  * the device after every cycle. Read the outcome with sg_gmg_stats. */
 int sg_gmg_solve_async(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div, int div_dtype,
                        double alpha, double tol, int max_cycles, void* stream);
+/* As sg_gmg_solve_async from the initial guess p = 0: p is written, never read (the
+ * reference zeroes the pressure before every solve, simulation.py:310; this saves the
+ * first residual pass). */
+int sg_gmg_solve_from_zero_async(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div,
+                                 int div_dtype, double alpha, double tol, int max_cycles, void* stream);
 /* Outcome of the last solve (synchronises stream): cycles run, last relative residual,
  * status (1 converged, 2 cycle cap reached, 3 non-finite residual) and the number of
  * cycles run by all solves since sg_gmg_bind. Any output may be NULL. */

@@ -56,6 +56,7 @@ SIGNATURES = {
     "sg_gmg_num_levels": [P],
     "sg_gmg_bind": [P, P, P],
     "sg_gmg_solve_async": [P, P, I64, P, I64, I, D, D, I, P],
+    "sg_gmg_solve_from_zero_async": [P, P, I64, P, I64, I, D, D, I, P],
     "sg_gmg_stats": [P, PI, PD, PI, ctypes.POINTER(ctypes.c_longlong), P],
     "sg_gmg_counters": [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                         ctypes.POINTER(ctypes.c_longlong), P],

@@ -257,9 +257,12 @@ __global__ void k_gmg_fine_residual(int H, int W, const T* __restrict__ p, int64
 }
 
 // bf = alpha * div on fluid cells (alpha from the solve state) plus per-block sums of bf^2.
-template <typename TD, typename TB>
+// For a zero initial guess (pz non-null) it also writes p = 0 and, bf being the residual,
+// the first cycle's rhs b0 (cycle precision) and the carried residual r64 (when kept).
+template <typename TD, typename TB, typename TC>
 __global__ void k_gmg_rhs(int H, int W, const TD* __restrict__ div, int64_t ldd, const GmgState* __restrict__ st,
-                          LevelMask m, TB* __restrict__ b, int64_t ldb, double* __restrict__ partial) {
+                          LevelMask m, TB* __restrict__ b, int64_t ldb, double* __restrict__ partial,
+                          TB* __restrict__ pz, int64_t ldpz, TC* __restrict__ b0, int64_t ld0, TB* __restrict__ r64) {
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int ib = blockIdx.x * kWX + threadIdx.x;
   const double alpha = st->alpha;
@@ -275,6 +278,11 @@ __global__ void k_gmg_rhs(int H, int W, const TD* __restrict__ div, int64_t ldd,
           sq += (double)v * (double)v;
         }
         b[(int64_t)j * ldb + i] = v;
+        if (pz) {
+          pz[(int64_t)j * ldpz + i] = (TB)0;
+          b0[(int64_t)j * ld0 + i] = (TC)v;
+          if (r64) r64[(int64_t)j * ld0 + i] = v;
+        }
       }
     }
   }
@@ -642,6 +650,7 @@ struct sg_gmg_plan {
   const void* g_div = nullptr;
   int64_t g_ldp = 0, g_ldd = 0;
   int g_div_dtype = -1;
+  int g_zero = 0;
   int prologue_nodes = 0, body_nodes = 0;
 };
 
@@ -1051,21 +1060,28 @@ static void cycle(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
 }
 
 // Prologue: bf = alpha div, ||bf||, r0 = bf - A p -> cycle rhs, relres0 and the loop condition.
+// zero_guess: p is not read; it starts at 0 (written here), so the first residual is bf.
 template <typename TP, typename TD, typename TC>
-static void prologue(const sg_gmg_plan* p, const TP* pp, int64_t ldp, const TD* div, int64_t ldd,
-                     cudaGraphConditionalHandle h, int use_handle, cudaStream_t s) {
+static void prologue(const sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div, int64_t ldd,
+                     cudaGraphConditionalHandle h, int use_handle, cudaStream_t s, bool zero_guess = false) {
   const Level& L = p->levels[0];
   LevelMask m = level_mask(p, 0);
   double* part = (double*)(p->ws + p->off_partial);
   GmgState* st = state_ptr(p);
   dim3 g = grid_wide(L.W, L.H);
   TP* bf = (TP*)(p->ws + p->off_bfine);
-  SG_LAUNCH(k_gmg_rhs<TD, TP><<<g, block2d(), 0, s>>>(L.H, L.W, div, ldd, st, m, bf, p->ld_bfine, part));
+  TP* r64 = p->off_r64 ? (TP*)(p->ws + p->off_r64) : nullptr;
+  SG_LAUNCH(k_gmg_rhs<TD, TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, div, ldd, st, m, bf, p->ld_bfine, part,
+                                                          zero_guess ? pp : nullptr, ldp, ws_ptr<TC>(p, L.off_b), L.ld,
+                                                          r64));
   SG_LAUNCH(k_gmg_finalize_norm<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st));
+  if (zero_guess) {
+    SG_LAUNCH(k_gmg_finalize_rel<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st, h, use_handle, 0));
+    return;
+  }
   SG_LAUNCH(k_gmg_fine_residual<TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, pp, ldp, bf, p->ld_bfine, m,
                                                                    ws_ptr<TC>(p, L.off_b), L.ld,
-                                                                   p->off_r64 ? (TP*)(p->ws + p->off_r64) : nullptr,
-                                                                   part));
+                                                                   r64, part));
   SG_LAUNCH(k_gmg_finalize_rel<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st, h, use_handle, 0));
 }
 
@@ -1116,7 +1132,7 @@ static unsigned long long counter() { return launch_count(); }
 
 // Capture prologue + WHILE(body) into one executable graph for these pointers.
 template <typename TP, typename TD, typename TC>
-static int build_graph(sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div, int64_t ldd) {
+static int build_graph(sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div, int64_t ldd, bool zero_guess) {
   if (p->exec) {
     cudaGraphExecDestroy(p->exec);
     p->exec = nullptr;
@@ -1130,7 +1146,7 @@ static int build_graph(sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div, int64
   SG_CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
               "begin capture");
   unsigned long long c0 = counter();
-  prologue<TP, TD, TC>(p, pp, ldp, div, ldd, h, 1, cs);
+  prologue<TP, TD, TC>(p, pp, ldp, div, ldd, h, 1, cs, zero_guess);
   unsigned long long c1 = counter();
   cudaStreamCaptureStatus cst;
   cudaGraph_t cg = nullptr;
@@ -1164,15 +1180,17 @@ static int build_graph(sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div, int64
   p->g_div = div;
   p->g_ldd = ldd;
   p->g_div_dtype = sizeof(TD) == 4 ? SG_F32 : SG_F64;
+  p->g_zero = zero_guess ? 1 : 0;
   return SG_OK;
 }
 
 template <typename TP, typename TD, typename TC>
 static int solve_async_impl(sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div, int64_t ldd, double alpha, double tol,
-                            int max_cycles, cudaStream_t s) {
+                            int max_cycles, cudaStream_t s, bool zero_guess) {
   int dd = sizeof(TD) == 4 ? SG_F32 : SG_F64;
-  if (!p->exec || p->g_p != pp || p->g_ldp != ldp || p->g_div != div || p->g_ldd != ldd || p->g_div_dtype != dd) {
-    int rc = build_graph<TP, TD, TC>(p, pp, ldp, div, ldd);
+  if (!p->exec || p->g_p != pp || p->g_ldp != ldp || p->g_div != div || p->g_ldd != ldd || p->g_div_dtype != dd ||
+      p->g_zero != (zero_guess ? 1 : 0)) {
+    int rc = build_graph<TP, TD, TC>(p, pp, ldp, div, ldd, zero_guess);
     if (rc != SG_OK) return rc;
   }
   SG_LAUNCH(k_gmg_set_params<<<1, 1, 0, s>>>(state_ptr(p), alpha, tol, max_cycles));
@@ -1196,8 +1214,9 @@ static int cycles_eager_impl(sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div,
 
 template <typename TP, typename TD, typename TC>
 static int solve_async_typed(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div, double alpha,
-                             double tol, int max_cycles, cudaStream_t s) {
-  return solve_async_impl<TP, TD, TC>(plan, (TP*)p, ld_p, (const TD*)div, ld_div, alpha, tol, max_cycles, s);
+                             double tol, int max_cycles, cudaStream_t s, bool zero_guess) {
+  return solve_async_impl<TP, TD, TC>(plan, (TP*)p, ld_p, (const TD*)div, ld_div, alpha, tol, max_cycles, s,
+                                      zero_guess);
 }
 
 template <typename TP, typename TD, typename TC>
@@ -1448,7 +1467,16 @@ int sg_gmg_solve_async(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div
   if (rc != SG_OK) return rc;
   SG_REQUIRE(max_cycles >= 0 && max_cycles < kHist, "max_cycles must be in 0..%d", kHist - 1);
   cudaStream_t s = as_stream(stream);
-  SG_GMG_TYPED(solve_async_typed, plan, p, ld_p, div, ld_div, alpha, tol, max_cycles, s);
+  SG_GMG_TYPED(solve_async_typed, plan, p, ld_p, div, ld_div, alpha, tol, max_cycles, s, false);
+}
+
+int sg_gmg_solve_from_zero_async(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div,
+                                 int div_dtype, double alpha, double tol, int max_cycles, void* stream) {
+  int rc = check_solve_args(plan, p, ld_p, div, ld_div, div_dtype);
+  if (rc != SG_OK) return rc;
+  SG_REQUIRE(max_cycles >= 0 && max_cycles < kHist, "max_cycles must be in 0..%d", kHist - 1);
+  cudaStream_t s = as_stream(stream);
+  SG_GMG_TYPED(solve_async_typed, plan, p, ld_p, div, ld_div, alpha, tol, max_cycles, s, true);
 }
 
 int sg_gmg_stats(sg_gmg_plan* plan, int* cycles, double* relres, int* status, long long* total_cycles, void* stream) {

@@ -387,7 +387,8 @@ class SmokeSimulation2D:
     def _solve_pressure(self):
         fmu, fmv, _ = self._kmasks
         self.pressure.zero_()
-        solve_pressure(self.pressure, self.divergence, fmu, fmv, self.fluid_density, self.cell_size, self.dt, self)
+        solve_pressure(self.pressure, self.divergence, fmu, fmv, self.fluid_density, self.cell_size, self.dt, self,
+                       zero_initial_guess=True)
 
     def _apply_pressure_gradient(self, dt):
         fmu, fmv, _ = self._kmasks

@@ -255,12 +255,13 @@ class GMGPlan:
             L._lib.sg_gmg_plan_destroy(h)
             self.handle = None
 
-    def solve_async(self, pressure, divergence, alpha, tol, max_cycles):
-        """Graph solve without host synchronisation (outcome: stats())."""
+    def solve_async(self, pressure, divergence, alpha, tol, max_cycles, zero_guess=False):
+        """Graph solve without host synchronisation (outcome: stats()). zero_guess: start
+        from p = 0 without reading `pressure` (it is only written)."""
         p, ldp = L.field(pressure, "pressure")
         d, ldd = L.field(divergence, "divergence")
-        L.call("sg_gmg_solve_async", self.handle, p, ldp, d, ldd, L.dtype_code(divergence), float(alpha), float(tol),
-               int(max_cycles), L.stream_ptr())
+        L.call("sg_gmg_solve_from_zero_async" if zero_guess else "sg_gmg_solve_async", self.handle, p, ldp, d, ldd,
+               L.dtype_code(divergence), float(alpha), float(tol), int(max_cycles), L.stream_ptr())
 
     def stats(self):
         """(cycles, relres, status, total_cycles) of the last solve; synchronises the stream."""
@@ -361,7 +362,8 @@ class GeometricMultigridSolver:
 
     def __call__(self, pressure, divergence, face_mask_u, face_mask_v, fluid_density, cell_size, dt, tol=1e-6,
                  max_cycles=50, cycle="V", pre_sweeps=2, post_sweeps=2, omega=1.4, coarsest=8, precision="fp64",
-                 check_every=1, fixed_cycles=0, rebuild_masks=False, strict=False, **_ignored):
+                 check_every=1, fixed_cycles=0, rebuild_masks=False, strict=False, zero_initial_guess=False,
+                 **_ignored):
         H, W = pressure.shape
         plan = self.plan_for(H, W, face_mask_u, face_mask_v, pressure.device, coarsest, omega, pre_sweeps, post_sweeps,
                              cycle, precision, rebuild_masks)
@@ -374,7 +376,8 @@ class GeometricMultigridSolver:
             if p is None:
                 p = torch.empty((H, W), dtype=want, device=pressure.device)
                 self._buffers = {key: p}
-            p.copy_(pressure)
+            if not zero_initial_guess or fixed_cycles:
+                p.copy_(pressure)
         alpha = calculate_alpha(cell_size, fluid_density, dt)
         self._pending = None
         if fixed_cycles and fixed_cycles > 0:
@@ -383,7 +386,7 @@ class GeometricMultigridSolver:
             plan.cycles_async(p, divergence, alpha, fixed_cycles, self.last_relres_dev)
             self._last = (fixed_cycles, None, None)
         else:
-            plan.solve_async(p, divergence, alpha, tol, max_cycles)
+            plan.solve_async(p, divergence, alpha, tol, max_cycles, zero_guess=bool(zero_initial_guess))
             self._pending = plan
             if strict:
                 cycles, rel, ok = self._outcome()
@@ -395,10 +398,13 @@ class GeometricMultigridSolver:
 
 
 # ---------------------------------------------------------------- dispatch + registration
-def solve_pressure(pressure, divergence, face_mask_u, face_mask_v, fluid_density, cell_size, dt, params):
-    """solvers/dispatch.py:5-12: look up (method, backend) and call with the params as kwargs."""
+def solve_pressure(pressure, divergence, face_mask_u, face_mask_v, fluid_density, cell_size, dt, params, **hints):
+    """solvers/dispatch.py:5-12: look up (method, backend) and call with the params as kwargs.
+    ``hints`` (e.g. zero_initial_guess=True from a caller that just zeroed the pressure) are
+    passed along; solvers that do not use them ignore them."""
     fn = get_solver(params.pressure_solver_method, params.pressure_solver_backend)
     kwargs = asdict(params.solver_params)
+    kwargs.update(hints)
     fn(pressure, divergence, face_mask_u, face_mask_v, fluid_density, cell_size, dt,
        profiler=getattr(params, "profiler", None), **kwargs)
 
