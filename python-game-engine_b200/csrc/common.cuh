@@ -62,6 +62,16 @@ inline dim3 grid2d(int64_t cols, int64_t rows) {
 }
 inline dim3 block2d() { return dim3(kBX, kBY); }
 
+// Row-blocked launches: each thread takes kRows cells of one column, kBY rows apart (a
+// warp still reads one contiguous row segment per access), so a thread keeps several
+// independent loads in flight.
+constexpr int kRows = 4;
+inline dim3 grid2d_rows(int64_t cols, int64_t rows) {
+  return dim3((unsigned)((cols + kBX - 1) / kBX), (unsigned)((rows + kBY * kRows - 1) / (kBY * kRows)));
+}
+// j of the thread's q-th row in a row-blocked launch
+__device__ __forceinline__ int row_of(int q) { return (blockIdx.y * kRows + q) * blockDim.y + threadIdx.y; }
+
 // ------------------------------------------------------------------ masks
 // Face/fluid masks of an H x W cell grid, either explicit planes (as the reference
 // passes them) or analytic: SG_MASK_OPEN (all interior faces open) or SG_MASK_RING

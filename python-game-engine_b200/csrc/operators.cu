@@ -53,10 +53,15 @@ __global__ void k_advect_scalar(int H, int W, const T* __restrict__ src, int64_t
                                 const T* __restrict__ u, int64_t ur, int64_t uc, int64_t ldu,
                                 const T* __restrict__ v, int64_t vr, int64_t vc, int64_t ldv, Masks m,
                                 double dt, double inv, T diss) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= W || j >= H) return;
-  dst[(int64_t)j * ldd + i] = advect_scalar_cell(j, i, H, W, src, lds, u, ur, uc, ldu, v, vr, vc, ldv, m, dt, inv, diss);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= W) return;
+#pragma unroll
+  for (int q = 0; q < kRows; ++q) {
+    const int j = row_of(q);
+    if (j < H)
+      dst[(int64_t)j * ldd + i] =
+          advect_scalar_cell(j, i, H, W, src, lds, u, ur, uc, ldu, v, vr, vc, ldv, m, dt, inv, diss);
+  }
 }
 
 template <typename T>
@@ -82,8 +87,10 @@ template <typename T>
 __global__ void k_advect_uv(int H, int W, const T* __restrict__ us, int64_t ldus, T* __restrict__ ud, int64_t ldud,
                             const T* __restrict__ vs, int64_t ldvs, T* __restrict__ vd, int64_t ldvd, Masks m,
                             double dt, double inv) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+  for (int q = 0; q < kRows; ++q) {
+  const int j = row_of(q);
   if (j < H && i <= W)
     ud[(int64_t)j * ldud + i] =
         m.u(j, i) ? advect_u_face(j, i, us, ldus, (int64_t)H, (int64_t)W + 1, vs, (int64_t)H + 1, (int64_t)W, ldvs, dt, inv)
@@ -92,6 +99,7 @@ __global__ void k_advect_uv(int H, int W, const T* __restrict__ us, int64_t ldus
     vd[(int64_t)j * ldvd + i] =
         m.v(j, i) ? advect_v_face(j, i, vs, ldvs, (int64_t)H + 1, (int64_t)W, us, (int64_t)H, (int64_t)W + 1, ldus, dt, inv)
                   : (T)0;
+  }
 }
 
 // ------------------------------------------------------------------ forces
@@ -100,10 +108,13 @@ template <typename T>
 __global__ void k_apply_forces(int H, int W, T* __restrict__ v, int64_t ldv, const T* __restrict__ d, int64_t ldd,
                                const T* __restrict__ t, int64_t ldt, double dt, double g, double bc, double dc,
                                double amb, int f32tmp) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= W || j > H) return;
-  forces_face(j, i, H, W, v, ldv, d, ldd, t, ldt, dt, g, bc, dc, amb, f32tmp);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= W) return;
+#pragma unroll
+  for (int q = 0; q < kRows; ++q) {
+    const int j = row_of(q);
+    if (j <= H) forces_face(j, i, H, W, v, ldv, d, ldd, t, ldt, dt, g, bc, dc, amb, f32tmp);
+  }
 }
 
 // forces.py:108-123
@@ -121,10 +132,13 @@ __global__ void k_cool(int H, int W, T* __restrict__ t, int64_t ld, double amb, 
 template <typename T>
 __global__ void k_divergence(int H, int W, const T* __restrict__ u, int64_t ldu, const T* __restrict__ v, int64_t ldv,
                              T* __restrict__ div, int64_t ldd, Masks m, double inv) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= W || j >= H) return;
-  div[(int64_t)j * ldd + i] = divergence_cell(j, i, u, ldu, v, ldv, m, inv);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= W) return;
+#pragma unroll
+  for (int q = 0; q < kRows; ++q) {
+    const int j = row_of(q);
+    if (j < H) div[(int64_t)j * ldd + i] = divergence_cell(j, i, u, ldu, v, ldv, m, inv);
+  }
 }
 
 // ------------------------------------------------------------------ residual
@@ -132,13 +146,16 @@ __global__ void k_divergence(int H, int W, const T* __restrict__ u, int64_t ldu,
 template <typename T>
 __global__ void k_residual(int H, int W, const T* __restrict__ p, int64_t ldp, const T* __restrict__ div, int64_t ldd,
                            Masks m, double alpha, double beta, T* __restrict__ out, int64_t ldo, double* sumsq) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double sq = 0.0;
-  if (i < W && j < H) {
-    T res = residual_cell(j, i, H, W, p, ldp, div, ldd, m, alpha, beta);
-    sq = (double)res * (double)res;
-    if (out) out[(int64_t)j * ldo + i] = res;
+#pragma unroll
+  for (int q = 0; q < kRows; ++q) {
+    const int j = row_of(q);
+    if (i < W && j < H) {
+      T res = residual_cell(j, i, H, W, p, ldp, div, ldd, m, alpha, beta);
+      sq += (double)res * (double)res;
+      if (out) out[(int64_t)j * ldo + i] = res;
+    }
   }
   if (sumsq) {
     double s = block_sum(sq);
@@ -152,9 +169,10 @@ template <typename T>
 __global__ void k_project(int H, int W, T* __restrict__ u, int64_t ldu, T* __restrict__ v, int64_t ldv,
                           const T* __restrict__ p, int64_t ldp, Masks m, int do_grad, int solid_mode,
                           const uint8_t* __restrict__ solid, int64_t lds, double scale) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  project_faces(j, i, H, W, u, ldu, v, ldv, p, ldp, m, do_grad, solid_mode, solid, lds, scale);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+  for (int q = 0; q < kRows; ++q)
+    project_faces(row_of(q), i, H, W, u, ldu, v, ldv, p, ldp, m, do_grad, solid_mode, solid, lds, scale);
 }
 
 // ------------------------------------------------------------------ sources
@@ -384,7 +402,7 @@ int sg_advect_scalar(int dtype, int64_t H, int64_t W, const void* src, int64_t l
   Masks m = make_masks(mask_mode, H, W, nullptr, 0, nullptr, 0, is_fluid, ld_fluid);
   if (mask_mode == SG_MASK_PLANES) m.mode = SG_MASK_PLANES;
   SG_DISPATCH(dtype, {
-    SG_LAUNCH(k_advect_scalar<T><<<grid2d(W, H), block2d(), 0, as_stream(stream)>>>(
+    SG_LAUNCH(k_advect_scalar<T><<<grid2d_rows(W, H), block2d(), 0, as_stream(stream)>>>(
         (int)H, (int)W, (const T*)src, ld_src, (T*)dst, ld_dst, (const T*)u, u_rows, u_cols, ld_u, (const T*)v, v_rows,
         v_cols, ld_v, m, dt, 1.0 / cell_size, (T)dissipation));
   });
@@ -435,7 +453,7 @@ int sg_advect_velocity(int dtype, int64_t H, int64_t W, const void* u_src, int64
   SG_CHECK(check_mask_mode(mask_mode, fmu, fmv));
   Masks m = make_masks(mask_mode, H, W, fmu, ld_fmu, fmv, ld_fmv, nullptr, 0);
   SG_DISPATCH(dtype, {
-    SG_LAUNCH(k_advect_uv<T><<<grid2d(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
+    SG_LAUNCH(k_advect_uv<T><<<grid2d_rows(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
         (int)H, (int)W, (const T*)u_src, ld_us, (T*)u_dst, ld_ud, (const T*)v_src, ld_vs, (T*)v_dst, ld_vd, m, dt,
         1.0 / cell_size));
   });
@@ -449,7 +467,7 @@ int sg_apply_forces(int dtype, int64_t H, int64_t W, void* v, int64_t ld_v, cons
   SG_REQUIRE(v && density, "null field pointer");
   SG_REQUIRE(ld_v >= W && ld_d >= W && (!temperature || ld_t >= W), "row stride below row length");
   SG_DISPATCH(dtype, {
-    SG_LAUNCH(k_apply_forces<T><<<grid2d(W, H + 1), block2d(), 0, as_stream(stream)>>>(
+    SG_LAUNCH(k_apply_forces<T><<<grid2d_rows(W, H + 1), block2d(), 0, as_stream(stream)>>>(
         (int)H, (int)W, (T*)v, ld_v, (const T*)density, ld_d, (const T*)temperature, ld_t, dt, gravity,
         buoyancy_coefficient, density_coefficient, ambient_temperature, f32_temporaries));
   });
@@ -477,7 +495,7 @@ int sg_compute_divergence(int dtype, int64_t H, int64_t W, const void* u, int64_
   SG_CHECK(check_mask_mode(mask_mode, fmu, fmv));
   Masks m = make_masks(mask_mode, H, W, fmu, ld_fmu, fmv, ld_fmv, nullptr, 0);
   SG_DISPATCH(dtype, {
-    SG_LAUNCH(k_divergence<T><<<grid2d(W, H), block2d(), 0, as_stream(stream)>>>((int)H, (int)W, (const T*)u, ld_u, (const T*)v,
+    SG_LAUNCH(k_divergence<T><<<grid2d_rows(W, H), block2d(), 0, as_stream(stream)>>>((int)H, (int)W, (const T*)u, ld_u, (const T*)v,
                                                                         ld_v, (T*)div, ld_div, m, 1.0 / cell_size));
   });
   return check_launch("sg_compute_divergence");
@@ -494,7 +512,7 @@ int sg_compute_residual(int dtype, int64_t H, int64_t W, const void* p, int64_t 
   SG_CHECK(check_mask_mode(mask_mode, fmu, fmv));
   Masks m = make_masks(mask_mode, H, W, fmu, ld_fmu, fmv, ld_fmv, is_fluid, ld_fluid);
   SG_DISPATCH(dtype, {
-    SG_LAUNCH(k_residual<T><<<grid2d(W, H), block2d(), 0, as_stream(stream)>>>((int)H, (int)W, (const T*)p, ld_p,
+    SG_LAUNCH(k_residual<T><<<grid2d_rows(W, H), block2d(), 0, as_stream(stream)>>>((int)H, (int)W, (const T*)p, ld_p,
                                                                       (const T*)div, ld_div, m, alpha,
                                                                       1.0 / reciprocal_beta, (T*)out, ld_out, sumsq));
   });
@@ -518,7 +536,7 @@ int sg_enforce_boundary_conditions(int dtype, int64_t H, int64_t W, void* u, int
   if (solid_mode == SG_MASK_NONE) return SG_OK;
   Masks m = make_masks(SG_MASK_OPEN, H, W, nullptr, 0, nullptr, 0, nullptr, 0);
   SG_DISPATCH(dtype, {
-    SG_LAUNCH(k_project<T><<<grid2d(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
+    SG_LAUNCH(k_project<T><<<grid2d_rows(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
         (int)H, (int)W, (T*)u, ld_u, (T*)v, ld_v, (const T*)nullptr, 0, m, 0, solid_mode, solid, ld_s, 0.0));
   });
   return check_launch("sg_enforce_boundary_conditions");
@@ -538,7 +556,7 @@ int sg_project(int dtype, int64_t H, int64_t W, void* u, int64_t ld_u, void* v, 
   Masks m = make_masks(mask_mode, H, W, fmu, ld_fmu, fmv, ld_fmv, nullptr, 0);
   double scale = dt / (fluid_density * cell_size);
   SG_DISPATCH(dtype, {
-    SG_LAUNCH(k_project<T><<<grid2d(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
+    SG_LAUNCH(k_project<T><<<grid2d_rows(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
         (int)H, (int)W, (T*)u, ld_u, (T*)v, ld_v, (const T*)p, ld_p, m, 1, solid_mode, solid, ld_s, scale));
   });
   return check_launch("sg_project");
