@@ -134,6 +134,19 @@ int sg_project(int dtype, int64_t H, int64_t W, void* u, int64_t ld_u, void* v, 
                const uint8_t* fmv, int64_t ld_fmv, int solid_mode, const uint8_t* solid, int64_t ld_s,
                double fluid_density, double cell_size, double dt, void* stream);
 
+/* The substep's tail in one pass (simulation.py:244-265): sg_project of (u_in, v_in) into
+ * (u_out, v_out) (out of place; the inputs are not changed), then sg_compute_divergence of
+ * the projected field into div and sg_compute_residual of p with that divergence into res.
+ * Every value equals the three separate passes'. No single reference function: it fuses
+ * apply_pressure_gradient + enforce_boundary_conditions + compute_divergence +
+ * compute_residual. */
+int sg_project_metrics(int dtype, int64_t H, int64_t W, const void* u_in, int64_t ld_ui, const void* v_in,
+                       int64_t ld_vi, void* u_out, int64_t ld_uo, void* v_out, int64_t ld_vo, const void* p,
+                       int64_t ld_p, int mask_mode, const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv,
+                       int64_t ld_fmv, const uint8_t* is_fluid, int64_t ld_fluid, int solid_mode, const uint8_t* solid,
+                       int64_t ld_s, double fluid_density, double cell_size, double dt, double alpha,
+                       double reciprocal_beta, void* div, int64_t ld_div, void* res, int64_t ld_res, void* stream);
+
 /* common/emitters.py:37-66 (_apply_scalar_field_numba); approach 0 hard_cutoff,
  * 1 linear, 2 quadratic, 3 gaussian (emitters.py:6-35). */
 int sg_emit_scalar(int dtype, int64_t H, int64_t W, void* field, int64_t ld, double value, double dt,

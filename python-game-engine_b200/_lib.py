@@ -67,6 +67,8 @@ SIGNATURES = {
     "sg_gmg_level_shape": [P, I, PI, PI],
     "sg_gmg_smooth_async": [P, I, I, P],
     "sg_gmg_fine_fused": [P],
+    "sg_project_metrics": [I, I64, I64, P, I64, P, I64, P, I64, P, I64, P, I64, I, P, I64, P, I64, P, I64, I, P, I64,
+                           D, D, D, D, D, P, I64, P, I64, P],
     "sg_gmg_fine_kernel_async": [P, I, P, I64, P],
     "sg_add_control": [I, I64, I64, P, I64, P, I64, P, I64, P, I64, D, P],
     "sg_adjoint_advect_scalar_workspace": [I, I64, I64, I],

@@ -127,43 +127,99 @@ __device__ __forceinline__ T residual_cell(int j, int i, int H, int W, const T* 
   return (T)(((double)s + alpha * (double)div[(int64_t)j * ldd + i]) - beta * (double)c);
 }
 
-// pressure_gradient.py:4-37 then, if solid_mode != SG_MASK_NONE, boundaries.py:7-39, for
-// u face (j, i) (j < H, i <= W) and v face (j, i) (j <= H, i < W) of the same thread.
+// pressure_gradient.py:4-37 then, if solid_mode != SG_MASK_NONE, boundaries.py:7-39: the
+// projected value of u face (j, i) (j < H, i <= W) from the face's current value uk.
+template <typename T>
+__device__ __forceinline__ T projected_u(int j, int i, int H, int W, T uk, const T* __restrict__ p, int64_t ldp,
+                                         const Masks& m, int do_grad, int solid_mode,
+                                         const uint8_t* __restrict__ solid, int64_t lds, double scale) {
+  bool zero = (i > 0 && solid_at(solid_mode, solid, lds, H, W, j, i - 1)) ||
+              (i < W && solid_at(solid_mode, solid, lds, H, W, j, i));
+  if (zero) return (T)0;
+  if (!do_grad) return uk;
+  if (m.u(j, i) && i > 0 && i < W) {
+    T dp = p[(int64_t)j * ldp + i] - p[(int64_t)j * ldp + i - 1];
+    return (T)((double)uk - scale * (double)dp);
+  }
+  return (T)0;
+}
+
+// the same for v face (j, i) (j <= H, i < W)
+template <typename T>
+__device__ __forceinline__ T projected_v(int j, int i, int H, int W, T vk, const T* __restrict__ p, int64_t ldp,
+                                         const Masks& m, int do_grad, int solid_mode,
+                                         const uint8_t* __restrict__ solid, int64_t lds, double scale) {
+  bool zero = (j > 0 && solid_at(solid_mode, solid, lds, H, W, j - 1, i)) ||
+              (j < H && solid_at(solid_mode, solid, lds, H, W, j, i));
+  if (zero) return (T)0;
+  if (!do_grad) return vk;
+  if (m.v(j, i) && j > 0 && j < H) {
+    T dp = p[(int64_t)j * ldp + i] - p[(int64_t)(j - 1) * ldp + i];
+    return (T)((double)vk - scale * (double)dp);
+  }
+  return (T)0;
+}
+
+// Projection of u face (j, i) (j < H, i <= W) and v face (j, i) (j <= H, i < W) in place.
 template <typename T>
 __device__ __forceinline__ void project_faces(int j, int i, int H, int W, T* __restrict__ u, int64_t ldu,
                                               T* __restrict__ v, int64_t ldv, const T* __restrict__ p, int64_t ldp,
                                               const Masks& m, int do_grad, int solid_mode,
                                               const uint8_t* __restrict__ solid, int64_t lds, double scale) {
   if (j < H && i <= W) {
-    int64_t k = (int64_t)j * ldu + i;
-    bool zero = (i > 0 && solid_at(solid_mode, solid, lds, H, W, j, i - 1)) ||
-                (i < W && solid_at(solid_mode, solid, lds, H, W, j, i));
-    if (zero) {
-      u[k] = (T)0;
-    } else if (do_grad) {
-      if (m.u(j, i) && i > 0 && i < W) {
-        T dp = p[(int64_t)j * ldp + i] - p[(int64_t)j * ldp + i - 1];
-        u[k] = (T)((double)u[k] - scale * (double)dp);
-      } else {
-        u[k] = (T)0;
-      }
-    }
+    T* q = u + (int64_t)j * ldu + i;
+    *q = projected_u(j, i, H, W, *q, p, ldp, m, do_grad, solid_mode, solid, lds, scale);
   }
   if (j <= H && i < W) {
-    int64_t k = (int64_t)j * ldv + i;
-    bool zero = (j > 0 && solid_at(solid_mode, solid, lds, H, W, j - 1, i)) ||
-                (j < H && solid_at(solid_mode, solid, lds, H, W, j, i));
-    if (zero) {
-      v[k] = (T)0;
-    } else if (do_grad) {
-      if (m.v(j, i) && j > 0 && j < H) {
-        T dp = p[(int64_t)j * ldp + i] - p[(int64_t)(j - 1) * ldp + i];
-        v[k] = (T)((double)v[k] - scale * (double)dp);
-      } else {
-        v[k] = (T)0;
-      }
-    }
+    T* q = v + (int64_t)j * ldv + i;
+    *q = projected_v(j, i, H, W, *q, p, ldp, m, do_grad, solid_mode, solid, lds, scale);
   }
+}
+
+// The substep's tail in one pass (simulation.py:244-265): project the faces of cell (j, i)
+// from (u_in, v_in) into (u_out, v_out), then the divergence of the projected field and the
+// reference residual of p at the cell. The cell's right and upper faces belong to the
+// neighbouring threads; their projected values are recomputed here from the inputs (which
+// nobody writes), with the same expressions, so every value equals the separate passes'.
+template <typename T>
+__device__ __forceinline__ void project_metrics_point(int j, int i, int H, int W, const T* __restrict__ u_in,
+                                                      int64_t ldui, const T* __restrict__ v_in, int64_t ldvi,
+                                                      T* __restrict__ u_out, int64_t lduo, T* __restrict__ v_out,
+                                                      int64_t ldvo, const T* __restrict__ p, int64_t ldp,
+                                                      const Masks& m, int solid_mode,
+                                                      const uint8_t* __restrict__ solid, int64_t lds, double scale,
+                                                      T* __restrict__ div, int64_t ldd, double inv, double alpha,
+                                                      double beta, T* __restrict__ res, int64_t ldr) {
+  T ul = (T)0, vd = (T)0;
+  if (j < H && i <= W) {
+    ul = projected_u(j, i, H, W, u_in[(int64_t)j * ldui + i], p, ldp, m, 1, solid_mode, solid, lds, scale);
+    u_out[(int64_t)j * lduo + i] = ul;
+  }
+  if (j <= H && i < W) {
+    vd = projected_v(j, i, H, W, v_in[(int64_t)j * ldvi + i], p, ldp, m, 1, solid_mode, solid, lds, scale);
+    v_out[(int64_t)j * ldvo + i] = vd;
+  }
+  if (j >= H || i >= W) return;
+  const T ur = projected_u(j, i + 1, H, W, u_in[(int64_t)j * ldui + i + 1], p, ldp, m, 1, solid_mode, solid, lds,
+                           scale);
+  const T vu = projected_v(j + 1, i, H, W, v_in[(int64_t)(j + 1) * ldvi + i], p, ldp, m, 1, solid_mode, solid, lds,
+                           scale);
+  // divergence.py:4-25 on the projected faces
+  T a = ur * (T)(m.u(j, i + 1) ? 1 : 0);
+  T b = ul * (T)(m.u(j, i) ? 1 : 0);
+  T c = vu * (T)(m.v(j + 1, i) ? 1 : 0);
+  T e = vd * (T)(m.v(j, i) ? 1 : 0);
+  T du = a - b, dv = c - e;
+  const T dval = (T)((double)du * inv + (double)dv * inv);
+  div[(int64_t)j * ldd + i] = dval;
+  // residual.py:6-42 with that divergence
+  T r = (T)0;
+  if (m.fluid(j, i)) {
+    T cc = p[(int64_t)j * ldp + i];
+    T s = nbsum_ref(p, ldp, H, W, j, i, m, cc);
+    r = (T)(((double)s + alpha * (double)dval) - beta * (double)cc);
+  }
+  res[(int64_t)j * ldr + i] = r;
 }
 
 // Overwriting disc sources at cell (j, i), u face (j, i) and v face (j, i) (j <= H, i <= W):

@@ -175,6 +175,24 @@ __global__ void k_project(int H, int W, T* __restrict__ u, int64_t ldu, T* __res
     project_faces(row_of(q), i, H, W, u, ldu, v, ldv, p, ldp, m, do_grad, solid_mode, solid, lds, scale);
 }
 
+// The substep's tail: projection out of place, divergence and residual in one pass.
+template <typename T>
+__global__ void k_project_metrics(int H, int W, const T* __restrict__ ui, int64_t ldui, const T* __restrict__ vi,
+                                  int64_t ldvi, T* __restrict__ uo, int64_t lduo, T* __restrict__ vo, int64_t ldvo,
+                                  const T* __restrict__ p, int64_t ldp, Masks m, int solid_mode,
+                                  const uint8_t* __restrict__ solid, int64_t lds, double scale, T* __restrict__ div,
+                                  int64_t ldd, double inv, double alpha, double beta, T* __restrict__ res,
+                                  int64_t ldr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+  for (int q = 0; q < kRows; ++q) {
+    const int j = row_of(q);
+    if (j <= H && i <= W)
+      project_metrics_point(j, i, H, W, ui, ldui, vi, ldvi, uo, lduo, vo, ldvo, p, ldp, m, solid_mode, solid, lds,
+                            scale, div, ldd, inv, alpha, beta, res, ldr);
+  }
+}
+
 // ------------------------------------------------------------------ sources
 // emitters.py:6-66 over the emitter's bounding box (x0, y0 offset).
 template <typename T>
@@ -560,6 +578,33 @@ int sg_project(int dtype, int64_t H, int64_t W, void* u, int64_t ld_u, void* v, 
         (int)H, (int)W, (T*)u, ld_u, (T*)v, ld_v, (const T*)p, ld_p, m, 1, solid_mode, solid, ld_s, scale));
   });
   return check_launch("sg_project");
+}
+
+int sg_project_metrics(int dtype, int64_t H, int64_t W, const void* u_in, int64_t ld_ui, const void* v_in,
+                       int64_t ld_vi, void* u_out, int64_t ld_uo, void* v_out, int64_t ld_vo, const void* p,
+                       int64_t ld_p, int mask_mode, const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv,
+                       int64_t ld_fmv, const uint8_t* is_fluid, int64_t ld_fluid, int solid_mode, const uint8_t* solid,
+                       int64_t ld_s, double fluid_density, double cell_size, double dt, double alpha,
+                       double reciprocal_beta, void* div, int64_t ld_div, void* res, int64_t ld_res, void* stream) {
+  SG_CHECK(check_grid(H, W));
+  SG_REQUIRE(u_in && v_in && u_out && v_out && p && div && res, "null field pointer");
+  SG_REQUIRE(u_in != u_out && v_in != v_out, "the projection here is out of place");
+  SG_REQUIRE(ld_ui >= W + 1 && ld_vi >= W && ld_uo >= W + 1 && ld_vo >= W && ld_p >= W && ld_div >= W && ld_res >= W,
+             "row stride below row length");
+  SG_REQUIRE(fluid_density != 0.0 && cell_size > 0.0 && reciprocal_beta != 0.0, "bad coefficients");
+  SG_CHECK(check_mask_mode(mask_mode, fmu, fmv));
+  SG_REQUIRE(mask_mode != SG_MASK_PLANES || is_fluid, "is_fluid plane required");
+  SG_REQUIRE(solid_mode == SG_MASK_NONE || solid_mode == SG_MASK_RING || (solid_mode == SG_MASK_PLANES && solid),
+             "bad solid mode or missing solid plane");
+  Masks m = make_masks(mask_mode, H, W, fmu, ld_fmu, fmv, ld_fmv, is_fluid, ld_fluid);
+  const double scale = dt / (fluid_density * cell_size);
+  SG_DISPATCH(dtype, {
+    SG_LAUNCH(k_project_metrics<T><<<grid2d_rows(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
+        (int)H, (int)W, (const T*)u_in, ld_ui, (const T*)v_in, ld_vi, (T*)u_out, ld_uo, (T*)v_out, ld_vo,
+        (const T*)p, ld_p, m, solid_mode, solid, ld_s, scale, (T*)div, ld_div, 1.0 / cell_size, alpha,
+        1.0 / reciprocal_beta, (T*)res, ld_res));
+  });
+  return check_launch("sg_project_metrics");
 }
 
 int sg_emit_scalar(int dtype, int64_t H, int64_t W, void* field, int64_t ld, double value, double dt, double pos_x,

@@ -225,6 +225,29 @@ def project(velocity_u, velocity_v, pressure, face_mask_u, face_mask_v, solid_ma
 APPROACH_CODES = {"hard_cutoff": 0, "linear": 1, "quadratic": 2, "gaussian": 3}
 
 
+def project_metrics(u_in, v_in, u_out, v_out, pressure, face_mask_u, face_mask_v, is_fluid, solid_mask, fluid_density,
+                    cell_size, dt, alpha, reciprocal_beta, divergence_out, residual_out):
+    """The substep's tail in one pass (simulation.py:244-265): project (u_in, v_in) into
+    (u_out, v_out) (apply_pressure_gradient + enforce_boundary_conditions, out of place),
+    then the divergence of the projected field into ``divergence_out`` and the reference
+    residual of ``pressure`` with it into ``residual_out`` -- the values the four separate
+    operators give."""
+    dt_code = _same_dtype(u_in, v_in, u_out, v_out, pressure, divergence_out, residual_out)
+    H, W = pressure.shape
+    mode, pu, lu, pv, lv = _face_pair(face_mask_u, face_mask_v, H, W)
+    fmode, pf, ldf = _masks(is_fluid, "is_fluid", (H, W))
+    if fmode != mode:
+        raise ValueError("is_fluid and the face masks must both be planes or the same analytic mask")
+    smode, ps, lds = _solid_arg(solid_mask, H, W)
+    a = [L.field(x, n) for x, n in ((u_in, "u_in"), (v_in, "v_in"), (u_out, "u_out"), (v_out, "v_out"),
+                                    (pressure, "pressure"), (divergence_out, "divergence_out"),
+                                    (residual_out, "residual_out"))]
+    L.call("sg_project_metrics", dt_code, H, W, a[0][0], a[0][1], a[1][0], a[1][1], a[2][0], a[2][1], a[3][0],
+           a[3][1], a[4][0], a[4][1], mode, pu, lu, pv, lv, pf, ldf, smode, ps, lds, float(fluid_density),
+           float(cell_size), float(dt), float(alpha), float(reciprocal_beta), a[5][0], a[5][1], a[6][0], a[6][1],
+           L.stream_ptr())
+
+
 def emit_scalar(field, value, dt, pos_x, pos_y, radius, approach):
     """emitters.py:37-66: field += value * falloff(dist) * dt inside the radius."""
     if approach not in APPROACH_CODES:

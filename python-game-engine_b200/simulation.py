@@ -330,15 +330,11 @@ class SmokeSimulation2D:
             with scope("simulation.pressure.solve"):
                 self._solve_pressure()
             with scope("simulation.pressure.apply"):
-                self._project(dt)
+                # projection plus the metrics tail's divergence and residual in one pass
+                self._project_and_metrics(dt)
         with scope("profiling.metrics"):
-            self._compute_divergence()
             prof.metrics.capture("divergence", "after_projection", self.divergence)
             prof.metrics.capture("pressure", "final", self.pressure)
-            fmu, fmv, fl = self._kmasks
-            ops.compute_residual(self.pressure, self.divergence, fl, fmu, fmv,
-                                 calculate_alpha(self.cell_size, self.fluid_density, dt), calculate_reciprocal_beta(),
-                                 self.pressure_residual)
             prof.metrics.capture("pressure_residual", "final", self.pressure_residual)
             prof.metrics.process()
         self.step_index += 1
@@ -397,6 +393,17 @@ class SmokeSimulation2D:
 
     def _enforce_boundaries(self):
         ops.enforce_boundary_conditions(self.velocity_u, self.velocity_v, self._ksolid)
+
+    def _project_and_metrics(self, dt):
+        """simulation.py:244-265 fused: the projected velocity (written to the spare buffers,
+        then swapped in), the divergence after projection and the pressure residual."""
+        fmu, fmv, fl = self._kmasks
+        ops.project_metrics(self.velocity_u, self.velocity_v, self.velocity_u_temp, self.velocity_v_temp,
+                            self.pressure, fmu, fmv, fl, self._ksolid, self.fluid_density, self.cell_size, dt,
+                            calculate_alpha(self.cell_size, self.fluid_density, dt), calculate_reciprocal_beta(),
+                            self.divergence, self.pressure_residual)
+        self.velocity_u, self.velocity_u_temp = self.velocity_u_temp, self.velocity_u
+        self.velocity_v, self.velocity_v_temp = self.velocity_v_temp, self.velocity_v
 
     def _project(self, dt):
         fmu, fmv, _ = self._kmasks

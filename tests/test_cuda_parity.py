@@ -232,3 +232,37 @@ def test_emitters_vs_reference(approach):
     got = f.cpu().numpy()
     assert rel(got, d[approach + "_numba"]) <= 1e-6
     assert rel(got, d[approach + "_python"]) <= 1e-6
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("planes", [False, True])
+def test_fused_tail_equals_separate_operators(dtype, planes):
+    """project_metrics (projection out of place + divergence + residual in one pass) must
+    give bit for bit what project, compute_divergence and compute_residual give."""
+    H, W = 67, 90
+    g = torch.Generator().manual_seed(11)
+    r = lambda *s: torch.randn(s, generator=g, dtype=torch.float64).to(dtype).cuda()  # noqa: E731
+    u, v, p = r(H, W + 1), r(H + 1, W), r(H, W)
+    if planes:
+        solid = torch.zeros((H, W), dtype=torch.bool)
+        solid[0, :] = solid[-1, :] = solid[:, 0] = solid[:, -1] = True
+        solid[20:30, 40:55] = True
+        fmu, fmv, fl = sg.operators.build_masks(solid.cuda())
+        solid_arg = solid.cuda()
+    else:
+        fmu = fmv = fl = sg.OPEN_BOX
+        solid_arg = sg.RING_BOX
+    h, dt, rho = 1.0 / W, 0.5 / W, 1.0
+    alpha = sg.calculate_alpha(h, rho, dt)
+    # separate passes
+    u1, v1 = u.clone(), v.clone()
+    sg.operators.project(u1, v1, p, fmu, fmv, solid_arg, rho, h, dt)
+    d1 = torch.empty((H, W), dtype=dtype, device="cuda")
+    sg.operators.compute_divergence(u1, v1, d1, fmu, fmv, h)
+    r1 = torch.empty_like(d1)
+    sg.operators.compute_residual(p, d1, fl, fmu, fmv, alpha, 0.25, r1)
+    # fused
+    u2, v2, d2, r2 = torch.empty_like(u), torch.empty_like(v), torch.empty_like(d1), torch.empty_like(d1)
+    sg.operators.project_metrics(u, v, u2, v2, p, fmu, fmv, fl, solid_arg, rho, h, dt, alpha, 0.25, d2, r2)
+    for a, b in ((u1, u2), (v1, v2), (d1, d2), (r1, r2)):
+        assert torch.equal(a, b)
