@@ -246,6 +246,10 @@ int sg_mg_coarsen_solid(int64_t H, int64_t W, const uint8_t* solid, int64_t ld_s
 
 typedef struct sg_gmg_plan sg_gmg_plan;
 
+/* Copy the last solve's relative residual (a double) to `dst` (host-pinned or device
+ * memory) on `stream`, without synchronising. */
+int sg_gmg_relres_async(sg_gmg_plan* plan, double* dst, void* stream);
+
 /* Host-side planning (allocates host memory only). The masks are HOST arrays
  * (NULL in SG_MASK_OPEN / SG_MASK_RING modes). cycle: 0 = V, 1 = W. */
 int sg_gmg_plan_create(sg_gmg_plan** plan, int64_t H, int64_t W, int mask_mode, const uint8_t* is_fluid,

@@ -1492,6 +1492,13 @@ int sg_gmg_stats(sg_gmg_plan* plan, int* cycles, double* relres, int* status, lo
   return SG_OK;
 }
 
+int sg_gmg_relres_async(sg_gmg_plan* plan, double* dst, void* stream) {
+  SG_REQUIRE(plan && plan->ws && dst, "plan not bound / null destination");
+  SG_CUDA_TRY(cudaMemcpyAsync(dst, &state_ptr(plan)->relres, sizeof(double), cudaMemcpyDefault, as_stream(stream)),
+              "sg_gmg_relres_async");
+  return SG_OK;
+}
+
 int sg_gmg_counters(sg_gmg_plan* plan, long long* solves, long long* cycles, long long* failures, void* stream) {
   SG_REQUIRE(plan && plan->ws, "plan not bound to a workspace");
   GmgState st;

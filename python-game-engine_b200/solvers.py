@@ -286,6 +286,11 @@ class GMGPlan:
     def tail_start(self):
         return L.load().sg_gmg_tail_start(self.handle)
 
+    def relres_async(self, dst, stream=None):
+        """Enqueue a copy of the last solve's relative residual into `dst` (one float64,
+        pinned host or CUDA tensor) on `stream`; no synchronisation."""
+        L.call("sg_gmg_relres_async", self.handle, ctypes.c_void_p(dst.data_ptr()), L.stream_ptr(stream))
+
     def fine_fused(self):
         """True when the fine level runs the fused register-tiled pre/post kernels."""
         return bool(L.load().sg_gmg_fine_fused(self.handle))
