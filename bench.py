@@ -139,6 +139,40 @@ def cpu_oracle_steps(n_steps, warmup):
     return times, cycles[warmup:], threads
 
 
+def cpu_oracle_batch(scenes, steps):
+    """The CPU oracle on a sample of the batch: each scene stepped `steps` times (after one
+    warm-up step) with the oracle's multigrid in mixed precision to 1e-6."""
+    import numpy as np
+
+    import oracle as O
+
+    total_cells, total_s = 0, 0.0
+    for sc in scenes:
+        fmu, fmv = O.face_masks_from_solid(np.zeros((sc.H, sc.W), bool))
+        fl = O.is_fluid_from_faces(fmu, fmv)
+        gmg = O.GMGOracle(fmu, fmv, fl, coarsest=8, omega=1.4)
+
+        def solver(p, div, fmu_, fmv_, rho, h, dt, gmg=gmg, fl=fl, **_):
+            b = O.alpha_coeff(h, rho, dt) * div.astype(np.float64) * fl
+            p64 = np.zeros(p.shape)
+            gmg.solve(p64, b, tol=1e-6, max_cycles=50, precision="mixed")
+            p[:] = p64.astype(p.dtype)
+
+        sim = O.OracleSim(sc.H, sc.W, sc.cell_size, solver, {}, dtype=np.float32)
+        sim.dt, sim.gravity = sc.dt, sc.gravity
+        sim.plumes = [O.PlumeSpec(*row, seed=sc.seed) for row in sc.plumes]
+        sim.substep(sc.dt)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            sim.substep(sc.dt)
+        total_s += time.perf_counter() - t0
+        total_cells += sc.H * sc.W * steps
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": total_cells / total_s, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(scenes)} of the batch's scenes x {steps} substeps each on the CPU oracle (C/OpenMP "
+                      f"restatement of the reference kernels + the same multigrid to 1e-6), after 1 warm-up step"}
+
+
 def run_reference(args):
     world, rank, _ = _dist()
     if rank != 0:
@@ -476,6 +510,9 @@ def run_batch(args):
         return 0
     value = total_cells * args.steps / (ms / 1e3)
     peak, peak_kind = _peaks()
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_oracle_batch(scenes[:8], 2)
     # algorithmic bytes per cell and step outside the solver (float32): forces 12, advect u/v
     # 12 + 12, advect density + dissipation 16, divergence 12, projection 20, metrics
     # divergence 12 + residual 12 = 108 B; per cycle the solver moves >= the fine level's
@@ -498,6 +535,7 @@ def run_batch(args):
                      "achieved": alg_bytes / (ms / 1e3) / 1e9},
     }
     line["roofline"]["frac"] = line["roofline"]["achieved"] / peak
+    line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     return 0
 

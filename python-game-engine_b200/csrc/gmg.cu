@@ -901,9 +901,12 @@ static bool fused_level(const sg_gmg_plan* p, int k) { return p->levels[k].fused
 
 // Large tiles while a level fills the GPU with them (two blocks per SM), small tiles below:
 // a small level is latency-bound, and more blocks with less serial work each finish sooner.
+#ifndef SG_GMG_REG_MIN_TILES
+#define SG_GMG_REG_MIN_TILES (2 * 148)
+#endif
 static bool small_tiles(const Level& L) {
   const int64_t large_blocks = (int64_t)((L.W + kTX - 1) / kTX) * ((L.H + kTY - 1) / kTY);
-  return large_blocks < 2 * 148;
+  return large_blocks < SG_GMG_REG_MIN_TILES;
 }
 
 template <typename T, int SW, int TX, int TY>
