@@ -527,7 +527,7 @@ __global__ void __launch_bounds__(32 * NWARP, MINB)
 // tiles (the last caps the registers a thread may use); MINB_FINAL for the fused fine-level
 // post kernel.
 #ifndef SG_REG_F32_RPT
-#define SG_REG_F32_RPT 8
+#define SG_REG_F32_RPT 6
 #define SG_REG_F32_NWARP 8
 #define SG_REG_F32_MINB 4
 #endif
@@ -539,8 +539,8 @@ __global__ void __launch_bounds__(32 * NWARP, MINB)
 #ifndef SG_REG_FINAL_MINB
 #define SG_REG_FINAL_MINB 4
 #endif
-// the fused fine-level post kernel's rows per thread and warps (measured: 6 x 8 for FP32
-// cycles, the level kernels' 4 x 8 for FP64)
+// the fused fine-level post kernel's rows per thread and warps (measured on B200: 6 x 8 for
+// FP32 cycles, 4 x 8 for FP64, as for the level kernels)
 #ifndef SG_REG_FINAL_F32_RPT
 #define SG_REG_FINAL_F32_RPT 6
 #define SG_REG_FINAL_F32_NWARP 8
