@@ -401,6 +401,19 @@ int64_t sg_batch_snapshot_bytes(const sg_batch* batch);
 int sg_batch_autotune(sg_batch* batch, int steps, void* scratch, int64_t scratch_bytes, void* stream, int* tile,
                       int* sweeps, int* wcycle, double* ms_per_step);
 
+/* ---------------------------------------------------------------- profiling metrics
+ * Replaces the numpy reductions of MetricsRecorder.process (src/cfd/profiling/metrics.py:
+ * 113-133) over the scopes of _build_scope_mask (metrics.py:7-29) with the reducers of
+ * profiling/config.py:270-299: one launch reduces an H x W field (float32 or float64, row
+ * stride ld) in float64 and writes 18 doubles to device memory at `out`, ordered scope
+ * (all, interior = [1:-1, 1:-1], boundary = the rest) x reducer (rms, mean, mean_abs, max,
+ * max_abs, std with ddof 0). An empty scope gives NaN. `workspace`:
+ * sg_field_stats_workspace_bytes() bytes of device memory, 256-byte aligned, zero-filled
+ * before first use; launches sharing one workspace must be stream-ordered. */
+int64_t sg_field_stats_workspace_bytes(void);
+int sg_field_stats(int dtype, int64_t H, int64_t W, const void* field, int64_t ld, void* workspace, double* out,
+                   void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,7 +9,7 @@ include/smoke_b200.h); there is no CPU fallback.
 The package directory name is not a Python identifier; import it with
 ``importlib.import_module("python-game-engine_b200")``.
 """
-from . import _lib, adjoint, batch, scenes
+from . import _lib, adjoint, batch, profiling, scenes
 from .config import Backend, GridConfig, OperatorBackendConfig, PressureSolverConfig, SimulationConfig
 from .operators import OPEN_BOX, RING_BOX, AnalyticMask, register_operators
 from .params import (DEFAULT_SOLVER_PARAMS, SOLVER_PARAM_TYPES, GaussSeidelParams, GeometricMultigridParams,
@@ -19,6 +19,7 @@ from .simulation import Emitter2D, NullProfileSession, PlumeSource, SmokeSimulat
 from .solvers import (GeometricMultigridSolver, MultigridSolver, SORToleranceSolver, calculate_alpha,
                       calculate_optimal_omega, calculate_reciprocal_beta, register_solvers, solve_pressure)
 from ._lib import NotConverged, SmokeCudaError
+from .profiling import ProfileConfig, ProfileSession
 
 register_operators()
 register_solvers()
@@ -30,5 +31,6 @@ __all__ = [
     "OPERATOR_REGISTRY", "SOLVER_REGISTRY", "get_operator", "get_solver", "register_operator", "register_solver",
     "Emitter2D", "NullProfileSession", "PlumeSource", "SmokeSimulation2D", "GeometricMultigridSolver",
     "MultigridSolver", "SORToleranceSolver", "calculate_alpha", "calculate_optimal_omega",
-    "calculate_reciprocal_beta", "solve_pressure", "NotConverged", "SmokeCudaError",
+    "calculate_reciprocal_beta", "solve_pressure", "NotConverged", "SmokeCudaError", "ProfileConfig",
+    "ProfileSession",
 ]

@@ -95,6 +95,8 @@ SIGNATURES = {
     "sg_batch_stats": [P, P, P, P, P],
     "sg_batch_snapshot_bytes": [P],
     "sg_batch_autotune": [P, I, P, I64, P, PI, PI, PI, PD],
+    "sg_field_stats_workspace_bytes": [],
+    "sg_field_stats": [I, I64, I64, P, I64, P, P, P],
     "sg_version": [],
     "sg_last_error": [],
     "sg_launch_count": [],
@@ -109,6 +111,7 @@ _RESTYPE = {
     "sg_batch_destroy": None,
     "sg_batch_workspace_bytes": ctypes.c_int64,
     "sg_batch_snapshot_bytes": ctypes.c_int64,
+    "sg_field_stats_workspace_bytes": ctypes.c_int64,
 }
 
 _lib = None

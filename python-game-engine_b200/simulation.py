@@ -323,6 +323,8 @@ class SmokeSimulation2D:
             with scope("simulation.cooling"):
                 if temp_on:
                     self._cool_temperature(dt)
+            with scope("simulation.dissipation"):
+                pass  # applied inside the density advection
             with scope("simulation.divergence"):
                 self._compute_divergence()
             with scope("profiling.capture"):
