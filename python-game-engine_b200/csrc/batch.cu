@@ -75,8 +75,8 @@ struct BCtl {
   long long loops;  // cycle-loop iterations run since bind (all scenes together)
 };
 
-__device__ __forceinline__ Masks open_masks(int H, int W) {
-  Masks m;
+__device__ __forceinline__ MasksT<SG_MASK_OPEN> open_masks(int H, int W) {
+  MasksT<SG_MASK_OPEN> m;
   m.fmu = m.fmv = m.fl = nullptr;
   m.ldu = m.ldv = m.ldf = 0;
   m.mode = SG_MASK_OPEN;
@@ -187,7 +187,7 @@ struct OpAdvectUV {
   __device__ void operator()(int sc, int j, int i) const {
     const BScene& s = P.scenes[sc];
     const int H = s.H, W = s.W;
-    const Masks m = open_masks(H, W);
+    const MasksT<SG_MASK_OPEN> m = open_masks(H, W);
     const float* us = P.u[cur] + s.ou;
     const float* vs = P.v[cur] + s.ov;
     if (j < H && i <= W)
@@ -211,7 +211,7 @@ struct OpAdvectD {
     const BScene& s = P.scenes[sc];
     const int H = s.H, W = s.W;
     if (j >= H || i >= W) return;
-    const Masks m = open_masks(H, W);
+    const MasksT<SG_MASK_OPEN> m = open_masks(H, W);
     P.d[1 - cur][s.oc + (int64_t)j * W + i] =
         advect_scalar_cell(j, i, H, W, (const float*)(P.d[cur] + s.oc), (int64_t)W,
                            (const float*)(P.u[1 - cur] + s.ou), (int64_t)H, (int64_t)W + 1, (int64_t)W + 1,
@@ -226,7 +226,7 @@ struct OpDivergence {
   __device__ void operator()(int sc, int j, int i) const {
     const BScene& s = P.scenes[sc];
     if (j >= s.H || i >= s.W) return;
-    const Masks m = open_masks(s.H, s.W);
+    const MasksT<SG_MASK_OPEN> m = open_masks(s.H, s.W);
     P.div[s.oc + (int64_t)j * s.W + i] = divergence_cell(j, i, (const float*)(P.u[nxt] + s.ou), (int64_t)s.W + 1,
                                                          (const float*)(P.v[nxt] + s.ov), (int64_t)s.W, m, s.inv);
   }
@@ -237,8 +237,8 @@ struct OpProject {
   int nxt;
   __device__ void operator()(int sc, int j, int i) const {
     const BScene& s = P.scenes[sc];
-    const Masks m = open_masks(s.H, s.W);
-    project_faces(j, i, s.H, s.W, P.u[nxt] + s.ou, (int64_t)s.W + 1, P.v[nxt] + s.ov, (int64_t)s.W,
+    const MasksT<SG_MASK_OPEN> m = open_masks(s.H, s.W);
+    project_faces<float, MasksT<SG_MASK_OPEN>, SG_MASK_RING>(j, i, s.H, s.W, P.u[nxt] + s.ou, (int64_t)s.W + 1, P.v[nxt] + s.ov, (int64_t)s.W,
                   (const float*)(P.p + s.oc), (int64_t)s.W, m, 1, SG_MASK_RING, (const uint8_t*)nullptr, 0, s.scale);
   }
 };
@@ -249,7 +249,7 @@ struct OpResidual {
   __device__ void operator()(int sc, int j, int i) const {
     const BScene& s = P.scenes[sc];
     if (j >= s.H || i >= s.W) return;
-    const Masks m = open_masks(s.H, s.W);
+    const MasksT<SG_MASK_OPEN> m = open_masks(s.H, s.W);
     P.res[s.oc + (int64_t)j * s.W + i] =
         residual_cell(j, i, s.H, s.W, (const float*)(P.p + s.oc), (int64_t)s.W, (const float*)(P.div + s.oc),
                       (int64_t)s.W, m, s.alpha, 4.0);

@@ -9,13 +9,13 @@
 namespace sg {
 
 // advection.py:112-128 (+ dissipation, simulation.py:232): the new value of cell (j, i).
-template <typename T>
+template <typename T, typename MK>
 __device__ __forceinline__ T advect_scalar_cell(int j, int i, int H, int W, const T* __restrict__ src, int64_t lds,
                                                 const T* __restrict__ u, int64_t ur, int64_t uc, int64_t ldu,
                                                 const T* __restrict__ v, int64_t vr, int64_t vc, int64_t ldv,
-                                                const Masks& m, double dt, double inv, T diss) {
+                                                const MK& m, double dt, double inv, T diss) {
   if (!m.fluid(j, i)) return (T)0;
-  double px = (double)i + 0.5, py = (double)j + 0.5;
+  double px = idx_double(i) + 0.5, py = idx_double(j) + 0.5;
   double uu = sample_ref(u, ldu, ur, uc, px, py - 0.5);
   double vv = sample_ref(v, ldv, vr, vc, px - 0.5, py);
   double x = px - (uu * dt * inv);
@@ -29,7 +29,7 @@ template <typename T>
 __device__ __forceinline__ T advect_u_face(int j, int i, const T* __restrict__ us, int64_t ldus, int64_t ur, int64_t uc,
                                            const T* __restrict__ v, int64_t vr, int64_t vc, int64_t ldv, double dt,
                                            double inv) {
-  double px = (double)i, py = (double)j + 0.5;
+  double px = idx_double(i), py = idx_double(j) + 0.5;
   T uu = us[(int64_t)j * ldus + i];
   double vv = sample_ref(v, ldv, vr, vc, px - 0.5, py);
   double x = px - ((double)uu * dt * inv);
@@ -42,7 +42,7 @@ template <typename T>
 __device__ __forceinline__ T advect_v_face(int j, int i, const T* __restrict__ vs, int64_t ldvs, int64_t vr, int64_t vc,
                                            const T* __restrict__ u, int64_t ur, int64_t uc, int64_t ldu, double dt,
                                            double inv) {
-  double px = (double)i + 0.5, py = (double)j;
+  double px = idx_double(i) + 0.5, py = idx_double(j);
   double uu = sample_ref(u, ldu, ur, uc, px, py - 0.5);
   T vv = vs[(int64_t)j * ldvs + i];
   double x = px - (uu * dt * inv);
@@ -91,9 +91,9 @@ __device__ __forceinline__ void forces_face(int j, int i, int H, int W, T* __res
 }
 
 // divergence.py:4-25: divergence of cell (j, i).
-template <typename T>
+template <typename T, typename MK>
 __device__ __forceinline__ T divergence_cell(int j, int i, const T* __restrict__ u, int64_t ldu, const T* __restrict__ v,
-                                             int64_t ldv, const Masks& m, double inv) {
+                                             int64_t ldv, const MK& m, double inv) {
   T a = u[(int64_t)j * ldu + i + 1] * (T)(m.u(j, i + 1) ? 1 : 0);
   T b = u[(int64_t)j * ldu + i] * (T)(m.u(j, i) ? 1 : 0);
   T c = v[(int64_t)(j + 1) * ldv + i] * (T)(m.v(j + 1, i) ? 1 : 0);
@@ -103,8 +103,8 @@ __device__ __forceinline__ T divergence_cell(int j, int i, const T* __restrict__
 }
 
 // Masked neighbour sum shared with jacobi.py:18-21 and red_black_sor_gauss_seidel.py:19-22.
-template <typename T>
-__device__ __forceinline__ T nbsum_ref(const T* __restrict__ p, int64_t ld, int H, int W, int j, int i, const Masks& m,
+template <typename T, typename MK>
+__device__ __forceinline__ T nbsum_ref(const T* __restrict__ p, int64_t ld, int H, int W, int j, int i, const MK& m,
                                        T c) {
   T l = m.u(j, i) ? p[(int64_t)j * ld + (i - 1 > 0 ? i - 1 : 0)] : c;
   T r = m.u(j, i + 1) ? p[(int64_t)j * ld + (i + 1 < W - 1 ? i + 1 : W - 1)] : c;
@@ -117,9 +117,9 @@ __device__ __forceinline__ T nbsum_ref(const T* __restrict__ p, int64_t ld, int 
 }
 
 // residual.py:6-42: the residual of cell (j, i) (0 off the fluid).
-template <typename T>
+template <typename T, typename MK>
 __device__ __forceinline__ T residual_cell(int j, int i, int H, int W, const T* __restrict__ p, int64_t ldp,
-                                           const T* __restrict__ div, int64_t ldd, const Masks& m, double alpha,
+                                           const T* __restrict__ div, int64_t ldd, const MK& m, double alpha,
                                            double beta) {
   if (!m.fluid(j, i)) return (T)0;
   T c = p[(int64_t)j * ldp + i];
@@ -129,12 +129,12 @@ __device__ __forceinline__ T residual_cell(int j, int i, int H, int W, const T* 
 
 // pressure_gradient.py:4-37 then, if solid_mode != SG_MASK_NONE, boundaries.py:7-39: the
 // projected value of u face (j, i) (j < H, i <= W) from the face's current value uk.
-template <typename T>
+template <typename T, typename MK, int SM = -1>
 __device__ __forceinline__ T projected_u(int j, int i, int H, int W, T uk, const T* __restrict__ p, int64_t ldp,
-                                         const Masks& m, int do_grad, int solid_mode,
+                                         const MK& m, int do_grad, int solid_mode,
                                          const uint8_t* __restrict__ solid, int64_t lds, double scale) {
-  bool zero = (i > 0 && solid_at(solid_mode, solid, lds, H, W, j, i - 1)) ||
-              (i < W && solid_at(solid_mode, solid, lds, H, W, j, i));
+  bool zero = (i > 0 && solid_at_t<SM>(solid_mode, solid, lds, H, W, j, i - 1)) ||
+              (i < W && solid_at_t<SM>(solid_mode, solid, lds, H, W, j, i));
   if (zero) return (T)0;
   if (!do_grad) return uk;
   if (m.u(j, i) && i > 0 && i < W) {
@@ -145,12 +145,12 @@ __device__ __forceinline__ T projected_u(int j, int i, int H, int W, T uk, const
 }
 
 // the same for v face (j, i) (j <= H, i < W)
-template <typename T>
+template <typename T, typename MK, int SM = -1>
 __device__ __forceinline__ T projected_v(int j, int i, int H, int W, T vk, const T* __restrict__ p, int64_t ldp,
-                                         const Masks& m, int do_grad, int solid_mode,
+                                         const MK& m, int do_grad, int solid_mode,
                                          const uint8_t* __restrict__ solid, int64_t lds, double scale) {
-  bool zero = (j > 0 && solid_at(solid_mode, solid, lds, H, W, j - 1, i)) ||
-              (j < H && solid_at(solid_mode, solid, lds, H, W, j, i));
+  bool zero = (j > 0 && solid_at_t<SM>(solid_mode, solid, lds, H, W, j - 1, i)) ||
+              (j < H && solid_at_t<SM>(solid_mode, solid, lds, H, W, j, i));
   if (zero) return (T)0;
   if (!do_grad) return vk;
   if (m.v(j, i) && j > 0 && j < H) {
@@ -161,18 +161,18 @@ __device__ __forceinline__ T projected_v(int j, int i, int H, int W, T vk, const
 }
 
 // Projection of u face (j, i) (j < H, i <= W) and v face (j, i) (j <= H, i < W) in place.
-template <typename T>
+template <typename T, typename MK, int SM = -1>
 __device__ __forceinline__ void project_faces(int j, int i, int H, int W, T* __restrict__ u, int64_t ldu,
                                               T* __restrict__ v, int64_t ldv, const T* __restrict__ p, int64_t ldp,
-                                              const Masks& m, int do_grad, int solid_mode,
+                                              const MK& m, int do_grad, int solid_mode,
                                               const uint8_t* __restrict__ solid, int64_t lds, double scale) {
   if (j < H && i <= W) {
     T* q = u + (int64_t)j * ldu + i;
-    *q = projected_u(j, i, H, W, *q, p, ldp, m, do_grad, solid_mode, solid, lds, scale);
+    *q = projected_u<T, MK, SM>(j, i, H, W, *q, p, ldp, m, do_grad, solid_mode, solid, lds, scale);
   }
   if (j <= H && i < W) {
     T* q = v + (int64_t)j * ldv + i;
-    *q = projected_v(j, i, H, W, *q, p, ldp, m, do_grad, solid_mode, solid, lds, scale);
+    *q = projected_v<T, MK, SM>(j, i, H, W, *q, p, ldp, m, do_grad, solid_mode, solid, lds, scale);
   }
 }
 
@@ -181,28 +181,28 @@ __device__ __forceinline__ void project_faces(int j, int i, int H, int W, T* __r
 // reference residual of p at the cell. The cell's right and upper faces belong to the
 // neighbouring threads; their projected values are recomputed here from the inputs (which
 // nobody writes), with the same expressions, so every value equals the separate passes'.
-template <typename T>
+template <typename T, typename MK, int SM = -1>
 __device__ __forceinline__ void project_metrics_point(int j, int i, int H, int W, const T* __restrict__ u_in,
                                                       int64_t ldui, const T* __restrict__ v_in, int64_t ldvi,
                                                       T* __restrict__ u_out, int64_t lduo, T* __restrict__ v_out,
                                                       int64_t ldvo, const T* __restrict__ p, int64_t ldp,
-                                                      const Masks& m, int solid_mode,
+                                                      const MK& m, int solid_mode,
                                                       const uint8_t* __restrict__ solid, int64_t lds, double scale,
                                                       T* __restrict__ div, int64_t ldd, double inv, double alpha,
                                                       double beta, T* __restrict__ res, int64_t ldr) {
   T ul = (T)0, vd = (T)0;
   if (j < H && i <= W) {
-    ul = projected_u(j, i, H, W, u_in[(int64_t)j * ldui + i], p, ldp, m, 1, solid_mode, solid, lds, scale);
+    ul = projected_u<T, MK, SM>(j, i, H, W, u_in[(int64_t)j * ldui + i], p, ldp, m, 1, solid_mode, solid, lds, scale);
     u_out[(int64_t)j * lduo + i] = ul;
   }
   if (j <= H && i < W) {
-    vd = projected_v(j, i, H, W, v_in[(int64_t)j * ldvi + i], p, ldp, m, 1, solid_mode, solid, lds, scale);
+    vd = projected_v<T, MK, SM>(j, i, H, W, v_in[(int64_t)j * ldvi + i], p, ldp, m, 1, solid_mode, solid, lds, scale);
     v_out[(int64_t)j * ldvo + i] = vd;
   }
   if (j >= H || i >= W) return;
-  const T ur = projected_u(j, i + 1, H, W, u_in[(int64_t)j * ldui + i + 1], p, ldp, m, 1, solid_mode, solid, lds,
+  const T ur = projected_u<T, MK, SM>(j, i + 1, H, W, u_in[(int64_t)j * ldui + i + 1], p, ldp, m, 1, solid_mode, solid, lds,
                            scale);
-  const T vu = projected_v(j + 1, i, H, W, v_in[(int64_t)(j + 1) * ldvi + i], p, ldp, m, 1, solid_mode, solid, lds,
+  const T vu = projected_v<T, MK, SM>(j + 1, i, H, W, v_in[(int64_t)(j + 1) * ldvi + i], p, ldp, m, 1, solid_mode, solid, lds,
                            scale);
   // divergence.py:4-25 on the projected faces
   T a = ur * (T)(m.u(j, i + 1) ? 1 : 0);

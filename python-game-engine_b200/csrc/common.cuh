@@ -52,6 +52,36 @@ unsigned long long launch_count();
     }                                                               \
   } while (0)
 
+// Compile-time mask kind MM (SG_MASK_OPEN / RING / PLANES) for a validated mask_mode.
+#define SG_MASK_DISPATCH(mask_mode, ...)                     \
+  do {                                                      \
+    if ((mask_mode) == SG_MASK_OPEN) {                      \
+      constexpr int MM = SG_MASK_OPEN;                      \
+      __VA_ARGS__                                           \
+    } else if ((mask_mode) == SG_MASK_RING) {               \
+      constexpr int MM = SG_MASK_RING;                      \
+      __VA_ARGS__                                           \
+    } else {                                                \
+      constexpr int MM = SG_MASK_PLANES;                    \
+      __VA_ARGS__                                           \
+    }                                                       \
+  } while (0)
+
+// Compile-time solid kind SM (SG_MASK_NONE / RING / PLANES) for a validated solid_mode.
+#define SG_SOLID_DISPATCH(solid_mode, ...)                   \
+  do {                                                      \
+    if ((solid_mode) == SG_MASK_NONE) {                     \
+      constexpr int SM = SG_MASK_NONE;                      \
+      __VA_ARGS__                                           \
+    } else if ((solid_mode) == SG_MASK_RING) {              \
+      constexpr int SM = SG_MASK_RING;                      \
+      __VA_ARGS__                                           \
+    } else {                                                \
+      constexpr int SM = SG_MASK_PLANES;                    \
+      __VA_ARGS__                                           \
+    }                                                       \
+  } while (0)
+
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // ------------------------------------------------------------------ launch shapes
@@ -75,8 +105,10 @@ __device__ __forceinline__ int row_of(int q) { return (blockIdx.y * kRows + q) *
 // ------------------------------------------------------------------ masks
 // Face/fluid masks of an H x W cell grid, either explicit planes (as the reference
 // passes them) or analytic: SG_MASK_OPEN (all interior faces open) or SG_MASK_RING
-// (a box whose outermost cells are solid).
-struct Masks {
+// (a box whose outermost cells are solid). MODE fixes the kind at compile time (the
+// analytic tests then fold into index comparisons); MODE = -1 reads it from `mode`.
+template <int MODE>
+struct MasksT {
   const uint8_t* fmu;
   int64_t ldu;
   const uint8_t* fmv;
@@ -86,28 +118,40 @@ struct Masks {
   int mode;
   int H, W;
 
+  __device__ __forceinline__ int kind() const { return MODE < 0 ? mode : MODE; }
   __device__ __forceinline__ bool u(int j, int i) const {
-    if (mode == SG_MASK_PLANES) return fmu[(int64_t)j * ldu + i] != 0;
-    if (mode == SG_MASK_OPEN) return i >= 1 && i <= W - 1;
+    if (kind() == SG_MASK_PLANES) return fmu[(int64_t)j * ldu + i] != 0;
+    if (kind() == SG_MASK_OPEN) return i >= 1 && i <= W - 1;
     return j >= 1 && j <= H - 2 && i >= 2 && i <= W - 2;
   }
   __device__ __forceinline__ bool v(int j, int i) const {
-    if (mode == SG_MASK_PLANES) return fmv[(int64_t)j * ldv + i] != 0;
-    if (mode == SG_MASK_OPEN) return j >= 1 && j <= H - 1;
+    if (kind() == SG_MASK_PLANES) return fmv[(int64_t)j * ldv + i] != 0;
+    if (kind() == SG_MASK_OPEN) return j >= 1 && j <= H - 1;
     return i >= 1 && i <= W - 2 && j >= 2 && j <= H - 2;
   }
   // common/simulation.py:108: a cell is fluid when any of its four faces is open.
   __device__ __forceinline__ bool fluid(int j, int i) const {
-    if (mode == SG_MASK_PLANES && fl) return fl[(int64_t)j * ldf + i] != 0;
+    if (kind() == SG_MASK_PLANES && fl) return fl[(int64_t)j * ldf + i] != 0;
     return u(j, i) || u(j, i + 1) || v(j, i) || v(j + 1, i);
   }
+  template <int M>
+  __host__ __device__ MasksT<M> as() const {
+    return MasksT<M>{fmu, ldu, fmv, ldv, fl, ldf, mode, H, W};
+  }
 };
+using Masks = MasksT<-1>;
 
-// Solid cell test of boundaries.py:7-39 (plane: value 1; ring: the outermost cells).
-__device__ __forceinline__ bool solid_at(int mode, const uint8_t* s, int64_t ld, int H, int W, int j, int i) {
-  if (mode == SG_MASK_PLANES) return s[(int64_t)j * ld + i] == 1;
-  if (mode == SG_MASK_RING) return j == 0 || j == H - 1 || i == 0 || i == W - 1;
+// Solid cell test of boundaries.py:7-39 (plane: value 1; ring: the outermost cells);
+// SM fixes the mode at compile time, -1 takes `mode`.
+template <int SM>
+__device__ __forceinline__ bool solid_at_t(int mode, const uint8_t* s, int64_t ld, int H, int W, int j, int i) {
+  const int md = SM < 0 ? mode : SM;
+  if (md == SG_MASK_PLANES) return s[(int64_t)j * ld + i] == 1;
+  if (md == SG_MASK_RING) return j == 0 || j == H - 1 || i == 0 || i == W - 1;
   return false;
+}
+__device__ __forceinline__ bool solid_at(int mode, const uint8_t* s, int64_t ld, int H, int W, int j, int i) {
+  return solid_at_t<-1>(mode, s, ld, H, W, j, i);
 }
 
 inline Masks make_masks(int mode, int64_t H, int64_t W, const uint8_t* fmu, int64_t ldu, const uint8_t* fmv,
@@ -139,21 +183,33 @@ __device__ __forceinline__ double lerp_ref(T a, T b, double t) {
   return (double)a + (double)d * t;
 }
 
-// floor/ceil are taken with saturating 32-bit conversions (cvt.rmi / cvt.rpi): after the
-// clamp to [0, n-1] they give the same indices as the reference's int(math.floor(x)) for
-// every double, NaN and +-Inf included (both end at an edge index).
+constexpr double kMagicInt = 4503599627370496.0;  // 2^52
+
+// Exact double of 0 <= k < 2^31 without a conversion instruction (the conversion unit is
+// the busiest pipe of the advection kernels): the double whose high word is that of 2^52
+// and whose low word is k equals 2^52 + k.
+__device__ __forceinline__ double idx_double(int k) { return __hiloint2double(0x43300000, k) - kMagicInt; }
+
+// Clamped floor / ceil of x on [0, n] (n = length - 1) as the reference takes them
+// (int(math.floor(x)), int(math.ceil(x)), then clamp; advection.py:31-38), f0 = (double)i0.
+// Saturating 32-bit conversions (cvt.rmi / cvt.rpi) give, after the clamp, the reference's
+// indices for every double, NaN and +-Inf included (both end at an edge index).
+__device__ __forceinline__ void bracket(double x, int n, int& i0, int& i1, double& f0) {
+  i0 = min(max(__double2int_rd(x), 0), n);
+  i1 = min(max(__double2int_ru(x), 0), n);
+  f0 = idx_double(i0);
+}
+
 template <typename T>
 __device__ __forceinline__ double sample_ref(const T* __restrict__ f, int64_t ld, int64_t rows, int64_t cols,
                                              double x, double y) {
   const int nc = (int)cols - 1, nr = (int)rows - 1;
-  int x0 = __double2int_rd(x), x1 = __double2int_ru(x);
-  int y0 = __double2int_rd(y), y1 = __double2int_ru(y);
-  x0 = min(max(x0, 0), nc);
-  x1 = min(max(x1, 0), nc);
-  y0 = min(max(y0, 0), nr);
-  y1 = min(max(y1, 0), nr);
-  double tx = x - (double)x0;
-  double ty = y - (double)y0;
+  int x0, x1, y0, y1;
+  double fx, fy;
+  bracket(x, nc, x0, x1, fx);
+  bracket(y, nr, y0, y1, fy);
+  double tx = x - fx;
+  double ty = y - fy;
   const T* r0 = f + (int64_t)y0 * ld;
   const T* r1 = f + (int64_t)y1 * ld;
   T c00 = r0[x0], c10 = r0[x1];

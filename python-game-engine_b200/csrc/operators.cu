@@ -48,10 +48,10 @@ unsigned long long launch_count() { return g_launches.load(std::memory_order_rel
 
 // ------------------------------------------------------------------ advection
 // advection.py:112-128 (+ dissipation, simulation.py:232)
-template <typename T>
+template <typename T, int MM>
 __global__ void k_advect_scalar(int H, int W, const T* __restrict__ src, int64_t lds, T* __restrict__ dst, int64_t ldd,
                                 const T* __restrict__ u, int64_t ur, int64_t uc, int64_t ldu,
-                                const T* __restrict__ v, int64_t vr, int64_t vc, int64_t ldv, Masks m,
+                                const T* __restrict__ v, int64_t vr, int64_t vc, int64_t ldv, MasksT<MM> m,
                                 double dt, double inv, T diss) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= W) return;
@@ -83,9 +83,9 @@ __global__ void k_advect_v(int vr, int vc, const T* __restrict__ vs, int64_t ldv
 }
 
 // Both faces of the MAC grid in one launch (grid covers (W+1) x (H+1)).
-template <typename T>
+template <typename T, int MM>
 __global__ void k_advect_uv(int H, int W, const T* __restrict__ us, int64_t ldus, T* __restrict__ ud, int64_t ldud,
-                            const T* __restrict__ vs, int64_t ldvs, T* __restrict__ vd, int64_t ldvd, Masks m,
+                            const T* __restrict__ vs, int64_t ldvs, T* __restrict__ vd, int64_t ldvd, MasksT<MM> m,
                             double dt, double inv) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
 #pragma unroll
@@ -129,9 +129,9 @@ __global__ void k_cool(int H, int W, T* __restrict__ t, int64_t ld, double amb, 
 
 // ------------------------------------------------------------------ divergence
 // divergence.py:4-25
-template <typename T>
+template <typename T, int MM>
 __global__ void k_divergence(int H, int W, const T* __restrict__ u, int64_t ldu, const T* __restrict__ v, int64_t ldv,
-                             T* __restrict__ div, int64_t ldd, Masks m, double inv) {
+                             T* __restrict__ div, int64_t ldd, MasksT<MM> m, double inv) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= W) return;
 #pragma unroll
@@ -143,9 +143,9 @@ __global__ void k_divergence(int H, int W, const T* __restrict__ u, int64_t ldu,
 
 // ------------------------------------------------------------------ residual
 // residual.py:6-42 (+ optional sum of squares)
-template <typename T>
+template <typename T, int MM>
 __global__ void k_residual(int H, int W, const T* __restrict__ p, int64_t ldp, const T* __restrict__ div, int64_t ldd,
-                           Masks m, double alpha, double beta, T* __restrict__ out, int64_t ldo, double* sumsq) {
+                           MasksT<MM> m, double alpha, double beta, T* __restrict__ out, int64_t ldo, double* sumsq) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double sq = 0.0;
 #pragma unroll
@@ -165,21 +165,22 @@ __global__ void k_residual(int H, int W, const T* __restrict__ p, int64_t ldp, c
 
 // ------------------------------------------------------------------ projection
 // pressure_gradient.py:4-37 then, if solid_mode != SG_MASK_NONE, boundaries.py:7-39.
-template <typename T>
+template <typename T, int MM, int SM>
 __global__ void k_project(int H, int W, T* __restrict__ u, int64_t ldu, T* __restrict__ v, int64_t ldv,
-                          const T* __restrict__ p, int64_t ldp, Masks m, int do_grad, int solid_mode,
+                          const T* __restrict__ p, int64_t ldp, MasksT<MM> m, int do_grad, int solid_mode,
                           const uint8_t* __restrict__ solid, int64_t lds, double scale) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
 #pragma unroll
   for (int q = 0; q < kRows; ++q)
-    project_faces(row_of(q), i, H, W, u, ldu, v, ldv, p, ldp, m, do_grad, solid_mode, solid, lds, scale);
+    project_faces<T, MasksT<MM>, SM>(row_of(q), i, H, W, u, ldu, v, ldv, p, ldp, m, do_grad, solid_mode, solid, lds,
+                                     scale);
 }
 
 // The substep's tail: projection out of place, divergence and residual in one pass.
-template <typename T>
+template <typename T, int MM, int SM>
 __global__ void k_project_metrics(int H, int W, const T* __restrict__ ui, int64_t ldui, const T* __restrict__ vi,
                                   int64_t ldvi, T* __restrict__ uo, int64_t lduo, T* __restrict__ vo, int64_t ldvo,
-                                  const T* __restrict__ p, int64_t ldp, Masks m, int solid_mode,
+                                  const T* __restrict__ p, int64_t ldp, MasksT<MM> m, int solid_mode,
                                   const uint8_t* __restrict__ solid, int64_t lds, double scale, T* __restrict__ div,
                                   int64_t ldd, double inv, double alpha, double beta, T* __restrict__ res,
                                   int64_t ldr) {
@@ -188,8 +189,8 @@ __global__ void k_project_metrics(int H, int W, const T* __restrict__ ui, int64_
   for (int q = 0; q < kRows; ++q) {
     const int j = row_of(q);
     if (j <= H && i <= W)
-      project_metrics_point(j, i, H, W, ui, ldui, vi, ldvi, uo, lduo, vo, ldvo, p, ldp, m, solid_mode, solid, lds,
-                            scale, div, ldd, inv, alpha, beta, res, ldr);
+      project_metrics_point<T, MasksT<MM>, SM>(j, i, H, W, ui, ldui, vi, ldvi, uo, lduo, vo, ldvo, p, ldp, m,
+                                               solid_mode, solid, lds, scale, div, ldd, inv, alpha, beta, res, ldr);
   }
 }
 
@@ -420,9 +421,11 @@ int sg_advect_scalar(int dtype, int64_t H, int64_t W, const void* src, int64_t l
   Masks m = make_masks(mask_mode, H, W, nullptr, 0, nullptr, 0, is_fluid, ld_fluid);
   if (mask_mode == SG_MASK_PLANES) m.mode = SG_MASK_PLANES;
   SG_DISPATCH(dtype, {
-    SG_LAUNCH(k_advect_scalar<T><<<grid2d_rows(W, H), block2d(), 0, as_stream(stream)>>>(
-        (int)H, (int)W, (const T*)src, ld_src, (T*)dst, ld_dst, (const T*)u, u_rows, u_cols, ld_u, (const T*)v, v_rows,
-        v_cols, ld_v, m, dt, 1.0 / cell_size, (T)dissipation));
+    SG_MASK_DISPATCH(mask_mode, {
+      SG_LAUNCH(k_advect_scalar<T, MM><<<grid2d_rows(W, H), block2d(), 0, as_stream(stream)>>>(
+          (int)H, (int)W, (const T*)src, ld_src, (T*)dst, ld_dst, (const T*)u, u_rows, u_cols, ld_u, (const T*)v,
+          v_rows, v_cols, ld_v, m.as<MM>(), dt, 1.0 / cell_size, (T)dissipation));
+    });
   });
   return check_launch("sg_advect_scalar");
 }
@@ -471,9 +474,11 @@ int sg_advect_velocity(int dtype, int64_t H, int64_t W, const void* u_src, int64
   SG_CHECK(check_mask_mode(mask_mode, fmu, fmv));
   Masks m = make_masks(mask_mode, H, W, fmu, ld_fmu, fmv, ld_fmv, nullptr, 0);
   SG_DISPATCH(dtype, {
-    SG_LAUNCH(k_advect_uv<T><<<grid2d_rows(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
-        (int)H, (int)W, (const T*)u_src, ld_us, (T*)u_dst, ld_ud, (const T*)v_src, ld_vs, (T*)v_dst, ld_vd, m, dt,
-        1.0 / cell_size));
+    SG_MASK_DISPATCH(mask_mode, {
+      SG_LAUNCH(k_advect_uv<T, MM><<<grid2d_rows(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
+          (int)H, (int)W, (const T*)u_src, ld_us, (T*)u_dst, ld_ud, (const T*)v_src, ld_vs, (T*)v_dst, ld_vd,
+          m.as<MM>(), dt, 1.0 / cell_size));
+    });
   });
   return check_launch("sg_advect_velocity");
 }
@@ -513,8 +518,10 @@ int sg_compute_divergence(int dtype, int64_t H, int64_t W, const void* u, int64_
   SG_CHECK(check_mask_mode(mask_mode, fmu, fmv));
   Masks m = make_masks(mask_mode, H, W, fmu, ld_fmu, fmv, ld_fmv, nullptr, 0);
   SG_DISPATCH(dtype, {
-    SG_LAUNCH(k_divergence<T><<<grid2d_rows(W, H), block2d(), 0, as_stream(stream)>>>((int)H, (int)W, (const T*)u, ld_u, (const T*)v,
-                                                                        ld_v, (T*)div, ld_div, m, 1.0 / cell_size));
+    SG_MASK_DISPATCH(mask_mode, {
+      SG_LAUNCH(k_divergence<T, MM><<<grid2d_rows(W, H), block2d(), 0, as_stream(stream)>>>(
+          (int)H, (int)W, (const T*)u, ld_u, (const T*)v, ld_v, (T*)div, ld_div, m.as<MM>(), 1.0 / cell_size));
+    });
   });
   return check_launch("sg_compute_divergence");
 }
@@ -530,9 +537,11 @@ int sg_compute_residual(int dtype, int64_t H, int64_t W, const void* p, int64_t 
   SG_CHECK(check_mask_mode(mask_mode, fmu, fmv));
   Masks m = make_masks(mask_mode, H, W, fmu, ld_fmu, fmv, ld_fmv, is_fluid, ld_fluid);
   SG_DISPATCH(dtype, {
-    SG_LAUNCH(k_residual<T><<<grid2d_rows(W, H), block2d(), 0, as_stream(stream)>>>((int)H, (int)W, (const T*)p, ld_p,
-                                                                      (const T*)div, ld_div, m, alpha,
-                                                                      1.0 / reciprocal_beta, (T*)out, ld_out, sumsq));
+    SG_MASK_DISPATCH(mask_mode, {
+      SG_LAUNCH(k_residual<T, MM><<<grid2d_rows(W, H), block2d(), 0, as_stream(stream)>>>(
+          (int)H, (int)W, (const T*)p, ld_p, (const T*)div, ld_div, m.as<MM>(), alpha, 1.0 / reciprocal_beta, (T*)out,
+          ld_out, sumsq));
+    });
   });
   return check_launch("sg_compute_residual");
 }
@@ -554,8 +563,11 @@ int sg_enforce_boundary_conditions(int dtype, int64_t H, int64_t W, void* u, int
   if (solid_mode == SG_MASK_NONE) return SG_OK;
   Masks m = make_masks(SG_MASK_OPEN, H, W, nullptr, 0, nullptr, 0, nullptr, 0);
   SG_DISPATCH(dtype, {
-    SG_LAUNCH(k_project<T><<<grid2d_rows(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
-        (int)H, (int)W, (T*)u, ld_u, (T*)v, ld_v, (const T*)nullptr, 0, m, 0, solid_mode, solid, ld_s, 0.0));
+    SG_SOLID_DISPATCH(solid_mode, {
+      SG_LAUNCH(k_project<T, SG_MASK_OPEN, SM><<<grid2d_rows(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
+          (int)H, (int)W, (T*)u, ld_u, (T*)v, ld_v, (const T*)nullptr, 0, m.as<SG_MASK_OPEN>(), 0, solid_mode, solid,
+          ld_s, 0.0));
+    });
   });
   return check_launch("sg_enforce_boundary_conditions");
 }
@@ -574,8 +586,13 @@ int sg_project(int dtype, int64_t H, int64_t W, void* u, int64_t ld_u, void* v, 
   Masks m = make_masks(mask_mode, H, W, fmu, ld_fmu, fmv, ld_fmv, nullptr, 0);
   double scale = dt / (fluid_density * cell_size);
   SG_DISPATCH(dtype, {
-    SG_LAUNCH(k_project<T><<<grid2d_rows(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
-        (int)H, (int)W, (T*)u, ld_u, (T*)v, ld_v, (const T*)p, ld_p, m, 1, solid_mode, solid, ld_s, scale));
+    SG_MASK_DISPATCH(mask_mode, {
+      SG_SOLID_DISPATCH(solid_mode, {
+        SG_LAUNCH(k_project<T, MM, SM><<<grid2d_rows(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
+            (int)H, (int)W, (T*)u, ld_u, (T*)v, ld_v, (const T*)p, ld_p, m.as<MM>(), 1, solid_mode, solid, ld_s,
+            scale));
+      });
+    });
   });
   return check_launch("sg_project");
 }
@@ -599,10 +616,14 @@ int sg_project_metrics(int dtype, int64_t H, int64_t W, const void* u_in, int64_
   Masks m = make_masks(mask_mode, H, W, fmu, ld_fmu, fmv, ld_fmv, is_fluid, ld_fluid);
   const double scale = dt / (fluid_density * cell_size);
   SG_DISPATCH(dtype, {
-    SG_LAUNCH(k_project_metrics<T><<<grid2d_rows(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
-        (int)H, (int)W, (const T*)u_in, ld_ui, (const T*)v_in, ld_vi, (T*)u_out, ld_uo, (T*)v_out, ld_vo,
-        (const T*)p, ld_p, m, solid_mode, solid, ld_s, scale, (T*)div, ld_div, 1.0 / cell_size, alpha,
-        1.0 / reciprocal_beta, (T*)res, ld_res));
+    SG_MASK_DISPATCH(mask_mode, {
+      SG_SOLID_DISPATCH(solid_mode, {
+        SG_LAUNCH(k_project_metrics<T, MM, SM><<<grid2d_rows(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
+            (int)H, (int)W, (const T*)u_in, ld_ui, (const T*)v_in, ld_vi, (T*)u_out, ld_uo, (T*)v_out, ld_vo,
+            (const T*)p, ld_p, m.as<MM>(), solid_mode, solid, ld_s, scale, (T*)div, ld_div, 1.0 / cell_size, alpha,
+            1.0 / reciprocal_beta, (T*)res, ld_res));
+      });
+    });
   });
   return check_launch("sg_project_metrics");
 }
