@@ -176,50 +176,61 @@ __device__ __forceinline__ void project_faces(int j, int i, int H, int W, T* __r
   }
 }
 
-// The substep's tail in one pass (simulation.py:244-265): project the faces of cell (j, i)
-// from (u_in, v_in) into (u_out, v_out), then the divergence of the projected field and the
-// reference residual of p at the cell. The cell's right and upper faces belong to the
-// neighbouring threads; their projected values are recomputed here from the inputs (which
-// nobody writes), with the same expressions, so every value equals the separate passes'.
-template <typename T, typename MK, int SM = -1>
-__device__ __forceinline__ void project_metrics_point(int j, int i, int H, int W, const T* __restrict__ u_in,
-                                                      int64_t ldui, const T* __restrict__ v_in, int64_t ldvi,
-                                                      T* __restrict__ u_out, int64_t lduo, T* __restrict__ v_out,
-                                                      int64_t ldvo, const T* __restrict__ p, int64_t ldp,
-                                                      const MK& m, int solid_mode,
-                                                      const uint8_t* __restrict__ solid, int64_t lds, double scale,
-                                                      T* __restrict__ div, int64_t ldd, double inv, double alpha,
-                                                      double beta, T* __restrict__ res, int64_t ldr) {
-  T ul = (T)0, vd = (T)0;
-  if (j < H && i <= W) {
-    ul = projected_u<T, MK, SM>(j, i, H, W, u_in[(int64_t)j * ldui + i], p, ldp, m, 1, solid_mode, solid, lds, scale);
-    u_out[(int64_t)j * lduo + i] = ul;
+// projected_u / projected_v (gradient branch) from the pressure values at the face's two
+// cells, pc = p(j, i) and pn = p(j, i - 1) (u) or p(j - 1, i) (v), with the same
+// expressions; the values are read only where the reference reads them.
+template <typename T, typename MK, int SM>
+__device__ __forceinline__ T projected_u_pv(int j, int i, int H, int W, T uk, T pc, T pn, const MK& m, int solid_mode,
+                                           const uint8_t* __restrict__ solid, int64_t lds, double scale) {
+  bool zero = (i > 0 && solid_at_t<SM>(solid_mode, solid, lds, H, W, j, i - 1)) ||
+              (i < W && solid_at_t<SM>(solid_mode, solid, lds, H, W, j, i));
+  if (zero) return (T)0;
+  if (m.u(j, i) && i > 0 && i < W) {
+    T dp = pc - pn;
+    return (T)((double)uk - scale * (double)dp);
   }
-  if (j <= H && i < W) {
-    vd = projected_v<T, MK, SM>(j, i, H, W, v_in[(int64_t)j * ldvi + i], p, ldp, m, 1, solid_mode, solid, lds, scale);
-    v_out[(int64_t)j * ldvo + i] = vd;
+  return (T)0;
+}
+
+template <typename T, typename MK, int SM>
+__device__ __forceinline__ T projected_v_pv(int j, int i, int H, int W, T vk, T pc, T pn, const MK& m, int solid_mode,
+                                           const uint8_t* __restrict__ solid, int64_t lds, double scale) {
+  bool zero = (j > 0 && solid_at_t<SM>(solid_mode, solid, lds, H, W, j - 1, i)) ||
+              (j < H && solid_at_t<SM>(solid_mode, solid, lds, H, W, j, i));
+  if (zero) return (T)0;
+  if (m.v(j, i) && j > 0 && j < H) {
+    T dp = pc - pn;
+    return (T)((double)vk - scale * (double)dp);
   }
-  if (j >= H || i >= W) return;
-  const T ur = projected_u<T, MK, SM>(j, i + 1, H, W, u_in[(int64_t)j * ldui + i + 1], p, ldp, m, 1, solid_mode, solid, lds,
-                           scale);
-  const T vu = projected_v<T, MK, SM>(j + 1, i, H, W, v_in[(int64_t)(j + 1) * ldvi + i], p, ldp, m, 1, solid_mode, solid, lds,
-                           scale);
-  // divergence.py:4-25 on the projected faces
+  return (T)0;
+}
+
+// divergence.py:4-25 of cell (j, i) from its four face values (ul, ur: u faces i, i + 1;
+// vd, vu: v faces j, j + 1).
+template <typename T, typename MK>
+__device__ __forceinline__ T divergence_from_faces(int j, int i, T ul, T ur, T vd, T vu, const MK& m, double inv) {
   T a = ur * (T)(m.u(j, i + 1) ? 1 : 0);
   T b = ul * (T)(m.u(j, i) ? 1 : 0);
   T c = vu * (T)(m.v(j + 1, i) ? 1 : 0);
   T e = vd * (T)(m.v(j, i) ? 1 : 0);
   T du = a - b, dv = c - e;
-  const T dval = (T)((double)du * inv + (double)dv * inv);
-  div[(int64_t)j * ldd + i] = dval;
-  // residual.py:6-42 with that divergence
-  T r = (T)0;
-  if (m.fluid(j, i)) {
-    T cc = p[(int64_t)j * ldp + i];
-    T s = nbsum_ref(p, ldp, H, W, j, i, m, cc);
-    r = (T)(((double)s + alpha * (double)dval) - beta * (double)cc);
-  }
-  res[(int64_t)j * ldr + i] = r;
+  return (T)((double)du * inv + (double)dv * inv);
+}
+
+// residual.py:6-42 of cell (j, i) from the pressure values around it (pl, pr, pd, pu: the
+// neighbours at i - 1, i + 1, j - 1, j + 1, read only inside the grid) and its divergence.
+template <typename T, typename MK>
+__device__ __forceinline__ T residual_from_values(int j, int i, int H, int W, T c, T pl, T pr, T pd, T pu, T dval,
+                                                  const MK& m, double alpha, double beta) {
+  if (!m.fluid(j, i)) return (T)0;
+  T l = m.u(j, i) ? (i > 0 ? pl : c) : c;  // p[j, max(i - 1, 0)]
+  T r = m.u(j, i + 1) ? (i < W - 1 ? pr : c) : c;
+  T d = m.v(j, i) ? (j > 0 ? pd : c) : c;
+  T up = m.v(j + 1, i) ? (j < H - 1 ? pu : c) : c;
+  T s = l + r;
+  s = s + d;
+  s = s + up;
+  return (T)(((double)s + alpha * (double)dval) - beta * (double)c);
 }
 
 // Overwriting disc sources at cell (j, i), u face (j, i) and v face (j, i) (j <= H, i <= W):

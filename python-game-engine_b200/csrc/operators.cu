@@ -176,21 +176,67 @@ __global__ void k_project(int H, int W, T* __restrict__ u, int64_t ldu, T* __res
                                      scale);
 }
 
-// The substep's tail: projection out of place, divergence and residual in one pass.
+// The substep's tail in one pass (simulation.py:244-265): the projection of (ui, vi) into
+// (uo, vo) (out of place), the divergence of the projected field and the reference residual
+// of p. A warp owns 32 consecutive columns and walks kTailRows rows down them: the pressure
+// of the next row and the v face above the current row are computed one row ahead and
+// carried in registers, the horizontal neighbours (p at i -+ 1, the u face at i + 1) come
+// from the adjacent lane, so each face is projected once (plus one u face per warp edge and
+// row). Every value is formed by the same expressions as the separate passes, so the
+// results are identical to them.
+constexpr int kTailRows = 8;
+
 template <typename T, int MM, int SM>
-__global__ void k_project_metrics(int H, int W, const T* __restrict__ ui, int64_t ldui, const T* __restrict__ vi,
-                                  int64_t ldvi, T* __restrict__ uo, int64_t lduo, T* __restrict__ vo, int64_t ldvo,
-                                  const T* __restrict__ p, int64_t ldp, MasksT<MM> m, int solid_mode,
-                                  const uint8_t* __restrict__ solid, int64_t lds, double scale, T* __restrict__ div,
-                                  int64_t ldd, double inv, double alpha, double beta, T* __restrict__ res,
-                                  int64_t ldr) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-#pragma unroll
-  for (int q = 0; q < kRows; ++q) {
-    const int j = row_of(q);
-    if (j <= H && i <= W)
-      project_metrics_point<T, MasksT<MM>, SM>(j, i, H, W, ui, ldui, vi, ldvi, uo, lduo, vo, ldvo, p, ldp, m,
-                                               solid_mode, solid, lds, scale, div, ldd, inv, alpha, beta, res, ldr);
+__global__ void __launch_bounds__(kBX * kBY) k_project_metrics(
+    int H, int W, const T* __restrict__ ui, int64_t ldui, const T* __restrict__ vi, int64_t ldvi, T* __restrict__ uo,
+    int64_t lduo, T* __restrict__ vo, int64_t ldvo, const T* __restrict__ p, int64_t ldp, MasksT<MM> m, int solid_mode,
+    const uint8_t* __restrict__ solid, int64_t lds, double scale, T* __restrict__ div, int64_t ldd, double inv,
+    double alpha, double beta, T* __restrict__ res, int64_t ldr) {
+  using MK = MasksT<MM>;
+  const int lane = threadIdx.x;  // blockDim.x == 32: a warp is one row segment
+  const int i = blockIdx.x * kBX + lane;
+  const int j0 = (blockIdx.y * kBY + threadIdx.y) * kTailRows;
+  if (j0 >= H) return;  // uniform over the warp
+  const bool cell = i < W, ucol = i <= W;
+  const T* pc_col = p + i;
+  T p_dn = (cell && j0 > 0) ? pc_col[(int64_t)(j0 - 1) * ldp] : (T)0;
+  T p_c = cell ? pc_col[(int64_t)j0 * ldp] : (T)0;
+  T v_lo = (T)0;  // projected v face (j, i) of the current row
+  if (cell) {
+    v_lo = projected_v_pv<T, MK, SM>(j0, i, H, W, vi[(int64_t)j0 * ldvi + i], p_c, p_dn, m, solid_mode, solid, lds,
+                                     scale);
+    if (j0 == 0) vo[i] = v_lo;
+  }
+  const int jend = min(j0 + kTailRows, H);
+#pragma unroll 2
+  for (int j = j0; j < jend; ++j) {
+    const T p_up = (cell && j + 1 < H) ? pc_col[(int64_t)(j + 1) * ldp] : (T)0;
+    const T uin = ucol ? ui[(int64_t)j * ldui + i] : (T)0;
+    const T vin = cell ? vi[(int64_t)(j + 1) * ldvi + i] : (T)0;
+    T p_l = __shfl_up_sync(0xffffffffu, p_c, 1);
+    T p_r = __shfl_down_sync(0xffffffffu, p_c, 1);
+    if (lane == 0) p_l = (i > 0 && i - 1 < W) ? pc_col[(int64_t)j * ldp - 1] : (T)0;
+    if (lane == kBX - 1) p_r = (i + 1 < W) ? pc_col[(int64_t)j * ldp + 1] : (T)0;
+    T ul = (T)0;
+    if (ucol) {
+      ul = projected_u_pv<T, MK, SM>(j, i, H, W, uin, p_c, p_l, m, solid_mode, solid, lds, scale);
+      uo[(int64_t)j * lduo + i] = ul;
+    }
+    T ur = __shfl_down_sync(0xffffffffu, ul, 1);
+    if (lane == kBX - 1 && i + 1 <= W)
+      ur = projected_u_pv<T, MK, SM>(j, i + 1, H, W, ui[(int64_t)j * ldui + i + 1], p_r, p_c, m, solid_mode, solid,
+                                     lds, scale);
+    if (cell) {
+      const T v_hi = projected_v_pv<T, MK, SM>(j + 1, i, H, W, vin, p_up, p_c, m, solid_mode, solid, lds, scale);
+      vo[(int64_t)(j + 1) * ldvo + i] = v_hi;
+      const T dval = divergence_from_faces<T, MK>(j, i, ul, ur, v_lo, v_hi, m, inv);
+      div[(int64_t)j * ldd + i] = dval;
+      res[(int64_t)j * ldr + i] = residual_from_values<T, MK>(j, i, H, W, p_c, p_l, p_r, p_dn, p_up, dval, m, alpha,
+                                                               beta);
+      v_lo = v_hi;
+    }
+    p_dn = p_c;
+    p_c = p_up;
   }
 }
 
@@ -618,7 +664,9 @@ int sg_project_metrics(int dtype, int64_t H, int64_t W, const void* u_in, int64_
   SG_DISPATCH(dtype, {
     SG_MASK_DISPATCH(mask_mode, {
       SG_SOLID_DISPATCH(solid_mode, {
-        SG_LAUNCH(k_project_metrics<T, MM, SM><<<grid2d_rows(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
+        SG_LAUNCH(k_project_metrics<T, MM, SM><<<dim3((unsigned)((W + 1 + kBX - 1) / kBX),
+                                                       (unsigned)((H + kBY * kTailRows - 1) / (kBY * kTailRows))),
+                                                  block2d(), 0, as_stream(stream)>>>(
             (int)H, (int)W, (const T*)u_in, ld_ui, (const T*)v_in, ld_vi, (T*)u_out, ld_uo, (T*)v_out, ld_vo,
             (const T*)p, ld_p, m.as<MM>(), solid_mode, solid, ld_s, scale, (T*)div, ld_div, 1.0 / cell_size, alpha,
             1.0 / reciprocal_beta, (T*)res, ld_res));

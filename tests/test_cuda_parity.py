@@ -236,17 +236,18 @@ def test_emitters_vs_reference(approach):
 
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
 @pytest.mark.parametrize("planes", [False, True])
-def test_fused_tail_equals_separate_operators(dtype, planes):
+@pytest.mark.parametrize("H, W", [(67, 90), (64, 31), (9, 33), (3, 65), (130, 64)])
+def test_fused_tail_equals_separate_operators(dtype, planes, H, W):
     """project_metrics (projection out of place + divergence + residual in one pass) must
-    give bit for bit what project, compute_divergence and compute_residual give."""
-    H, W = 67, 90
+    give bit for bit what project, compute_divergence and compute_residual give (shapes
+    with partial warps, partial row strips and warp-edge columns)."""
     g = torch.Generator().manual_seed(11)
     r = lambda *s: torch.randn(s, generator=g, dtype=torch.float64).to(dtype).cuda()  # noqa: E731
     u, v, p = r(H, W + 1), r(H + 1, W), r(H, W)
     if planes:
         solid = torch.zeros((H, W), dtype=torch.bool)
         solid[0, :] = solid[-1, :] = solid[:, 0] = solid[:, -1] = True
-        solid[20:30, 40:55] = True
+        solid[H // 3:H // 2 + 1, W // 3:W // 2 + 1] = True
         fmu, fmv, fl = sg.operators.build_masks(solid.cuda())
         solid_arg = solid.cuda()
     else:
