@@ -192,12 +192,14 @@ __device__ __forceinline__ double idx_double(int k) { return __hiloint2double(0x
 
 // Clamped floor / ceil of x on [0, n] (n = length - 1) as the reference takes them
 // (int(math.floor(x)), int(math.ceil(x)), then clamp; advection.py:31-38), f0 = (double)i0.
-// Saturating 32-bit conversions (cvt.rmi / cvt.rpi) give, after the clamp, the reference's
-// indices for every double, NaN and +-Inf included (both end at an edge index).
+// The saturating 32-bit conversion cvt.rmi gives, after the clamp, the reference's floor
+// index for every double, NaN and +-Inf included (both end at an edge index).
 __device__ __forceinline__ void bracket(double x, int n, int& i0, int& i1, double& f0) {
   i0 = min(max(__double2int_rd(x), 0), n);
-  i1 = min(max(__double2int_ru(x), 0), n);
   f0 = idx_double(i0);
+  // the clamped ceiling is the floor index, plus one where x lies above it (NaN, +-Inf and
+  // integral x included: those stay at the floor index, as the saturating cvt.rpi would)
+  i1 = min(i0 + (x > f0 ? 1 : 0), n);
 }
 
 template <typename T>
