@@ -4,9 +4,9 @@
 
 Workload ``mixed_2048``: one SmokeSimulation2D substep of the 2048^2 four-source
 scene (float32 state), pressure solved by the convergent multigrid (V(2,2),
-red-black Gauss-Seidel omega 1.4, full weighting, bilinear prolongation, 8^2
-coarsest) with FP32 cycles inside FP64 iterative refinement to a relative residual
-of 1e-8, then projection and the reference's metrics tail. The same scene is also
+red-black Gauss-Seidel omega 1.4, full weighting, bilinear prolongation, the 32^2
+coarsest level solved exactly by the cosine transform) with FP32 cycles inside FP64
+iterative refinement to a relative residual of 1e-8 (and, in a short second run, 1e-10), then projection and the reference's metrics tail. The same scene is also
 timed with a float64 state and an all-FP64 solve to the same residual ("fp64_gpu").
 
 A step runs on data resident in HBM (``value``); ``e2e`` repeats it through the
@@ -39,6 +39,8 @@ sys.path.insert(0, ROOT)
 METRIC = "cell-steps/s at 2048² mixed vs FP64 GPU at equal resid 1e-8; % HBM roofline"
 UNIT = "cell-steps/s"
 TOL = 1e-8
+TOL_TIGHT = 1e-10  # the workload's second residual target
+COARSEST = 32  # exact coarsest level (open box: cosine transform); the hierarchy is 2048^2 .. 32^2
 
 
 def _peaks():
@@ -263,9 +265,10 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def make(dtype, precision):
-        params = sg.GeometricMultigridParams(tol=TOL, max_cycles=40, precision=precision, omega=1.4,
-                                             fixed_cycles=args.fixed_cycles)
+    def make(dtype, precision, tol=TOL, remove_mean=False):
+        params = sg.GeometricMultigridParams(tol=tol, max_cycles=40, precision=precision, omega=1.4,
+                                             coarsest=COARSEST, fixed_cycles=args.fixed_cycles,
+                                             remove_mean=remove_mean)
         return sg.scenes.make_sim(sc, "geometric_multigrid", params, dtype=dtype, device=dev)
 
     solver = sg.get_solver("geometric_multigrid", "cuda")
@@ -420,13 +423,28 @@ def run_ours(args):
     value64 = world * cells * args.steps / (ms64 / 1e3)
     fp64_ok = info64["failures"] == 0 and info64["solves"] == args.steps
     del sim64
+    # ---- the second tolerance of the workload: both paths to 1e-10 (a short timed run each).
+    # The float32 state's divergence sums to zero only up to rounding, which leaves a constant
+    # part of the rhs near 1e-10 relative that no pressure removes; both solves take the fluid
+    # mean off the rhs first (remove_mean), so that the target is reachable.
+    tight = {"tol": TOL_TIGHT, "rhs": "fluid mean removed (remove_mean)"}
+    k_tight = min(args.steps, 5)
+    for name, dtype, precision in (("mixed", torch.float32, "mixed"), ("fp64", torch.float64, "fp64")):
+        st = make(dtype, precision, TOL_TIGHT, remove_mean=True)
+        ms_t, info_t, _, _ = timed(st, k_tight, args.warmup)
+        ms_t = max_over_ranks(ms_t)
+        tight[name] = {"value": world * cells * k_tight / (ms_t / 1e3), "ms_per_step": ms_t / k_tight,
+                       "mean_cycles_per_step": info_t["cycles"] / max(info_t["solves"], 1),
+                       "converged": bool(info_t["failures"] == 0 and info_t["solves"] == k_tight)}
+        del st
+    tight["mixed_speedup"] = tight["mixed"]["value"] / tight["fp64"]["value"]
     # ---- CPU baseline on a bounded sample (rank 0, one GPU only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         times, ccyc, threads = cpu_oracle_steps(args.cpu_steps, 1)
         cpu = {"value": cells * len(times) / sum(times), "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{len(times)} substeps of mixed_2048 on the CPU oracle (C/OpenMP restatement of the "
-                         f"reference kernels + the same multigrid to 1e-8), after 1 warm-up substep; "
+                         f"reference kernels + the multigrid, 8x8 exact coarsest, to 1e-8), after 1 warm-up substep; "
                          f"mean {sum(ccyc) / max(len(ccyc), 1):.1f} cycles/step"}
     if world > 1:
         dist.destroy_process_group()
@@ -437,13 +455,15 @@ def run_ours(args):
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 state + f64/f32 mixed solve", "data": "synthetic",
         "config": {"workload": "mixed_2048", "grid": [2048, 2048], "sources": 4, "solver":
-                   "multigrid V(2,2) RBGS w=1.4, full weighting, bilinear, 8x8 exact coarsest; FP32 cycles in FP64 "
+                   "multigrid V(2,2) RBGS w=1.4, full weighting, bilinear, 32x32 exact coarsest (cosine transform); "
+                   "FP32 cycles in FP64 "
                    "iterative refinement", "tol": TOL, "mean_cycles_per_step": info["cycles"] / max(info["solves"], 1),
                    "converged": bool(relres_ok), "l2": "working set > 126 MB L2; no flush",
                    "parallelism": f"replicas x{world}"},
         "fp64_gpu": {"value": value64, "ms_per_step": ms64 / args.steps,
                      "mean_cycles_per_step": info64["cycles"] / max(info64["solves"], 1), "converged": bool(fp64_ok),
                      "mixed_speedup": value / value64},
+        "tol_1e-10": tight,
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h + 8},
         "gpu_launches": int(launches),

@@ -275,6 +275,13 @@ int sg_gmg_solve_async(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div
  * first residual pass). */
 int sg_gmg_solve_from_zero_async(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int64_t ld_div,
                                  int div_dtype, double alpha, double tol, int max_cycles, void* stream);
+/* Remove the mean of alpha * div over the fluid cells from the rhs before solving (on = 1)
+ * or not (0, the default). The pressure equation with closed walls is a Neumann problem:
+ * its rhs must sum to zero, which a divergence does exactly only in exact arithmetic; the
+ * float rounding of that sum leaves a constant component that no pressure removes, and it
+ * sets a floor under the relative residual (near 1e-10 for a float32 state at 2048^2).
+ * No counterpart in the reference. */
+int sg_gmg_set_remove_mean(sg_gmg_plan* plan, int on);
 /* Outcome of the last solve (synchronises stream): cycles run, last relative residual,
  * status (1 converged, 2 cycle cap reached, 3 non-finite residual) and the number of
  * cycles run by all solves since sg_gmg_bind. Any output may be NULL. */

@@ -95,6 +95,7 @@ SIGNATURES = {
     "sg_batch_stats": [P, P, P, P, P],
     "sg_batch_snapshot_bytes": [P],
     "sg_batch_autotune": [P, I, P, I64, P, PI, PI, PI, PD],
+    "sg_gmg_set_remove_mean": [P, I],
     "sg_field_stats_workspace_bytes": [],
     "sg_field_stats": [I, I64, I64, P, I64, P, P, P],
     "sg_version": [],

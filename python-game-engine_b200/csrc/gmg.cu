@@ -65,6 +65,7 @@ struct GmgState {
   long long solves;
   long long failures;      // solves that ended at the cycle cap or on a non-finite residual
   double history[kHist];
+  double bmean;  // mean of alpha div over the fluid cells (when the plan removes it)
 };
 
 // ---------------------------------------------------------------- point operations
@@ -262,10 +263,12 @@ __global__ void k_gmg_fine_residual(int H, int W, const T* __restrict__ p, int64
 template <typename TD, typename TB, typename TC>
 __global__ void k_gmg_rhs(int H, int W, const TD* __restrict__ div, int64_t ldd, const GmgState* __restrict__ st,
                           LevelMask m, TB* __restrict__ b, int64_t ldb, double* __restrict__ partial,
-                          TB* __restrict__ pz, int64_t ldpz, TC* __restrict__ b0, int64_t ld0, TB* __restrict__ r64) {
+                          TB* __restrict__ pz, int64_t ldpz, TC* __restrict__ b0, int64_t ld0, TB* __restrict__ r64,
+                          int sub_mean) {
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int ib = blockIdx.x * kWX + threadIdx.x;
   const double alpha = st->alpha;
+  const double mean = sub_mean ? st->bmean : 0.0;
   double sq = 0.0;
   if (j < H) {
 #pragma unroll
@@ -274,7 +277,9 @@ __global__ void k_gmg_rhs(int H, int W, const TD* __restrict__ div, int64_t ldd,
       if (i < W) {
         TB v = (TB)0;
         if (m.fluid(j, i)) {
-          v = (TB)(alpha * (double)div[(int64_t)j * ldd + i]);
+          double x = alpha * (double)div[(int64_t)j * ldd + i];
+          if (sub_mean) x -= mean;
+          v = (TB)x;
           sq += (double)v * (double)v;
         }
         b[(int64_t)j * ldb + i] = v;
@@ -325,6 +330,29 @@ __global__ void k_gmg_set_params(GmgState* st, double alpha, double tol, int max
   st->solves += 1;
 }
 
+// Per-block sums of div over the fluid cells (for the mean the plan removes from the rhs).
+template <typename TD>
+__global__ void k_gmg_rhs_sum(int H, int W, const TD* __restrict__ div, int64_t ldd, LevelMask m,
+                              double* __restrict__ partial) {
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int ib = blockIdx.x * kWX + threadIdx.x;
+  double acc = 0.0;
+  if (j < H) {
+#pragma unroll
+    for (int q = 0; q < kWX / 32; ++q) {
+      const int i = ib + 32 * q;
+      if (i < W && m.fluid(j, i)) acc += (double)div[(int64_t)j * ldd + i];
+    }
+  }
+  double s = block_sum(acc);
+  if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
+}
+
+__global__ void k_gmg_finalize_mean(const double* __restrict__ partial, int n, GmgState* st, double inv_fluid) {
+  double s = sum_partials(partial, n);
+  if (threadIdx.x == 0) st->bmean = st->alpha * (s * inv_fluid);
+}
+
 __global__ void k_gmg_finalize_norm(const double* __restrict__ partial, int n, GmgState* st) {
   double s = sum_partials(partial, n);
   if (threadIdx.x == 0) st->bnorm = sqrt(s);
@@ -359,6 +387,101 @@ __global__ void k_gmg_finalize_rel(const double* __restrict__ partial, int n, Gm
 
 // ---------------------------------------------------------------- single-block tail
 constexpr int kMaxLevels = 16;
+constexpr int kPinvMaxSide = 16;  // coarsest levels up to this side: dense pseudo-inverse
+constexpr int kDctMaxSide = 64;   // open-box coarsest levels up to this side: cosine transform
+
+// Exact solve of an open-box coarsest level by the discrete cosine transform. Its operator
+// (sum over open faces of e - e_nb, walls closed) is L_y (x) I + I (x) L_x, L the Laplacian
+// of a path of n cells, whose orthonormal eigenvectors are the DCT-II basis
+// c_k(i) = s_k cos(pi k (i + 1/2) / n) (s_0 = sqrt(1/n), s_k = sqrt(2/n)) with eigenvalues
+// 4 sin^2(pi k / (2 n)). So e = C_y^T [(C_y b C_x^T) / (lambda_y + lambda_x)] C_x with the
+// constant mode (0, 0) set to 0, which is the pseudo-inverse solution the dense
+// pseudo-inverse gives on smaller coarsest levels. One block of 1024 threads; tab (in the
+// cycle precision, copied whole into shared memory) = C_x (c_k(i) at k W + i), C_x^T,
+// C_y (H x H), lambda_x (W), lambda_y (H). Every product keeps four partial sums.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_gmg_coarse_dct(const T* __restrict__ b, int64_t ldb, T* __restrict__ e,
+                                                         int64_t lde, int H, int W, const T* __restrict__ tab) {
+  extern __shared__ __align__(16) unsigned char dct_smem[];
+  T* sm = reinterpret_cast<T*>(dct_smem);
+  const int ntab = 2 * W * W + H * H + W + H;
+  const T* cx = sm;             // cx[k W + i]
+  const T* cxt = cx + W * W;    // cxt[i W + k]
+  const T* cy = cxt + W * W;    // cy[m H + j]
+  const T* lx = cy + H * H;
+  const T* ly = lx + W;
+  T* X = sm + ntab;
+  T* Y = X + H * W;
+  const int tid = threadIdx.x, nt = blockDim.x, n = H * W;
+  for (int q = tid; q < ntab; q += nt) sm[q] = tab[q];
+  for (int q = tid; q < n; q += nt) {
+    const int j = q / W, i = q - j * W;
+    Y[q] = b[(int64_t)j * ldb + i];
+  }
+  __syncthreads();
+  // sum_t a[t * sa] * c[t * sc] over t < len with four partial sums
+  auto dot = [](const T* a, int sa, const T* c, int sc, int len) {
+    T s0 = (T)0, s1 = (T)0, s2 = (T)0, s3 = (T)0;
+    int t = 0;
+    for (; t + 4 <= len; t += 4) {
+      s0 += a[t * sa] * c[t * sc];
+      s1 += a[(t + 1) * sa] * c[(t + 1) * sc];
+      s2 += a[(t + 2) * sa] * c[(t + 2) * sc];
+      s3 += a[(t + 3) * sa] * c[(t + 3) * sc];
+    }
+    for (; t < len; ++t) s0 += a[t * sa] * c[t * sc];
+    return (s0 + s1) + (s2 + s3);
+  };
+  for (int q = tid; q < n; q += nt) {  // X = B C_x^T
+    const int j = q / W, k = q - j * W;
+    X[q] = dot(Y + j * W, 1, cxt + k, W, W);
+  }
+  __syncthreads();
+  for (int q = tid; q < n; q += nt) {  // Y = (C_y X) / (lambda_y + lambda_x)
+    const int m = q / W, k = q - m * W;
+    const T acc = dot(cy + m * H, 1, X + k, W, H);
+    Y[q] = (m == 0 && k == 0) ? (T)0 : acc / (ly[m] + lx[k]);
+  }
+  __syncthreads();
+  for (int q = tid; q < n; q += nt) {  // X = C_y^T Y
+    const int j = q / W, k = q - j * W;
+    X[q] = dot(cy + j, H, Y + k, W, H);
+  }
+  __syncthreads();
+  for (int q = tid; q < n; q += nt) {  // e = X C_x
+    const int j = q / W, i = q - j * W;
+    e[(int64_t)j * lde + i] = dot(X + j * W, 1, cx + i, W, W);
+  }
+}
+
+template <typename T>
+static size_t coarse_dct_smem(int H, int W) {
+  return (size_t)(2 * W * W + H * H + W + H + 2 * H * W) * sizeof(T);
+}
+
+// The tables of k_gmg_coarse_dct for an H x W level (host, double): C_x, C_x^T, C_y,
+// lambda_x, lambda_y.
+static void coarse_dct_tables(int H, int W, std::vector<double>& tab) {
+  const double pi = 3.14159265358979323846;
+  tab.assign(2 * (size_t)W * W + (size_t)H * H + W + H, 0.0);
+  auto basis = [&](int n, double* c, double* lam) {
+    for (int k = 0; k < n; ++k) {
+      const double sk = std::sqrt((k == 0 ? 1.0 : 2.0) / n);
+      for (int i = 0; i < n; ++i) c[(size_t)k * n + i] = sk * std::cos(pi * k * (i + 0.5) / n);
+      const double sn = std::sin(pi * k / (2.0 * n));
+      lam[k] = 4.0 * sn * sn;
+    }
+  };
+  double* cx = tab.data();
+  double* cxt = cx + (size_t)W * W;
+  double* cy = cxt + (size_t)W * W;
+  double* lx = cy + (size_t)H * H;
+  double* ly = lx + W;
+  basis(W, cx, lx);
+  basis(H, cy, ly);
+  for (int k = 0; k < W; ++k)
+    for (int i = 0; i < W; ++i) cxt[(size_t)i * W + k] = cx[(size_t)k * W + i];
+}
 // Levels up to this many cells a side run inside the single-block tail kernel; larger
 // open-box levels use the fused tiled kernels (two launches per level and cycle).
 constexpr int kTailMaxSide = 16;
@@ -631,6 +754,12 @@ struct sg_gmg_plan {
   double omega = 1.0;
   std::vector<sg::Level> levels;
   std::vector<double> pinv;  // coarsest pseudo-inverse, n x n
+  // coarsest open-box level above kPinvMaxSide cells a side: exact solve by the cosine
+  // transform (k_gmg_coarse_dct) from the tables in dct (C_x, C_y, eigenvalues)
+  int coarse_dct = 0;
+  std::vector<double> dct;
+  std::vector<float> dct_f;  // the same in float, for FP32 cycles
+  int64_t off_dct = 0, dct_smem = 0;
   int tail_start = 0;        // first level handled by the single-block tail kernel
   int tail_open = 0;         // every tail level is an open box (k_gmg_tail_open)
   int64_t tail_smem = 0;     // its dynamic shared memory (bytes)
@@ -642,6 +771,10 @@ struct sg_gmg_plan {
   // the residual in the precision of p when that differs from the cycle precision
   int fused_ir = 0;
   int64_t off_b2 = 0, off_r64 = 0;
+  // remove the fluid mean of the rhs before solving (a Neumann problem's rhs must sum to
+  // zero; float rounding of a telescoping divergence sum leaves a component no p removes)
+  int remove_mean = 0;
+  double inv_fluid = 0.0;
   char* ws = nullptr;        // bound device workspace
   // cached solve graph
   cudaStream_t capture_stream = nullptr;
@@ -1016,6 +1149,12 @@ static int set_tiled_smem_limits() {
 // One cycle on level k for A_k e_k = b_k; zero_init: start from e_k = 0.
 template <typename T>
 static void cycle(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
+  if (p->coarse_dct && k == (int)p->levels.size() - 1) {
+    const Level& C = p->levels[k];
+    SG_LAUNCH(k_gmg_coarse_dct<T><<<1, 1024, p->dct_smem, s>>>(ws_ptr<T>(p, C.off_b), C.ld, ws_ptr<T>(p, C.off_e), C.ld,
+                                                                C.H, C.W, ws_ptr<T>(p, p->off_dct)));
+    return;
+  }
   if (k == p->tail_start) {
     tail_launch<T>(p, zero_init, s);
     return;
@@ -1074,9 +1213,13 @@ static void prologue(const sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div, i
   dim3 g = grid_wide(L.W, L.H);
   TP* bf = (TP*)(p->ws + p->off_bfine);
   TP* r64 = p->off_r64 ? (TP*)(p->ws + p->off_r64) : nullptr;
+  if (p->remove_mean) {
+    SG_LAUNCH(k_gmg_rhs_sum<TD><<<g, block2d(), 0, s>>>(L.H, L.W, div, ldd, m, part));
+    SG_LAUNCH(k_gmg_finalize_mean<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st, p->inv_fluid));
+  }
   SG_LAUNCH(k_gmg_rhs<TD, TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, div, ldd, st, m, bf, p->ld_bfine, part,
                                                           zero_guess ? pp : nullptr, ldp, ws_ptr<TC>(p, L.off_b), L.ld,
-                                                          r64));
+                                                          r64, p->remove_mean));
   SG_LAUNCH(k_gmg_finalize_norm<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st));
   if (zero_guess) {
     SG_LAUNCH(k_gmg_finalize_rel<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st, h, use_handle, 0));
@@ -1240,7 +1383,7 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
   SG_REQUIRE(out, "null plan pointer");
   *out = nullptr;
   SG_REQUIRE(H >= 1 && W >= 1 && H <= (1 << 16) && W <= (1 << 16), "bad grid %lld x %lld", (long long)H, (long long)W);
-  SG_REQUIRE(coarsest >= 1 && coarsest <= 16, "coarsest must be in 1..16");
+  SG_REQUIRE(coarsest >= 1 && coarsest <= kDctMaxSide, "coarsest must be in 1..%d", kDctMaxSide);
   SG_REQUIRE(omega > 0.0 && omega < 2.0, "omega must be in (0, 2)");
   SG_REQUIRE(pre_sweeps >= 0 && post_sweeps >= 0 && pre_sweeps + post_sweeps >= 1, "need at least one smoothing sweep");
   SG_REQUIRE(pre_sweeps <= 16 && post_sweeps <= 16, "at most 16 sweeps per side");
@@ -1276,6 +1419,11 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
   p->post = post_sweeps;
   p->coarsest = coarsest;
   p->omega = omega;
+  {
+    int64_t nf = 0;
+    for (uint8_t f : fl) nf += f ? 1 : 0;
+    p->inv_fluid = nf > 0 ? 1.0 / (double)nf : 0.0;
+  }
   int h = (int)H, w = (int)W;
   while (true) {
     Level L;
@@ -1312,10 +1460,21 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
     return fail(SG_ERR_CAPACITY, "grid needs more than %d levels", kMaxLevels);
   }
   Level& last = p->levels.back();
-  std::vector<uint8_t> lastcode = last.analytic ? pack_codes(fl, fu, fv, last.H, last.W) : last.code;
-  if (!coarsest_pinv(lastcode, last.H, last.W, p->pinv)) {
-    delete p;
-    return fail(SG_ERR_ARG, "coarsest operator could not be factorised");
+  if (std::max(last.H, last.W) > kPinvMaxSide) {
+    // above the dense pseudo-inverse's size: the cosine transform, which needs an open box
+    if (!last.analytic) {
+      delete p;
+      return fail(SG_ERR_ARG, "a coarsest level above %d cells a side must be an open box (no obstacles); "
+                  "lower coarsest", kPinvMaxSide);
+    }
+    p->coarse_dct = 1;
+    coarse_dct_tables(last.H, last.W, p->dct);
+  } else {
+    std::vector<uint8_t> lastcode = last.analytic ? pack_codes(fl, fu, fv, last.H, last.W) : last.code;
+    if (!coarsest_pinv(lastcode, last.H, last.W, p->pinv)) {
+      delete p;
+      return fail(SG_ERR_ARG, "coarsest operator could not be factorised");
+    }
   }
   // tail: the largest suffix of levels that fits one block's shared memory: open boxes up
   // to kOpenTailMaxSide cells a side (k_gmg_tail_open), otherwise up to kTailMaxSide
@@ -1329,9 +1488,9 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
     for (int k = start; k < nl; ++k) acc += ((2 * (int64_t)p->levels[k].H * p->levels[k].W + 3) & ~(int64_t)3);
     return acc + (int64_t)p->levels[start].H * ((p->levels[start].W + 1) / 2);
   };
-  p->tail_start = nl - 1;
-  bool open_suffix = true;
-  for (int k = nl - 1; k >= 0; --k) {
+  p->tail_start = p->coarse_dct ? nl : nl - 1;  // no tail kernel above a cosine-transform solve
+  bool open_suffix = !p->coarse_dct;
+  for (int k = p->coarse_dct ? -1 : nl - 1; k >= 0; --k) {
     const Level& L = p->levels[k];
     const bool open = open_suffix && L.analytic;
     const int side = std::max(L.H, L.W);
@@ -1341,9 +1500,16 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
     p->tail_start = k;
   }
   p->tail_open = open_suffix ? 1 : 0;
-  p->tail_smem = (p->tail_open ? (int64_t)open_tail_layout(p->levels, p->tail_start).total
-                               : generic_elems(p->tail_start)) *
-                 (int64_t)cyc;
+  if (p->coarse_dct) {
+    const Level& C = p->levels.back();
+    p->tail_smem = 0;
+    p->dct_smem = (int64_t)(precision == SG_GMG_FP64 ? coarse_dct_smem<double>(C.H, C.W)
+                                                     : coarse_dct_smem<float>(C.H, C.W));
+  } else {
+    p->tail_smem = (p->tail_open ? (int64_t)open_tail_layout(p->levels, p->tail_start).total
+                                 : generic_elems(p->tail_start)) *
+                   (int64_t)cyc;
+  }
   // workspace layout
   size_t fine = precision == SG_GMG_FP32 ? sizeof(float) : sizeof(double);
   int64_t off = 0;
@@ -1381,6 +1547,8 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
   }
   p->off_pinv = off;
   off = align256(off + (int64_t)p->pinv.size() * 8);
+  p->off_dct = off;
+  off = align256(off + (int64_t)p->dct.size() * 8);
   dim3 g = grid_wide(p->W, p->H);
   p->n_partial = (int64_t)g.x * g.y;
   if (p->fused_ir) {
@@ -1423,6 +1591,23 @@ int sg_gmg_bind(sg_gmg_plan* plan, void* workspace, void* stream) {
   SG_CUDA_TRY(cudaMemcpyAsync(plan->ws + plan->off_pinv, plan->pinv.data(), plan->pinv.size() * 8,
                               cudaMemcpyHostToDevice, s),
               "sg_gmg_bind pinv");
+  if (plan->coarse_dct) {
+    if (plan->precision == SG_GMG_FP64) {
+      SG_CUDA_TRY(cudaMemcpyAsync(plan->ws + plan->off_dct, plan->dct.data(), plan->dct.size() * 8,
+                                  cudaMemcpyHostToDevice, s),
+                  "sg_gmg_bind cosine tables");
+    } else {
+      plan->dct_f.assign(plan->dct.begin(), plan->dct.end());
+      SG_CUDA_TRY(cudaMemcpyAsync(plan->ws + plan->off_dct, plan->dct_f.data(), plan->dct_f.size() * 4,
+                                  cudaMemcpyHostToDevice, s),
+                  "sg_gmg_bind cosine tables");
+    }
+    const int ds = (int)plan->dct_smem;
+    SG_CUDA_TRY(plan->precision == SG_GMG_FP64
+                    ? cudaFuncSetAttribute(k_gmg_coarse_dct<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ds)
+                    : cudaFuncSetAttribute(k_gmg_coarse_dct<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, ds),
+                "smem attr");
+  }
   SG_CUDA_TRY(cudaMemsetAsync(plan->ws + plan->off_state, 0, sizeof(GmgState), s), "sg_gmg_bind state");
   // host vectors must outlive the asynchronous copies
   SG_CUDA_TRY(cudaStreamSynchronize(s), "sg_gmg_bind sync");
@@ -1556,6 +1741,17 @@ int sg_gmg_level_shape(const sg_gmg_plan* plan, int level, int* H, int* W) {
 }
 
 int sg_gmg_tail_start(const sg_gmg_plan* plan) { return plan ? plan->tail_start : -1; }
+
+int sg_gmg_set_remove_mean(sg_gmg_plan* plan, int on) {
+  SG_REQUIRE(plan, "null plan");
+  SG_REQUIRE(on == 0 || on == 1, "on must be 0 or 1");
+  if (plan->remove_mean != on && plan->exec) {  // the cached solve graph has the old prologue
+    cudaGraphExecDestroy(plan->exec);
+    plan->exec = nullptr;
+  }
+  plan->remove_mean = on;
+  return SG_OK;
+}
 
 int sg_gmg_smooth_async(sg_gmg_plan* plan, int level, int sweeps, void* stream) {
   SG_REQUIRE(plan && plan->ws, "plan not bound to a workspace");

@@ -96,6 +96,7 @@ class GeometricMultigridParams:
     check_every: int = 1        # host convergence check interval (cycles)
     fixed_cycles: int = 0       # > 0: run exactly this many cycles without host checks
     rebuild_masks: bool = False
+    remove_mean: bool = False   # subtract the fluid mean of the rhs (rounding of sum(div)) before solving
 
     def string(self):
         return (f"GeometricMultigridParams_{self.cycle}{self.pre_sweeps}{self.post_sweeps}_w{self.omega}"

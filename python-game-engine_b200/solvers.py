@@ -225,7 +225,8 @@ _PRECISION = {"fp32": L.SG_GMG_FP32, "fp64": L.SG_GMG_FP64, "mixed": L.SG_GMG_MI
 class GMGPlan:
     """A bound multigrid plan (host plan + device workspace) for one grid and mask."""
 
-    def __init__(self, H, W, fmu, fmv, device, coarsest=8, omega=1.4, pre=2, post=2, cycle="V", precision="fp64"):
+    def __init__(self, H, W, fmu, fmv, device, coarsest=8, omega=1.4, pre=2, post=2, cycle="V", precision="fp64",
+                 remove_mean=False):
         lib = L.load()
         self.H, self.W, self.precision = H, W, precision
         handle = ctypes.c_void_p()
@@ -243,6 +244,7 @@ class GMGPlan:
                                        int(post), 0 if cycle.upper() == "V" else 1, _PRECISION[precision]),
                 "sg_gmg_plan_create")
         self.handle = handle
+        L.check(lib.sg_gmg_set_remove_mean(handle, 1 if remove_mean else 0), "sg_gmg_set_remove_mean")
         nbytes = lib.sg_gmg_workspace_bytes(handle)
         self.workspace = torch.empty(int(nbytes), dtype=torch.uint8, device=device)
         L.check(lib.sg_gmg_bind(handle, self.workspace.data_ptr(), L.stream_ptr()), "sg_gmg_bind")
@@ -353,25 +355,26 @@ class GeometricMultigridSolver:
     def current_plan(self):
         return next(iter(self._plans.values()), None)
 
-    def plan_for(self, H, W, fmu, fmv, device, coarsest, omega, pre, post, cycle, precision, rebuild=False):
+    def plan_for(self, H, W, fmu, fmv, device, coarsest, omega, pre, post, cycle, precision, rebuild=False,
+                 remove_mean=False):
         if isinstance(fmu, AnalyticMask):
             mkey = ("analytic", fmu.mode)
         else:
             mkey = (fmu.data_ptr(), fmu._version, fmv.data_ptr(), fmv._version)
-        key = (H, W, mkey, coarsest, omega, pre, post, cycle, precision, str(device))
+        key = (H, W, mkey, coarsest, omega, pre, post, cycle, precision, str(device), bool(remove_mean))
         plan = self._plans.get(key)
         if plan is None or rebuild:
-            plan = GMGPlan(H, W, fmu, fmv, device, coarsest, omega, pre, post, cycle, precision)
+            plan = GMGPlan(H, W, fmu, fmv, device, coarsest, omega, pre, post, cycle, precision, remove_mean)
             self._plans = {key: plan}
         return plan
 
     def __call__(self, pressure, divergence, face_mask_u, face_mask_v, fluid_density, cell_size, dt, tol=1e-6,
                  max_cycles=50, cycle="V", pre_sweeps=2, post_sweeps=2, omega=1.4, coarsest=8, precision="fp64",
                  check_every=1, fixed_cycles=0, rebuild_masks=False, strict=False, zero_initial_guess=False,
-                 **_ignored):
+                 remove_mean=False, **_ignored):
         H, W = pressure.shape
         plan = self.plan_for(H, W, face_mask_u, face_mask_v, pressure.device, coarsest, omega, pre_sweeps, post_sweeps,
-                             cycle, precision, rebuild_masks)
+                             cycle, precision, rebuild_masks, remove_mean)
         want = torch.float32 if precision == "fp32" else torch.float64
         if pressure.dtype == want:
             p = pressure

@@ -100,6 +100,58 @@ def test_gmg_one_cycle_vs_oracle(shape, obstacles, cycle, precision):
     assert np.max(np.abs(got - pe)) <= tol * np.max(np.abs(pe))
 
 
+@pytest.mark.parametrize("shape,cycle,precision", [
+    ((64, 64), "V", "fp64"), ((200, 176), "V", "fp64"), ((200, 176), "W", "fp64"), ((20, 30), "V", "fp64"),
+    ((1100, 1300), "V", "fp64"), ((1100, 1300), "V", "mixed"), ((1201, 1025), "W", "fp32")])
+def test_gmg_one_cycle_cosine_coarsest_vs_oracle(shape, cycle, precision):
+    """coarsest=32: the last level (<= 32 a side, open box) is solved exactly by the cosine
+    transform instead of a dense pseudo-inverse; one cycle must equal the oracle's cycle with
+    the pseudo-inverse of that level (a single-level grid is solved outright)."""
+    H, W = shape
+    fmu, fmv, fl, div = _problem(H, W, False, 3)
+    alpha = -0.7
+    g = O.GMGOracle(fmu, fmv, fl, coarsest=32, omega=1.4, cycle=cycle)
+    pe = np.zeros((H, W))
+    g.vcycle(0, pe, alpha * div)
+    solver = sg.GeometricMultigridSolver()
+    p = torch.zeros((H, W), dtype=torch.float32 if precision == "fp32" else torch.float64, device="cuda")
+    solver(p, dev(div.astype(np.float64 if precision == "fp64" else np.float32)), sg.OPEN_BOX, sg.OPEN_BOX, 0.7,
+           1.0, 1.0, precision=precision, fixed_cycles=1, cycle=cycle, coarsest=32)
+    got = p.double().cpu().numpy()
+    tol = 1e-10 if precision == "fp64" else 2e-5
+    assert np.max(np.abs(got - pe)) <= tol * np.max(np.abs(pe))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gmg_remove_mean_reaches_1e10(precision):
+    """An rhs whose sum is not zero (as float rounding leaves a divergence) has a constant part
+    no pressure removes: the residual stalls above it. With remove_mean the fluid mean is
+    taken off first and the solve reaches 1e-10; its pressure equals the oracle's solve of
+    the mean-free rhs."""
+    H = W = 256
+    fmu, fmv, fl, div = _problem(H, W, False, 4)
+    div = div + 1e-7 * np.abs(div).max()
+    d = dev(div.astype(np.float64 if precision == "fp64" else np.float32))
+    h, rho, dt = 1.0 / H, 1.0, 0.5 / H
+    solver = sg.GeometricMultigridSolver()
+    p = torch.zeros((H, W), dtype=torch.float64, device="cuda")
+    solver(p, d, sg.OPEN_BOX, sg.OPEN_BOX, rho, h, dt, tol=1e-10, max_cycles=40, precision=precision, coarsest=32)
+    assert not solver.converged and solver.last_relres > 1e-10
+    p.zero_()
+    solver(p, d, sg.OPEN_BOX, sg.OPEN_BOX, rho, h, dt, tol=1e-10, max_cycles=40, precision=precision, coarsest=32,
+           remove_mean=True, strict=True)
+    assert solver.converged and solver.last_relres <= 1e-10 and solver.last_cycles <= 12
+    alpha = O.alpha_coeff(h, rho, dt)
+    b = alpha * d.double().cpu().numpy()
+    b -= b.mean()
+    g = O.GMGOracle(fmu, fmv, fl)
+    pe = np.zeros((H, W))
+    g.solve(pe, b, tol=1e-13, max_cycles=60)
+    got = p.double().cpu().numpy()
+    a, e = got - got.mean(), pe - pe.mean()
+    assert np.max(np.abs(a - e)) <= 1e-5 * np.max(np.abs(e))  # two 1e-10 solves differ by <~ kappa * 1e-10
+
+
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 1e-8), ("fp32", 1e-5)])
 @pytest.mark.parametrize("obstacles", [False, True])
 def test_gmg_reaches_tolerance(precision, tol, obstacles):

@@ -107,8 +107,40 @@ def test_gmg_plan_with_obstacle_planes():
     L.load().sg_gmg_plan_destroy(h)
 
 
-@pytest.mark.parametrize("kw", [dict(omega=2.5), dict(coarsest=0), dict(pre=0, post=0), dict(cycle=3),
-                                dict(precision=9)])
+@pytest.mark.parametrize("H,W,levels,last", [(2048, 2048, 7, (32, 32)), (1100, 1300, 7, (18, 21)),
+                                             (20, 30, 1, (20, 30)), (64, 64, 2, (32, 32))])
+def test_gmg_plan_cosine_coarsest(H, W, levels, last):
+    """coarsest=32 on an open box: the hierarchy stops at the first level <= 32 a side
+    (solved by the cosine transform)."""
+    lib = L.load()
+    rc, h = _plan(H, W, coarsest=32)
+    assert rc == L.SG_OK
+    try:
+        assert lib.sg_gmg_num_levels(h) == levels
+        hh, ww = ctypes.c_int(), ctypes.c_int()
+        assert lib.sg_gmg_level_shape(h, levels - 1, ctypes.byref(hh), ctypes.byref(ww)) == L.SG_OK
+        assert (hh.value, ww.value) == last
+    finally:
+        lib.sg_gmg_plan_destroy(h)
+
+
+def test_gmg_cosine_coarsest_needs_open_box():
+    """A coarsest level above 16 a side that is not an open box is refused at plan creation."""
+    import oracle as O
+
+    H, W = 96, 80
+    solid = O.box_solid(H, W)
+    solid[:, W // 2 - 8:W // 2 + 8] = True  # a wall that survives coarsening
+    fmu, fmv = O.face_masks_from_solid(solid)
+    fl = O.is_fluid_from_faces(fmu, fmv)
+    masks = [np.ascontiguousarray(x.astype(np.uint8)) for x in (fl, fmu, fmv)]
+    rc, h = _plan(H, W, L.SG_MASK_PLANES, masks, coarsest=32)
+    assert rc == L.SG_ERR_ARG and not h.value
+    assert "open box" in L.load().sg_last_error().decode()
+
+
+@pytest.mark.parametrize("kw", [dict(omega=2.5), dict(coarsest=0), dict(coarsest=65), dict(pre=0, post=0),
+                                dict(cycle=3), dict(precision=9)])
 def test_gmg_plan_rejects_bad_parameters(kw):
     rc, h = _plan(64, 64, **kw)
     assert rc == L.SG_ERR_ARG and not h.value
