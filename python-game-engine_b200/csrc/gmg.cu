@@ -257,7 +257,8 @@ __global__ void k_gmg_fine_residual(int H, int W, const T* __restrict__ p, int64
   if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
 }
 
-// bf = alpha * div on fluid cells (alpha from the solve state) plus per-block sums of bf^2.
+// bf = alpha * div on fluid cells (alpha from the solve state; b may be null when only the
+// outputs below are needed) plus per-block sums of bf^2.
 // For a zero initial guess (pz non-null) it also writes p = 0 and, bf being the residual,
 // the first cycle's rhs b0 (cycle precision) and the carried residual r64 (when kept).
 template <typename TD, typename TB, typename TC>
@@ -282,7 +283,7 @@ __global__ void k_gmg_rhs(int H, int W, const TD* __restrict__ div, int64_t ldd,
           v = (TB)x;
           sq += (double)v * (double)v;
         }
-        b[(int64_t)j * ldb + i] = v;
+        if (b) b[(int64_t)j * ldb + i] = v;
         if (pz) {
           pz[(int64_t)j * ldpz + i] = (TB)0;
           b0[(int64_t)j * ld0 + i] = (TC)v;
@@ -1042,13 +1043,26 @@ static bool small_tiles(const Level& L) {
   return large_blocks < SG_GMG_REG_MIN_TILES;
 }
 
+// Rows of 32 threads of a shared-memory tile block: kTBY, or SG_TILE_FEW_ROWS on levels of
+// at most SG_TILE_FEW_TILES tiles (a wave or less of blocks: more threads per block
+// shorten each phase of the block, which is all the level costs).
+#ifndef SG_TILE_FEW_TILES
+#define SG_TILE_FEW_TILES 256
+#endif
+#ifndef SG_TILE_FEW_ROWS
+#define SG_TILE_FEW_ROWS 16
+#endif
+static dim3 tile_block(dim3 g) {
+  return dim3(kTBX, (int64_t)g.x * g.y <= SG_TILE_FEW_TILES ? SG_TILE_FEW_ROWS : kTBY);
+}
+
 template <typename T, int SW, int TX, int TY>
 static void launch_pre_t(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
   const Level& L = p->levels[k];
   const Level& C = p->levels[k + 1];
   dim3 g((L.W + TX - 1) / TX, (L.H + TY - 1) / TY);
   // reads E0 (nothing for a zero initial guess), writes E1
-  SG_LAUNCH(k_gmg_pre_tiled<T, SW, TX, TY><<<g, dim3(kTBX, kTBY), PreShape<SW, TX, TY>::template bytes<T>(), s>>>(
+  SG_LAUNCH(k_gmg_pre_tiled<T, SW, TX, TY><<<g, tile_block(g), PreShape<SW, TX, TY>::template bytes<T>(), s>>>(
       zero_init ? nullptr : ws_ptr<T>(p, L.off_e), ws_ptr<T>(p, L.off_e2), ws_ptr<T>(p, L.off_b), L.ld, L.H, L.W,
       ws_ptr<T>(p, C.off_b), C.ld, C.H, C.W, (T)p->omega));
 }
@@ -1059,7 +1073,7 @@ static void launch_post_t(const sg_gmg_plan* p, int k, cudaStream_t s) {
   const Level& C = p->levels[k + 1];
   dim3 g((L.W + TX - 1) / TX, (L.H + TY - 1) / TY);
   // reads E1 and the coarse correction (the coarse level's E0), writes E0
-  SG_LAUNCH(k_gmg_post_tiled<T, SW, TX, TY><<<g, dim3(kTBX, kTBY), PostShape<SW, TX, TY>::template bytes<T>(), s>>>(
+  SG_LAUNCH(k_gmg_post_tiled<T, SW, TX, TY><<<g, tile_block(g), PostShape<SW, TX, TY>::template bytes<T>(), s>>>(
       ws_ptr<T>(p, L.off_e2), ws_ptr<T>(p, L.off_e), ws_ptr<T>(p, L.off_b), L.ld, L.H, L.W, ws_ptr<T>(p, C.off_e),
       C.ld, C.H, C.W, (T)p->omega));
 }
@@ -1217,7 +1231,10 @@ static void prologue(const sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div, i
     SG_LAUNCH(k_gmg_rhs_sum<TD><<<g, block2d(), 0, s>>>(L.H, L.W, div, ldd, m, part));
     SG_LAUNCH(k_gmg_finalize_mean<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st, p->inv_fluid));
   }
-  SG_LAUNCH(k_gmg_rhs<TD, TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, div, ldd, st, m, bf, p->ld_bfine, part,
+  // from a zero guess the fused fine level carries the residual from here on (b0 / r64), so
+  // the FP64 rhs itself is not kept
+  TP* bkeep = (zero_guess && p->fused_ir) ? nullptr : bf;
+  SG_LAUNCH(k_gmg_rhs<TD, TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, div, ldd, st, m, bkeep, p->ld_bfine, part,
                                                           zero_guess ? pp : nullptr, ldp, ws_ptr<TC>(p, L.off_b), L.ld,
                                                           r64, p->remove_mean));
   SG_LAUNCH(k_gmg_finalize_norm<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st));

@@ -36,6 +36,8 @@ struct SplitTile {
 };
 
 __device__ __forceinline__ int tile_tid() { return threadIdx.y * kTBX + threadIdx.x; }
+// threads of the block: kTThreads, or more on levels with few tiles (shorter phases)
+__device__ __forceinline__ int tile_nt() { return kTBX * blockDim.y; }
 
 // Relax the cells of colour col in the tile grown by RING rings (smem rows/cols
 // [HALO - RING, HALO + TY|TX + RING)); every neighbour is inside the loaded tile.
@@ -48,7 +50,7 @@ __device__ __forceinline__ void relax_ring(const SplitTile<T>& t, int col, T ome
   T* E = t.ep(col);
   const T* Bc = t.bp(col);
   const T* O = t.ep(1 - col);
-  for (int f = tile_tid(); f < N; f += kTThreads) {
+  for (int f = tile_tid(); f < N; f += tile_nt()) {
     const int rr = f / KW;
     const int r = RLO + rr;
     const int p = (col + t.par0 + r) & 1;  // columns of colour col in this row: c = p + 2k
@@ -88,7 +90,7 @@ __device__ __forceinline__ void relax_all(const SplitTile<T>& t, T omega) {
 template <typename T, bool INTERIOR, int EX, int EY>
 __device__ __forceinline__ void tile_load(const SplitTile<T>& t, const T* __restrict__ e, const T* __restrict__ b,
                                           int64_t ld) {
-  for (int f = tile_tid(); f < EX * EY; f += kTThreads) {
+  for (int f = tile_tid(); f < EX * EY; f += tile_nt()) {
     const int r = f / EX, c = f - r * EX;
     const int j = t.j0 + r, i = t.i0 + c;
     const bool in = INTERIOR || (j >= 0 && j < t.H && i >= 0 && i < t.W);
@@ -100,7 +102,7 @@ __device__ __forceinline__ void tile_load(const SplitTile<T>& t, const T* __rest
 
 template <typename T, bool INTERIOR, int HALO, int TX, int TY>
 __device__ __forceinline__ void tile_store(const SplitTile<T>& t, T* __restrict__ e, int64_t ld) {
-  for (int f = tile_tid(); f < TX * TY; f += kTThreads) {
+  for (int f = tile_tid(); f < TX * TY; f += tile_nt()) {
     const int rr = f / TX, cc = f - rr * TX;
     const int j = t.j0 + HALO + rr, i = t.i0 + HALO + cc;
     if (INTERIOR || (j < t.H && i < t.W)) e[(int64_t)j * ld + i] = t.E(HALO + rr, HALO + cc);
@@ -164,7 +166,7 @@ __device__ __forceinline__ void pre_body(const SplitTile<T>& t, const T* __restr
   relax_all<T, INTERIOR, S::HALO, S::EXh, TX, TY, 0, 2 * SW>(t, omega);
   // residual on the tile plus one ring, in place of b (each cell reads only its own b)
   constexpr int RW = TX + 2, RH = TY + 2, LO = S::HALO - 1;
-  for (int f = tile_tid(); f < RW * RH; f += kTThreads) {
+  for (int f = tile_tid(); f < RW * RH; f += tile_nt()) {
     const int rr = f / RW, cc = f - rr * RW;
     const T res = tile_residual<T, INTERIOR>(t, LO + rr, LO + cc);
     t.B(LO + rr, LO + cc) = res;
@@ -172,7 +174,7 @@ __device__ __forceinline__ void pre_body(const SplitTile<T>& t, const T* __restr
   __syncthreads();
   // full weighting along x: X[rr][I'] over fine rows of the tile plus one ring
   const int H = t.H, W = t.W;
-  for (int f = tile_tid(); f < S::XR * S::XC; f += kTThreads) {
+  for (int f = tile_tid(); f < S::XR * S::XC; f += tile_nt()) {
     const int rr = f / S::XC, Ip = f - rr * S::XC;
     const int I = blockIdx.x * S::XC + Ip;
     T acc = (T)0;
@@ -189,7 +191,7 @@ __device__ __forceinline__ void pre_body(const SplitTile<T>& t, const T* __restr
   }
   __syncthreads();
   // along y
-  for (int f = tile_tid(); f < (TY / 2) * S::XC; f += kTThreads) {
+  for (int f = tile_tid(); f < (TY / 2) * S::XC; f += tile_nt()) {
     const int Jp = f / S::XC, Ip = f - Jp * S::XC;
     const int J = blockIdx.y * (TY / 2) + Jp, I = blockIdx.x * S::XC + Ip;
     if (J >= Hc || I >= Wc) continue;
@@ -209,7 +211,7 @@ __device__ __forceinline__ void pre_body(const SplitTile<T>& t, const T* __restr
 // pre: SW sweeps from e_in (NULL: zero initial guess) + residual + full weighting into
 // bc (coarse tile TX/2 x TY/2); the smoothed tile goes to e_out.
 template <typename T, int SW, int TX, int TY>
-__global__ void __launch_bounds__(kTThreads) k_gmg_pre_tiled(const T* __restrict__ e_in, T* __restrict__ e_out,
+__global__ void __launch_bounds__(1024) k_gmg_pre_tiled(const T* __restrict__ e_in, T* __restrict__ e_out,
                                                              const T* __restrict__ b, int64_t ld, int H, int W,
                                                              T* __restrict__ bc, int64_t ldc, int Hc, int Wc, T omega) {
   using S = PreShape<SW, TX, TY>;
@@ -229,7 +231,7 @@ __device__ __forceinline__ void post_body(const SplitTile<T>& t, const T* __rest
                                           int Hc, int Wc, T omega) {
   using S = PostShape<SW, TX, TY>;
   const T w9 = (T)(9.0 / 16.0), w3 = (T)(3.0 / 16.0), wd = (T)(1.0 / 16.0);
-  for (int f = tile_tid(); f < S::EX * S::EY; f += kTThreads) {
+  for (int f = tile_tid(); f < S::EX * S::EY; f += tile_nt()) {
     const int r = f / S::EX, c = f - r * S::EX;
     const int j = t.j0 + r, i = t.i0 + c;
     T ev = (T)0, bv = (T)0;
@@ -259,7 +261,7 @@ __device__ __forceinline__ void post_body(const SplitTile<T>& t, const T* __rest
 
 // post: e_out = smoothed (e_in + P ec).
 template <typename T, int SW, int TX, int TY>
-__global__ void __launch_bounds__(kTThreads) k_gmg_post_tiled(const T* __restrict__ e_in, T* __restrict__ e_out,
+__global__ void __launch_bounds__(1024) k_gmg_post_tiled(const T* __restrict__ e_in, T* __restrict__ e_out,
                                                               const T* __restrict__ b, int64_t ld, int H, int W,
                                                               const T* __restrict__ ec, int64_t ldc, int Hc, int Wc,
                                                               T omega) {

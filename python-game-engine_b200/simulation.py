@@ -384,7 +384,11 @@ class SmokeSimulation2D:
 
     def _solve_pressure(self):
         fmu, fmv, _ = self._kmasks
-        self.pressure.zero_()
+        # simulation.py:310 zeroes the pressure before every solve; the multigrid solve from a
+        # zero guess does not read it (it writes p = 0 itself), so the fill is skipped there
+        if not (self.pressure_solver_method == "geometric_multigrid"
+                and not getattr(self.solver_params, "fixed_cycles", 0)):
+            self.pressure.zero_()
         solve_pressure(self.pressure, self.divergence, fmu, fmv, self.fluid_density, self.cell_size, self.dt, self,
                        zero_initial_guess=True)
 
