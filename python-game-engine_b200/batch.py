@@ -59,7 +59,10 @@ class BatchedSmoke:
     def __del__(self):
         h = getattr(self, "handle", None)
         if h is not None and h.value:
-            L.load().sg_batch_destroy(h)
+            try:
+                L.load().sg_batch_destroy(h)
+            except Exception:  # interpreter shutdown: the library may already be gone
+                pass
             self.handle = None
 
     # ------------------------------------------------------------------ configuration

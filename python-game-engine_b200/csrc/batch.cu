@@ -11,7 +11,9 @@
 //
 // The pressure solve is the convergent multigrid of the single-grid solver (red-black
 // Gauss-Seidel with omega, full-weighting restriction, bilinear prolongation, exact solve
-// on the coarsest level <= 8 x 8 through its pseudo-inverse) in the single-grid solver's
+// on the coarsest level <= 8 x 8 through its pseudo-inverse; each side of a level is one
+// launch over 16 x 16 tiles of all scenes, with the single-grid shared-memory tile bodies
+// of gmg_tiled.cuh: sweeps, residual and restriction in shared memory) in the single-grid solver's
 // mixed precision: float32 cycles on the correction equation inside float64 iterative
 // refinement (p and the residual b - A p in float64), until each scene's relative residual
 // ||b - A p|| / ||b|| is <= tol; the pressure the projection uses is p rounded to float32.
@@ -37,6 +39,9 @@ namespace sg {
 
 bool open_box_pinv(int H, int W, std::vector<double>& out);
 
+#include "gmg_weights.cuh"
+#include "gmg_tiled.cuh"
+
 constexpr int kBMaxLev = 12;
 constexpr int kBThreads = 256;
 
@@ -60,6 +65,7 @@ struct BPools {
   float* u[2];
   float* v[2];
   float *div, *p, *b0, *res, *e, *b;  // p: the float32 pressure, and the cycles' fine correction
+  float *e2c, *e2l;                     // pre-smoothed corrections: fine level (cell pool), levels >= 1
   double* p64;                          // the float64 pressure of the refinement
   const double* pinv;
   const BScene* scenes;
@@ -119,6 +125,11 @@ __device__ __forceinline__ BLevel level_of(const BPools& P, const BScene& s, int
     L.W = s.lW[k];
   }
   return L;
+}
+
+// The pre-smoothed correction of level k (the fused level kernels' second buffer).
+__device__ __forceinline__ float* e2_of(const BPools& P, const BScene& s, int k) {
+  return k == 0 ? P.e2c + s.oc : P.e2l + s.olev[k];
 }
 
 __device__ __forceinline__ float b_residual(const BLevel& L, int j, int i) {
@@ -425,6 +436,60 @@ __global__ void __launch_bounds__(kBThreads) k_b_coarse(BPools P, int k) {
   }
 }
 
+// Fused level kernels on 16 x 16 tiles of every scene's level k (the work list holds the
+// scenes that smooth at level k): the single-grid shared-memory tile bodies with the scene's
+// level arrays (row stride = row length). pre: SW sweeps from zero (or from e on a W-cycle's
+// second visit), the residual and its full weighting into the coarse rhs, the smoothed
+// correction into the second buffer; post: that correction plus the prolonged coarse one,
+// then SW sweeps, into the level's correction. Blocks stride over the list; inactive scenes
+// are skipped (whole tiles, so every barrier is block-uniform). Blocks are kTBX x kTBY
+// threads, the shape the tile bodies index by.
+template <int SW>
+__global__ void __launch_bounds__(kTThreads) k_b_pre16(BPools P, const BTile* __restrict__ work, int n, int k,
+                                                       float omega, int zero_init) {
+  using S = PreShape<SW, kSX, kSY>;
+  __shared__ __align__(16) float smem[4 * S::EY * S::EXh + S::XR * S::XC];
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    const BTile t = work[w];
+    if (!P.active[t.scene]) continue;
+    const BScene& sc = P.scenes[t.scene];
+    const BLevel L = level_of(P, sc, k), C = level_of(P, sc, k + 1);
+    SplitTile<float> tile =
+        make_tile<float, kSX, kSY>(reinterpret_cast<unsigned char*>(smem), S::HALO, S::EXh, S::EY, L.H, L.W, t.tx, t.ty);
+    float* X = smem + 4 * S::EY * S::EXh;
+    const bool interior = tile.i0 >= 0 && tile.i0 + S::EX <= L.W && tile.j0 >= 0 && tile.j0 + S::EY <= L.H;
+    const float* e_in = zero_init ? nullptr : L.e;
+    if (interior)
+      pre_body<float, SW, kSX, kSY, true>(tile, e_in, e2_of(P, sc, k), L.b, L.W, C.b, C.W, C.H, C.W, omega, X, t.tx,
+                                          t.ty);
+    else
+      pre_body<float, SW, kSX, kSY, false>(tile, e_in, e2_of(P, sc, k), L.b, L.W, C.b, C.W, C.H, C.W, omega, X, t.tx,
+                                           t.ty);
+    __syncthreads();  // the next tile reuses the shared memory
+  }
+}
+
+template <int SW>
+__global__ void __launch_bounds__(kTThreads) k_b_post16(BPools P, const BTile* __restrict__ work, int n, int k,
+                                                        float omega) {
+  using S = PostShape<SW, kSX, kSY>;
+  __shared__ __align__(16) float smem[4 * S::EY * S::EXh];
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    const BTile t = work[w];
+    if (!P.active[t.scene]) continue;
+    const BScene& sc = P.scenes[t.scene];
+    const BLevel L = level_of(P, sc, k), C = level_of(P, sc, k + 1);
+    SplitTile<float> tile =
+        make_tile<float, kSX, kSY>(reinterpret_cast<unsigned char*>(smem), S::HALO, S::EXh, S::EY, L.H, L.W, t.tx, t.ty);
+    const bool interior = tile.i0 >= 0 && tile.i0 + S::EX <= L.W && tile.j0 >= 0 && tile.j0 + S::EY <= L.H;
+    if (interior)
+      post_body<float, SW, kSX, kSY, true>(tile, e2_of(P, sc, k), L.e, L.b, L.W, C.e, C.W, C.H, C.W, omega);
+    else
+      post_body<float, SW, kSX, kSY, false>(tile, e2_of(P, sc, k), L.e, L.b, L.W, C.e, C.W, C.H, C.W, omega);
+    __syncthreads();
+  }
+}
+
 // After the rhs: ||b|| per scene, everyone starts active unless b = 0.
 __global__ void k_b_start(BPools P, BCtl* ctl, cudaGraphConditionalHandle h, int use_handle) {
   int any = 0;
@@ -491,7 +556,8 @@ struct sg_batch {
   // layout (bytes)
   int64_t cells = 0, ufaces = 0, vfaces = 0, lev = 0, pinv_n = 0;
   std::vector<double> pinv;
-  int64_t off_d[2], off_u[2], off_v[2], off_div, off_p, off_p64, off_b0, off_res, off_e, off_b, off_pinv, off_scenes,
+  int64_t off_d[2], off_u[2], off_v[2], off_div, off_p, off_p64, off_b0, off_res, off_e, off_b, off_e2c, off_e2l,
+      off_pinv, off_scenes,
       off_sums,
       off_ints, off_ctl, off_work, bytes = 0;
   int64_t work_cap = 0;  // tiles the work area holds
@@ -504,6 +570,9 @@ struct sg_batch {
   int n_cells = 0, n_faces = 0;
   int64_t lev_off[sg::kBMaxLev] = {0};
   int lev_n[sg::kBMaxLev] = {0};
+  // 16 x 16 tiles of level k of the scenes that smooth there (the fused level kernels)
+  int64_t lev16_off[sg::kBMaxLev] = {0};
+  int lev16_n[sg::kBMaxLev] = {0};
   // graphs: one per parity of the current buffer
   cudaStream_t cs = nullptr;
   cudaGraphExec_t exec[2] = {nullptr, nullptr};
@@ -536,6 +605,8 @@ static BPools pools(const sg_batch* b) {
   P.res = wsp<float>(b, b->off_res);
   P.e = wsp<float>(b, b->off_e);
   P.b = wsp<float>(b, b->off_b);
+  P.e2c = wsp<float>(b, b->off_e2c);
+  P.e2l = wsp<float>(b, b->off_e2l);
   P.pinv = wsp<double>(b, b->off_pinv);
   P.scenes = wsp<BScene>(b, b->off_scenes);
   double* sums = wsp<double>(b, b->off_sums);
@@ -581,6 +652,15 @@ static int build_work(sg_batch* b, cudaStream_t st) {
   }
   b->lev_off[0] = 0;
   b->lev_n[0] = b->n_cells;
+  for (int k = 0; k < b->max_depth; ++k) {
+    b->lev16_off[k] = (int64_t)all.size();
+    add_tiles(all, b, kSX, kSY, [k](const BScene& s, int& r, int& c) {
+      const bool smooths = k < s.nlev - 1;
+      r = smooths ? (k == 0 ? s.H : s.lH[k]) : 0;
+      c = smooths ? (k == 0 ? s.W : s.lW[k]) : 0;
+    });
+    b->lev16_n[k] = (int)((int64_t)all.size() - b->lev16_off[k]);
+  }
   if ((int64_t)all.size() > b->work_cap) return fail(SG_ERR_WORKSPACE, "work list exceeds its reserved area");
   cudaError_t e = cudaMemcpyAsync(b->ws + b->off_work, all.data(), all.size() * sizeof(BTile), cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return fail(SG_ERR_CUDA, "work list upload: %s", cudaGetErrorString(e));
@@ -606,23 +686,65 @@ static void run_sum(const BTile* work, int n, double* out, const F& f, cudaStrea
   SG_LAUNCH(k_b_tiles_sum<TX, TY, F><<<grid_for(n), kBThreads, 0, s>>>(work, n, out, f));
 }
 
+template <int SW>
+static void level_pre(const sg_batch* b, const BPools& P, int k, bool zero_init, cudaStream_t s) {
+  const int n = b->lev16_n[k];
+  if (n > 0)
+    SG_LAUNCH(k_b_pre16<SW><<<grid_for(n), dim3(kTBX, kTBY), 0, s>>>(P, work_at(b, b->lev16_off[k]), n, k, b->omega,
+                                                             zero_init ? 1 : 0));
+}
+
+template <int SW>
+static void level_post(const sg_batch* b, const BPools& P, int k, cudaStream_t s) {
+  const int n = b->lev16_n[k];
+  if (n > 0)
+    SG_LAUNCH(k_b_post16<SW><<<grid_for(n), dim3(kTBX, kTBY), 0, s>>>(P, work_at(b, b->lev16_off[k]), n, k, b->omega));
+}
+
+#ifndef SG_BATCH_FUSE_FROM
+#define SG_BATCH_FUSE_FROM 3
+#endif
+// Depth k of one cycle. Levels k >= SG_BATCH_FUSE_FROM (small: launch-latency-bound) run the
+// fused pre and post kernels; the larger ones run grid-wide half sweeps, the restriction and
+// the prolongation as separate tile-list launches (no halo work, and their data sit in L2).
+// Between them: the exact solve of the scenes whose coarsest level is k + 1 and the deeper
+// levels (twice for W).
 template <int TX, int TY>
-static void cycle_at(const sg_batch* b, const BPools& P, int k, cudaStream_t s) {
+static void cycle_at(const sg_batch* b, const BPools& P, int k, bool zero_init, cudaStream_t s) {
+  const bool fused = k >= SG_BATCH_FUSE_FROM;
   const BTile* lw = work_at(b, b->lev_off[k]);
   const int ln = b->lev_n[k];
-  for (int sw = 0; sw < b->sweeps; ++sw)
-    for (int c = 0; c < 2; ++c) run<TX, TY>(lw, ln, OpRelax{P, k, c, b->omega}, s);
-  run<TX, TY>(work_at(b, b->lev_off[k + 1]), b->lev_n[k + 1], OpRestrict{P, k}, s);
+  if (fused) {
+    switch (b->sweeps) {
+      case 1: level_pre<1>(b, P, k, zero_init, s); break;
+      case 2: level_pre<2>(b, P, k, zero_init, s); break;
+      case 3: level_pre<3>(b, P, k, zero_init, s); break;
+      default: level_pre<4>(b, P, k, zero_init, s); break;
+    }
+  } else {
+    for (int sw = 0; sw < b->sweeps; ++sw)
+      for (int c = 0; c < 2; ++c) run<TX, TY>(lw, ln, OpRelax{P, k, c, b->omega}, s);
+    run<TX, TY>(work_at(b, b->lev_off[k + 1]), b->lev_n[k + 1], OpRestrict{P, k}, s);
+  }
   bool coarse_here = false;
   for (const BScene& sc : b->scenes) coarse_here |= sc.nlev - 1 == k + 1;
   if (coarse_here) SG_LAUNCH(k_b_coarse<<<b->n, kBThreads, 0, s>>>(P, k + 1));
   if (k + 1 < b->max_depth) {
     const int reps = b->wcycle ? 2 : 1;
-    for (int q = 0; q < reps; ++q) cycle_at<TX, TY>(b, P, k + 1, s);
+    for (int q = 0; q < reps; ++q) cycle_at<TX, TY>(b, P, k + 1, q == 0, s);
   }
-  run<TX, TY>(lw, ln, OpProlong{P, k}, s);
-  for (int sw = 0; sw < b->sweeps; ++sw)
-    for (int c = 0; c < 2; ++c) run<TX, TY>(lw, ln, OpRelax{P, k, c, b->omega}, s);
+  if (fused) {
+    switch (b->sweeps) {
+      case 1: level_post<1>(b, P, k, s); break;
+      case 2: level_post<2>(b, P, k, s); break;
+      case 3: level_post<3>(b, P, k, s); break;
+      default: level_post<4>(b, P, k, s); break;
+    }
+  } else {
+    run<TX, TY>(lw, ln, OpProlong{P, k}, s);
+    for (int sw = 0; sw < b->sweeps; ++sw)
+      for (int c = 0; c < 2; ++c) run<TX, TY>(lw, ln, OpRelax{P, k, c, b->omega}, s);
+  }
 }
 
 // One step with the current state in buffer `cur`: everything up to the solve.
@@ -645,7 +767,7 @@ static void solve_body(const sg_batch* b, const BPools& P, cudaGraphConditionalH
   if (b->max_depth == 0) {
     SG_LAUNCH(k_b_coarse<<<b->n, kBThreads, 0, s>>>(P, 0));
   } else {
-    cycle_at<TX, TY>(b, P, 0, s);
+    cycle_at<TX, TY>(b, P, 0, true, s);
   }
   run<TX, TY>(work_at(b, 0), b->n_cells, OpCorrect{P}, s);
   run_sum<TX, TY>(work_at(b, 0), b->n_cells, P.rn2, OpFineResidual{P}, s);
@@ -846,6 +968,10 @@ int sg_batch_create(sg_batch** out, int n_scenes, const int* H, const int* W, co
       best = std::max(best, n);
     }
     b->work_cap += best;
+    for (int k = 0; k + 1 < c.nlev; ++k) {  // the fused level kernels' 16 x 16 tiles
+      const int h = k == 0 ? c.H : c.lH[k], w = k == 0 ? c.W : c.lW[k];
+      b->work_cap += (int64_t)((h + kSY - 1) / kSY) * ((w + kSX - 1) / kSX);
+    }
   }
   int64_t off = 0;
   auto take = [&](int64_t bytes) {
@@ -865,6 +991,8 @@ int sg_batch_create(sg_batch** out, int n_scenes, const int* H, const int* W, co
   b->off_res = take(4 * b->cells);
   b->off_e = take(4 * std::max<int64_t>(b->lev, 1));
   b->off_b = take(4 * std::max<int64_t>(b->lev, 1));
+  b->off_e2c = take(4 * b->cells);
+  b->off_e2l = take(4 * std::max<int64_t>(b->lev, 1));
   b->off_pinv = take(8 * (int64_t)b->pinv.size());
   b->off_scenes = take((int64_t)sizeof(BScene) * n_scenes);
   b->off_sums = take(8 * 3 * (int64_t)n_scenes);

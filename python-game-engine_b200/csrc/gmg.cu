@@ -119,13 +119,7 @@ __device__ __forceinline__ void pcand(int j, int i, int Hc, int Wc, const LevelM
     if (!cm.fluid(cj[q], ci[q])) { cj[q] = J; ci[q] = I; }
 }
 
-// 1-D prolongation weight of fine index i onto coarse index I (grid of n coarse cells).
-__device__ __forceinline__ float w1(int i, int I, int n) {
-  int h = i >> 1;
-  int x = h + ((i & 1) ? 1 : -1);
-  x = x < 0 ? 0 : (x > n - 1 ? n - 1 : x);
-  return (h == I ? 0.75f : 0.0f) + (x == I ? 0.25f : 0.0f);
-}
+#include "gmg_weights.cuh"
 
 // (P^T r)(J, I) with r evaluated on the fly from e and b of the fine level.
 template <typename T>
@@ -503,11 +497,6 @@ struct TailArgs {
   int pre, post, wcycle, zero_init;
 };
 
-// 1 / (number of open faces), n in 1..4.
-template <typename T>
-__device__ __forceinline__ T rcp_open(int n) {
-  return n == 4 ? (T)0.25 : (n == 3 ? (T)(1.0 / 3.0) : (n == 2 ? (T)0.5 : (T)1.0));
-}
 
 // Open-face bits of (j, i): analytic levels from the bounds, others from their codes.
 __device__ __forceinline__ uint8_t tail_code(const LevelMask& m, int j, int i) {

@@ -1,5 +1,5 @@
-// Fused tiled level kernels of the convergent multigrid (included by gmg.cu inside
-// namespace sg; uses w1 and rcp_open from there).
+// Fused tiled level kernels of the convergent multigrid (included by gmg.cu and batch.cu
+// inside namespace sg; uses w1 and rcp_open of gmg_weights.cuh).
 //
 // For open-box levels (every cell fluid, every interior face open) one launch runs a whole
 // side of a cycle on a tile of fine cells held in shared memory (64 x 32 on large levels,
@@ -140,16 +140,18 @@ struct PostShape {
   static constexpr size_t bytes() { return (size_t)(4 * EY * EXh) * sizeof(T); }
 };
 
+// (bx, by): the tile's position in the level's grid of TX x TY tiles.
 template <typename T, int TX, int TY>
-__device__ __forceinline__ SplitTile<T> make_tile(unsigned char* smem, int halo, int EXh, int EY, int H, int W) {
+__device__ __forceinline__ SplitTile<T> make_tile(unsigned char* smem, int halo, int EXh, int EY, int H, int W, int bx,
+                                                  int by) {
   SplitTile<T> t;
   T* base = reinterpret_cast<T*>(smem);
   t.e = base;
   t.b = base + 2 * EY * EXh;
   t.EXh = EXh;
   t.EY = EY;
-  t.i0 = blockIdx.x * TX - halo;
-  t.j0 = blockIdx.y * TY - halo;
+  t.i0 = bx * TX - halo;
+  t.j0 = by * TY - halo;
   t.par0 = (t.i0 + t.j0) & 1;
   t.H = H;
   t.W = W;
@@ -159,7 +161,7 @@ __device__ __forceinline__ SplitTile<T> make_tile(unsigned char* smem, int halo,
 template <typename T, int SW, int TX, int TY, bool INTERIOR>
 __device__ __forceinline__ void pre_body(const SplitTile<T>& t, const T* __restrict__ e_in, T* __restrict__ e_out,
                                          const T* __restrict__ b, int64_t ld, T* __restrict__ bc, int64_t ldc, int Hc,
-                                         int Wc, T omega, T* X) {
+                                         int Wc, T omega, T* X, int bx, int by) {
   using S = PreShape<SW, TX, TY>;
   tile_load<T, INTERIOR, S::EX, S::EY>(t, e_in, b, ld);
   __syncthreads();
@@ -176,7 +178,7 @@ __device__ __forceinline__ void pre_body(const SplitTile<T>& t, const T* __restr
   const int H = t.H, W = t.W;
   for (int f = tile_tid(); f < S::XR * S::XC; f += tile_nt()) {
     const int rr = f / S::XC, Ip = f - rr * S::XC;
-    const int I = blockIdx.x * S::XC + Ip;
+    const int I = bx * S::XC + Ip;
     T acc = (T)0;
     if (I < Wc) {
 #pragma unroll
@@ -193,7 +195,7 @@ __device__ __forceinline__ void pre_body(const SplitTile<T>& t, const T* __restr
   // along y
   for (int f = tile_tid(); f < (TY / 2) * S::XC; f += tile_nt()) {
     const int Jp = f / S::XC, Ip = f - Jp * S::XC;
-    const int J = blockIdx.y * (TY / 2) + Jp, I = blockIdx.x * S::XC + Ip;
+    const int J = by * (TY / 2) + Jp, I = bx * S::XC + Ip;
     if (J >= Hc || I >= Wc) continue;
     T acc = (T)0;
 #pragma unroll
@@ -216,13 +218,13 @@ __global__ void __launch_bounds__(1024) k_gmg_pre_tiled(const T* __restrict__ e_
                                                              T* __restrict__ bc, int64_t ldc, int Hc, int Wc, T omega) {
   using S = PreShape<SW, TX, TY>;
   extern __shared__ __align__(16) unsigned char smem[];
-  SplitTile<T> t = make_tile<T, TX, TY>(smem, S::HALO, S::EXh, S::EY, H, W);
+  SplitTile<T> t = make_tile<T, TX, TY>(smem, S::HALO, S::EXh, S::EY, H, W, blockIdx.x, blockIdx.y);
   T* X = reinterpret_cast<T*>(smem) + 4 * S::EY * S::EXh;
   const bool interior = t.i0 >= 0 && t.i0 + S::EX <= W && t.j0 >= 0 && t.j0 + S::EY <= H;
   if (interior)
-    pre_body<T, SW, TX, TY, true>(t, e_in, e_out, b, ld, bc, ldc, Hc, Wc, omega, X);
+    pre_body<T, SW, TX, TY, true>(t, e_in, e_out, b, ld, bc, ldc, Hc, Wc, omega, X, blockIdx.x, blockIdx.y);
   else
-    pre_body<T, SW, TX, TY, false>(t, e_in, e_out, b, ld, bc, ldc, Hc, Wc, omega, X);
+    pre_body<T, SW, TX, TY, false>(t, e_in, e_out, b, ld, bc, ldc, Hc, Wc, omega, X, blockIdx.x, blockIdx.y);
 }
 
 template <typename T, int SW, int TX, int TY, bool INTERIOR>
@@ -267,7 +269,7 @@ __global__ void __launch_bounds__(1024) k_gmg_post_tiled(const T* __restrict__ e
                                                               T omega) {
   using S = PostShape<SW, TX, TY>;
   extern __shared__ __align__(16) unsigned char smem[];
-  SplitTile<T> t = make_tile<T, TX, TY>(smem, S::HALO, S::EXh, S::EY, H, W);
+  SplitTile<T> t = make_tile<T, TX, TY>(smem, S::HALO, S::EXh, S::EY, H, W, blockIdx.x, blockIdx.y);
   const bool interior = t.i0 >= 0 && t.i0 + S::EX <= W && t.j0 >= 0 && t.j0 + S::EY <= H;
   if (interior)
     post_body<T, SW, TX, TY, true>(t, e_in, e_out, b, ld, ec, ldc, Hc, Wc, omega);
