@@ -102,6 +102,27 @@ __device__ __forceinline__ void reg_half_sweep(T (&e)[RPT][2], const T (&b)[RPT]
   }
 }
 
+// The first half sweep (colour 0) from e = 0: every neighbour is 0, so the update is
+// omega * (b * 1/n) (the general formula with x = 0 and a zero neighbour sum: the same
+// value, up to the sign of a zero) and needs no row exchange.
+template <typename T, int RPT, bool BOUNDED>
+__device__ __forceinline__ void reg_first_half_sweep_from_zero(T (&e)[RPT][2], const T (&b)[RPT][2], T omega, int j,
+                                                               int i, int H, int W) {
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) {
+    const int q = r & 1;
+    if (!BOUNDED) {
+      e[r][q] = omega * (b[r][q] * (T)0.25);
+    } else {
+      const int jj = j + r, ii = i + q;
+      if (jj >= 0 && jj < H && ii >= 0 && ii < W) {
+        const int n = (ii > 0) + (ii < W - 1) + (jj > 0) + (jj < H - 1);
+        if (n > 0) e[r][q] = omega * (b[r][q] * rcp_open<T>(n));
+      }
+    }
+  }
+}
+
 template <typename T, int RPT, int NWARP, int NHS, int HS, bool BOUNDED>
 __device__ __forceinline__ void reg_sweeps(RegXchg<T, NWARP>& x, T (&e)[RPT][2], const T (&b)[RPT][2], T omega,
                                            int w, int lane, int j, int i, int H, int W) {
@@ -183,11 +204,13 @@ __device__ __forceinline__ void reg_pre_body(RegXchg<T, NWARP>& x, const T* __re
   reg_load<T, RPT, BOUNDED>(b, bsrc, ld, j, i, H, W);
   if (e_in) {
     reg_load<T, RPT, BOUNDED>(e, e_in, ld, j, i, H, W);
+    reg_sweeps<T, RPT, NWARP, 2 * SW, 0, BOUNDED>(x, e, b, omega, w, lane, j, i, H, W);
   } else {
 #pragma unroll
     for (int r = 0; r < RPT; ++r) e[r][0] = e[r][1] = (T)0;
+    reg_first_half_sweep_from_zero<T, RPT, BOUNDED>(e, b, omega, j, i, H, W);
+    reg_sweeps<T, RPT, NWARP, 2 * SW, 1, BOUNDED>(x, e, b, omega, w, lane, j, i, H, W);
   }
-  reg_sweeps<T, RPT, NWARP, 2 * SW, 0, BOUNDED>(x, e, b, omega, w, lane, j, i, H, W);
   // residual b - A e in place of b
   T above[2], below[2];
   exchange_rows<T, RPT, NWARP>(x, (2 * SW) & 1, e, w, lane, above, below);
