@@ -77,6 +77,36 @@ __device__ __forceinline__ void relax_ring(const SplitTile<T>& t, int col, T ome
   }
 }
 
+// The first half sweep (colour 0, ring HALO - 1) from e = 0: every neighbour is 0, so a
+// cell's update is omega * (b / n) (the general formula with x = 0 and a zero neighbour sum).
+template <typename T, bool INTERIOR, int HALO, int EXh, int TX, int TY>
+__device__ __forceinline__ void relax_first_from_zero(const SplitTile<T>& t, T omega) {
+  constexpr int RING = HALO - 1;
+  constexpr int RLO = HALO - RING, NR = TY + 2 * RING;
+  constexpr int CLO = HALO - RING, CHI = HALO + TX + RING;
+  constexpr int KW = (CHI - CLO + 1) / 2;
+  constexpr int N = NR * KW;
+  T* E = t.ep(0);
+  const T* Bc = t.bp(0);
+  for (int f = tile_tid(); f < N; f += tile_nt()) {
+    const int rr = f / KW;
+    const int r = RLO + rr;
+    const int p = (t.par0 + r) & 1;
+    const int k = ((CLO - p + 1) >> 1) + (f - rr * KW);
+    if (p + 2 * k >= CHI) continue;
+    const int o = r * EXh + k;
+    if (INTERIOR) {
+      E[o] = omega * (Bc[o] * (T)0.25);
+    } else {
+      const int j = t.j0 + r, i = t.i0 + p + 2 * k;
+      if (j < 0 || j >= t.H || i < 0 || i >= t.W) continue;
+      const int n = (i > 0) + (i < t.W - 1) + (j > 0) + (j < t.H - 1);
+      if (n == 0) continue;
+      E[o] = omega * (Bc[o] * rcp_open<T>(n));
+    }
+  }
+}
+
 // Half sweeps HS .. NHS-1 (colour = HS & 1, ring HALO - 1 - HS).
 template <typename T, bool INTERIOR, int HALO, int EXh, int TX, int TY, int HS, int NHS>
 __device__ __forceinline__ void relax_all(const SplitTile<T>& t, T omega) {
@@ -165,7 +195,13 @@ __device__ __forceinline__ void pre_body(const SplitTile<T>& t, const T* __restr
   using S = PreShape<SW, TX, TY>;
   tile_load<T, INTERIOR, S::EX, S::EY>(t, e_in, b, ld);
   __syncthreads();
-  relax_all<T, INTERIOR, S::HALO, S::EXh, TX, TY, 0, 2 * SW>(t, omega);
+  if (e_in) {
+    relax_all<T, INTERIOR, S::HALO, S::EXh, TX, TY, 0, 2 * SW>(t, omega);
+  } else {
+    relax_first_from_zero<T, INTERIOR, S::HALO, S::EXh, TX, TY>(t, omega);
+    __syncthreads();
+    relax_all<T, INTERIOR, S::HALO, S::EXh, TX, TY, 1, 2 * SW>(t, omega);
+  }
   // residual on the tile plus one ring, in place of b (each cell reads only its own b)
   constexpr int RW = TX + 2, RH = TY + 2, LO = S::HALO - 1;
   for (int f = tile_tid(); f < RW * RH; f += tile_nt()) {
