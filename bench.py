@@ -107,8 +107,10 @@ def _dist():
 
 
 # ----------------------------------------------------------------------------- reference arm
-def cpu_oracle_steps(n_steps, warmup):
-    """Time the CPU oracle on the same scene: returns (seconds per step list, cycles, threads)."""
+def cpu_oracle_steps(n_steps, warmup, fields=None):
+    """Time the CPU oracle on the same scene: returns (seconds per step list, cycles, threads).
+    `fields` (a dict), when given, receives the oracle's density, u, v and pressure after
+    all warmup + n_steps substeps."""
     import numpy as np
 
     import oracle as O
@@ -117,7 +119,7 @@ def cpu_oracle_steps(n_steps, warmup):
     sc = sg.scenes.mixed_2048(steps=n_steps + warmup)
     fmu, fmv = O.face_masks_from_solid(np.zeros((sc.H, sc.W), bool))
     fl = O.is_fluid_from_faces(fmu, fmv)
-    gmg = O.GMGOracle(fmu, fmv, fl, coarsest=8, omega=1.4)
+    gmg = O.GMGOracle(fmu, fmv, fl, coarsest=COARSEST, omega=1.4)  # the GPU arm's hierarchy
     cycles = []
 
     def solver(p, div, fmu_, fmv_, rho, h, dt, **_):
@@ -138,6 +140,9 @@ def cpu_oracle_steps(n_steps, warmup):
         if k >= warmup:
             times.append(time.perf_counter() - t0)
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    if fields is not None:
+        fields.update(steps=n_steps + warmup, density=sim.density.copy(), velocity_u=sim.velocity_u.copy(),
+                      velocity_v=sim.velocity_v.copy(), pressure=sim.pressure.copy())
     return times, cycles[warmup:], threads
 
 
@@ -187,7 +192,9 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
         "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 state, f64/f32 mixed solve", "data": "synthetic",
-        "config": {"workload": "mixed_2048", "grid": [2048, 2048], "solver": "multigrid V(2,2) mixed IR",
+        "config": {"workload": "mixed_2048", "grid": [2048, 2048],
+                   "solver": f"multigrid V(2,2) RBGS w=1.4, full weighting, bilinear, {COARSEST}x{COARSEST} exact "
+                             f"coarsest; FP32 cycles in FP64 iterative refinement",
                    "tol": TOL, "mean_cycles": sum(cycles) / max(len(cycles), 1)},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{len(times)} substeps of mixed_2048 on the CPU oracle (C/OpenMP restatement of "
@@ -232,6 +239,37 @@ def compare_fp64(sg, sc, make, steps):
            "divergence_l2_mixed": float(mixed.divergence.double().norm()),
            "divergence_l2_fp64": float(full.divergence.double().norm())}
     del mixed, full
+    torch.cuda.empty_cache()
+    return out
+
+
+def compare_oracle(sg, sc, make, ofields):
+    """The mixed GPU path run for the CPU oracle's substeps from the same initial state:
+    relative L2 errors of its fields against the oracle's (the reference's kernels restated
+    in C, the same multigrid to 1e-8 in mixed precision on the CPU; pressures compared with
+    their means removed, the pressure being defined up to a constant)."""
+    import numpy as np
+    import torch
+
+    sim = make(torch.float32, "mixed")
+    for _ in range(ofields["steps"]):
+        sim.substep(sc.dt)
+    torch.cuda.synchronize()
+
+    def rel(a, b):
+        a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    p_gpu = sim.pressure.double().cpu().numpy()
+    p_cpu = np.asarray(ofields["pressure"], np.float64)
+    out = {"steps": ofields["steps"],
+           "density_rel_l2": rel(sim.density.cpu().numpy(), ofields["density"]),
+           "velocity_u_rel_l2": rel(sim.velocity_u.cpu().numpy(), ofields["velocity_u"]),
+           "velocity_v_rel_l2": rel(sim.velocity_v.cpu().numpy(), ofields["velocity_v"]),
+           "pressure_rel_l2": rel(p_gpu - p_gpu.mean(), p_cpu - p_cpu.mean()),
+           "oracle": f"CPU restatement of the reference kernels + the same multigrid ({COARSEST}x{COARSEST} exact "
+                     f"coarsest, dense pseudo-inverse) to 1e-8"}
+    del sim
     torch.cuda.empty_cache()
     return out
 
@@ -440,12 +478,15 @@ def run_ours(args):
     tight["mixed_speedup"] = tight["mixed"]["value"] / tight["fp64"]["value"]
     # ---- CPU baseline on a bounded sample (rank 0, one GPU only)
     cpu = None
+    cpu_error = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        times, ccyc, threads = cpu_oracle_steps(args.cpu_steps, 1)
+        ofields = {}
+        times, ccyc, threads = cpu_oracle_steps(args.cpu_steps, 1, ofields)
+        cpu_error = compare_oracle(sg, sc, make, ofields)
         cpu = {"value": cells * len(times) / sum(times), "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{len(times)} substeps of mixed_2048 on the CPU oracle (C/OpenMP restatement of the "
-                         f"reference kernels + the multigrid, 8x8 exact coarsest, to 1e-8), after 1 warm-up substep; "
-                         f"mean {sum(ccyc) / max(len(ccyc), 1):.1f} cycles/step"}
+                         f"reference kernels + the same multigrid, {COARSEST}x{COARSEST} exact coarsest, to "
+                         f"1e-8), after 1 warm-up substep; mean {sum(ccyc) / max(len(ccyc), 1):.1f} cycles/step"}
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -482,6 +523,7 @@ def run_ours(args):
                          "achieved": pre_bytes / (pre_ms / 1e3) / 1e9,
                          "frac": pre_bytes / (pre_ms / 1e3) / 1e9 / peak}}},
         "error_vs_fp64": errors,
+        "error_vs_cpu_oracle": cpu_error,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
