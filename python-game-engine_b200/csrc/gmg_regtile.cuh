@@ -226,7 +226,10 @@ __device__ __forceinline__ void reg_pre_body(RegXchg<T, NWARP>& x, const T* __re
       const T up = r > 0 ? e[r > 0 ? r - 1 : 0][q] : above[q];
       const T down = r < RPT - 1 ? e[r < RPT - 1 ? r + 1 : 0][q] : below[q];
       if (!BOUNDED) {
-        b[r][q] = b[r][q] + (left - xv) + (right - xv) + (up - xv) + (down - xv);
+        if constexpr (sizeof(T) == 8)  // float64: the cheaper sum form (see the fused post kernel)
+          b[r][q] = b[r][q] + (((left + right) + (up + down)) - (T)4 * xv);
+        else
+          b[r][q] = b[r][q] + (left - xv) + (right - xv) + (up - xv) + (down - xv);
       } else {
         const int jj = j + r, ii = i + q;
         T acc = (T)0;
@@ -481,10 +484,16 @@ __device__ __forceinline__ void reg_post_final_body(RegXchg<TC, NWARP>& x, const
       const TP up = (TP)(r > 0 ? e[r > 0 ? r - 1 : 0][q] : above[q]);
       const TP down = (TP)(r < RPT - 1 ? e[r < RPT - 1 ? r + 1 : 0][q] : below[q]);
       if (!BOUNDED) {
-        acc[q] += left - xv[q];
-        acc[q] += right - xv[q];
-        acc[q] += up - xv[q];
-        acc[q] += down - xv[q];
+        if constexpr (sizeof(TP) == 8) {
+          // float64: one sum and one fused multiply-add (the float32 form below keeps the
+          // differences, which stay exact near convergence where the sum would cancel)
+          acc[q] += ((left + right) + (up + down)) - (TP)4 * xv[q];
+        } else {
+          acc[q] += left - xv[q];
+          acc[q] += right - xv[q];
+          acc[q] += up - xv[q];
+          acc[q] += down - xv[q];
+        }
       } else {
         if (ii > 0) acc[q] += left - xv[q];
         if (ii < W - 1) acc[q] += right - xv[q];
