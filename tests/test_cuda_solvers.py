@@ -122,33 +122,35 @@ def test_gmg_one_cycle_cosine_coarsest_vs_oracle(shape, cycle, precision):
     assert np.max(np.abs(got - pe)) <= tol * np.max(np.abs(pe))
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_gmg_remove_mean_reaches_1e10(precision):
+@pytest.mark.parametrize("precision,obstacles", [("fp64", False), ("mixed", False), ("mixed", True)])
+def test_gmg_remove_mean_reaches_1e10(precision, obstacles):
     """An rhs whose sum is not zero (as float rounding leaves a divergence) has a constant part
     no pressure removes: the residual stalls above it. With remove_mean the fluid mean is
     taken off first and the solve reaches 1e-10; its pressure equals the oracle's solve of
     the mean-free rhs."""
     H = W = 256
-    fmu, fmv, fl, div = _problem(H, W, False, 4)
-    div = div + 1e-7 * np.abs(div).max()
+    fmu, fmv, fl, div = _problem(H, W, obstacles, 4)
+    div = (div + 1e-7 * np.abs(div).max()) * fl
     d = dev(div.astype(np.float64 if precision == "fp64" else np.float32))
     h, rho, dt = 1.0 / H, 1.0, 0.5 / H
+    masks = (sg.OPEN_BOX, sg.OPEN_BOX) if not obstacles else (dev(fmu), dev(fmv))
+    coarsest = 8 if obstacles else 32  # the cosine-transform coarsest level needs an open box
     solver = sg.GeometricMultigridSolver()
     p = torch.zeros((H, W), dtype=torch.float64, device="cuda")
-    solver(p, d, sg.OPEN_BOX, sg.OPEN_BOX, rho, h, dt, tol=1e-10, max_cycles=40, precision=precision, coarsest=32)
+    solver(p, d, *masks, rho, h, dt, tol=1e-10, max_cycles=40, precision=precision, coarsest=coarsest)
     assert not solver.converged and solver.last_relres > 1e-10
     p.zero_()
-    solver(p, d, sg.OPEN_BOX, sg.OPEN_BOX, rho, h, dt, tol=1e-10, max_cycles=40, precision=precision, coarsest=32,
+    solver(p, d, *masks, rho, h, dt, tol=1e-10, max_cycles=40, precision=precision, coarsest=coarsest,
            remove_mean=True, strict=True)
-    assert solver.converged and solver.last_relres <= 1e-10 and solver.last_cycles <= 12
+    assert solver.converged and solver.last_relres <= 1e-10 and solver.last_cycles <= (20 if obstacles else 12)
     alpha = O.alpha_coeff(h, rho, dt)
-    b = alpha * d.double().cpu().numpy()
-    b -= b.mean()
+    b = alpha * d.double().cpu().numpy() * fl
+    b[fl] -= b[fl].mean()  # the mean over the fluid cells
     g = O.GMGOracle(fmu, fmv, fl)
     pe = np.zeros((H, W))
     g.solve(pe, b, tol=1e-13, max_cycles=60)
     got = p.double().cpu().numpy()
-    a, e = got - got.mean(), pe - pe.mean()
+    a, e = got[fl] - got[fl].mean(), pe[fl] - pe[fl].mean()
     assert np.max(np.abs(a - e)) <= 1e-5 * np.max(np.abs(e))  # two 1e-10 solves differ by <~ kappa * 1e-10
 
 
