@@ -303,17 +303,20 @@ __global__ void k_gmg_correct(int H, int W, TP* __restrict__ p, int64_t ldp, con
   }
 }
 
+// Sum of partial[0 .. n) over one block (1-D, a multiple of 32 threads): strided sums, then
+// warp shuffles and one barrier (a fixed order, so the result is reproducible); the result
+// is valid in every thread of warp 0.
 __device__ __forceinline__ double sum_partials(const double* __restrict__ partial, int n) {
   double s = 0.0;
   for (int k = threadIdx.x; k < n; k += blockDim.x) s += partial[k];
-  __shared__ double red[1024];
-  red[threadIdx.x] = s;
+  s = warp_sum(s);
+  __shared__ double red[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) red[warp] = s;
   __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-    __syncthreads();
-  }
-  return red[0];
+  double t = 0.0;
+  if (warp == 0) t = warp_sum(lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0);
+  return t;
 }
 
 __global__ void k_gmg_set_params(GmgState* st, double alpha, double tol, int max_cycles) {
