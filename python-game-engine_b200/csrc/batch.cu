@@ -41,6 +41,9 @@ bool open_box_pinv(int H, int W, std::vector<double>& out);
 
 #include "gmg_weights.cuh"
 #include "gmg_tiled.cuh"
+#define SG_REGTILE_BODIES_ONLY
+#include "gmg_regtile.cuh"
+#undef SG_REGTILE_BODIES_ONLY
 
 constexpr int kBMaxLev = 12;
 constexpr int kBThreads = 256;
@@ -66,6 +69,8 @@ struct BPools {
   float* v[2];
   float *div, *p, *b0, *res, *e, *b;  // p: the float32 pressure, and the cycles' fine correction
   float *e2c, *e2l;                     // pre-smoothed corrections: fine level (cell pool), levels >= 1
+  float* b1;                            // the fine rhs of odd cycles (b0: even cycles)
+  double* r64;                          // the fine residual alpha div - A p64, carried in float64
   double* p64;                          // the float64 pressure of the refinement
   const double* pinv;
   const BScene* scenes;
@@ -278,6 +283,7 @@ struct OpRhs {
     const int64_t o = s.oc + (int64_t)j * s.W + i;
     const double b = s.alpha * (double)P.div[o];
     P.b0[o] = (float)b;
+    P.r64[o] = b;
     P.p[o] = 0.0f;
     P.p64[o] = 0.0;
     return b * b;
@@ -490,6 +496,68 @@ __global__ void __launch_bounds__(kTThreads) k_b_post16(BPools P, const BTile* _
   }
 }
 
+// Depth 0 with register tiles (the single-grid fine-level bodies, 64 x 48-cell tiles of
+// every scene's fine level). pre: sweeps from zero on the rhs of the scene's cycle parity,
+// residual and full weighting into level 1 (whose correction it zeroes); post: prolongation,
+// sweeps, p64 += e and the next residual r - A e carried in float64 (r64) with its float32
+// rounding as the next cycle's rhs, and the scene's ||r||^2 by atomic add.
+using BReg = RegShape<float>;
+static_assert(BReg::RPT == BReg::RPT_FINAL && BReg::NWARP == BReg::NWARP_FINAL,
+              "one tile list serves the pre and the fused post kernel");
+
+template <int SW>
+__global__ void __launch_bounds__(32 * BReg::NWARP, BReg::MINB) k_b_reg_pre(BPools P, const BTile* __restrict__ work,
+                                                                          int n, float omega) {
+  using S = RegPre<float, SW, BReg::RPT, BReg::NWARP>;
+  __shared__ RegXchg<float, BReg::NWARP> x;
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    const BTile t = work[w];
+    if (!P.active[t.scene]) continue;
+    const BScene& sc = P.scenes[t.scene];
+    const float* bsrc = ((P.cycles[t.scene] & 1) ? P.b1 : P.b0) + sc.oc;
+    const BLevel C = level_of(P, sc, 1);
+    const int i0 = t.tx * S::TXO - S::HALO, j0 = t.ty * S::TYO - S::HALO;
+    const bool inside = i0 >= 0 && i0 + kRW <= sc.W && j0 >= 0 && j0 + BReg::NWARP * BReg::RPT <= sc.H;
+    if (inside)
+      reg_pre_body<float, SW, BReg::RPT, BReg::NWARP, false>(x, nullptr, P.e2c + sc.oc, bsrc, sc.W, sc.H, sc.W, C.b,
+                                                             C.W, C.H, C.W, omega, i0, j0, C.e);
+    else
+      reg_pre_body<float, SW, BReg::RPT, BReg::NWARP, true>(x, nullptr, P.e2c + sc.oc, bsrc, sc.W, sc.H, sc.W, C.b,
+                                                            C.W, C.H, C.W, omega, i0, j0, C.e);
+    __syncthreads();  // the next tile's row exchange reuses the shared buffers
+  }
+}
+
+template <int SW>
+__global__ void __launch_bounds__(32 * BReg::NWARP, BReg::MINB_FINAL)
+    k_b_reg_post(BPools P, const BTile* __restrict__ work, int n, float omega) {
+  using S = RegPre<float, SW, BReg::RPT, BReg::NWARP>;
+  __shared__ RegXchg<float, BReg::NWARP> x;
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    const BTile t = work[w];
+    if (!P.active[t.scene]) continue;
+    const BScene& sc = P.scenes[t.scene];
+    const bool odd = P.cycles[t.scene] & 1;
+    const float* bsrc = (odd ? P.b1 : P.b0) + sc.oc;
+    float* bdst = (odd ? P.b0 : P.b1) + sc.oc;
+    const BLevel C = level_of(P, sc, 1);
+    const int i0 = t.tx * S::TXO - S::HALO, j0 = t.ty * S::TYO - S::HALO;
+    const bool inside = i0 >= 0 && i0 + kRW <= sc.W && j0 >= 0 && j0 + BReg::NWARP * BReg::RPT <= sc.H;
+    double sq = 0.0;
+    if (inside)
+      reg_post_final_body<float, double, SW, BReg::RPT, BReg::NWARP, false>(
+          x, P.e2c + sc.oc, bsrc, bdst, sc.W, sc.H, sc.W, C.e, C.W, C.H, C.W, omega, P.p64 + sc.oc, sc.W,
+          P.r64 + sc.oc, i0, j0, sq);
+    else
+      reg_post_final_body<float, double, SW, BReg::RPT, BReg::NWARP, true>(
+          x, P.e2c + sc.oc, bsrc, bdst, sc.W, sc.H, sc.W, C.e, C.W, C.H, C.W, omega, P.p64 + sc.oc, sc.W,
+          P.r64 + sc.oc, i0, j0, sq);
+    const double s = block_sum(sq);
+    if (threadIdx.x == 0 && s != 0.0) atomicAdd(P.rn2 + t.scene, s);
+    __syncthreads();
+  }
+}
+
 // After the rhs: ||b|| per scene, everyone starts active unless b = 0.
 __global__ void k_b_start(BPools P, BCtl* ctl, cudaGraphConditionalHandle h, int use_handle) {
   int any = 0;
@@ -557,7 +625,7 @@ struct sg_batch {
   int64_t cells = 0, ufaces = 0, vfaces = 0, lev = 0, pinv_n = 0;
   std::vector<double> pinv;
   int64_t off_d[2], off_u[2], off_v[2], off_div, off_p, off_p64, off_b0, off_res, off_e, off_b, off_e2c, off_e2l,
-      off_pinv, off_scenes,
+      off_b1, off_r64, off_pinv, off_scenes,
       off_sums,
       off_ints, off_ctl, off_work, bytes = 0;
   int64_t work_cap = 0;  // tiles the work area holds
@@ -573,6 +641,14 @@ struct sg_batch {
   // 16 x 16 tiles of level k of the scenes that smooth there (the fused level kernels)
   int64_t lev16_off[sg::kBMaxLev] = {0};
   int lev16_n[sg::kBMaxLev] = {0};
+  // depth 0 on register tiles (every scene smooths its fine level and has an even width
+  // and cell count, so that the paired loads stay aligned): its tile list
+  int reg0 = 0;
+  int64_t reg_off = 0;
+  int reg_n = 0;
+  // the face tiles that can meet a scene's source disc (the sources' launch)
+  int64_t src_off = 0;
+  int src_n = 0;
   // graphs: one per parity of the current buffer
   cudaStream_t cs = nullptr;
   cudaGraphExec_t exec[2] = {nullptr, nullptr};
@@ -607,6 +683,8 @@ static BPools pools(const sg_batch* b) {
   P.b = wsp<float>(b, b->off_b);
   P.e2c = wsp<float>(b, b->off_e2c);
   P.e2l = wsp<float>(b, b->off_e2l);
+  P.b1 = wsp<float>(b, b->off_b1);
+  P.r64 = wsp<double>(b, b->off_r64);
   P.pinv = wsp<double>(b, b->off_pinv);
   P.scenes = wsp<BScene>(b, b->off_scenes);
   double* sums = wsp<double>(b, b->off_sums);
@@ -635,6 +713,23 @@ static void add_tiles(std::vector<BTile>& out, const sg_batch* b, int TX, int TY
   }
 }
 
+// Owned cells of a depth-0 register tile for `sweeps` sweeps per side (1..3).
+static void reg_tile(int sweeps, int& txo, int& tyo) {
+  if (sweeps == 1) {
+    txo = RegPre<float, 1, BReg::RPT, BReg::NWARP>::TXO;
+    tyo = RegPre<float, 1, BReg::RPT, BReg::NWARP>::TYO;
+  } else if (sweeps == 2) {
+    txo = RegPre<float, 2, BReg::RPT, BReg::NWARP>::TXO;
+    tyo = RegPre<float, 2, BReg::RPT, BReg::NWARP>::TYO;
+  } else {
+    txo = RegPre<float, 3, BReg::RPT, BReg::NWARP>::TXO;
+    tyo = RegPre<float, 3, BReg::RPT, BReg::NWARP>::TYO;
+  }
+}
+
+// Depth 0 runs on register tiles when the batch allows it and the sweeps are 1..3.
+static bool reg0_active(const sg_batch* b) { return b->reg0 && b->sweeps >= 1 && b->sweeps <= 3; }
+
 static int build_work(sg_batch* b, cudaStream_t st) {
   const int TX = kTiles[b->tile][0], TY = kTiles[b->tile][1];
   std::vector<BTile> all;
@@ -660,6 +755,30 @@ static int build_work(sg_batch* b, cudaStream_t st) {
       c = smooths ? (k == 0 ? s.W : s.lW[k]) : 0;
     });
     b->lev16_n[k] = (int)((int64_t)all.size() - b->lev16_off[k]);
+  }
+  // source tiles: the face tiles over the disc's bounding box (a point inside the disc lies
+  // within r of its centre, and the points of face (j, i) lie in [i, i + 1] x [j, j + 1])
+  b->src_off = (int64_t)all.size();
+  for (int sidx = 0; sidx < b->n; ++sidx) {
+    const BScene& c = b->scenes[sidx];
+    const double cx = c.src[0], cy = c.src[1], r = c.src[2];
+    const int x0 = std::max(0, (int)std::floor(cx - r) - 2), x1 = std::min(c.W, (int)std::ceil(cx + r) + 2);
+    const int y0 = std::max(0, (int)std::floor(cy - r) - 2), y1 = std::min(c.H, (int)std::ceil(cy + r) + 2);
+    if (x1 < x0 || y1 < y0) continue;
+    for (int ty = y0 / TY; ty <= y1 / TY; ++ty)
+      for (int tx = x0 / TX; tx <= x1 / TX; ++tx) all.push_back(BTile{sidx, (short)ty, (short)tx});
+  }
+  b->src_n = (int)((int64_t)all.size() - b->src_off);
+  b->reg_n = 0;
+  if (reg0_active(b)) {
+    int txo = 0, tyo = 0;
+    reg_tile(b->sweeps, txo, tyo);
+    b->reg_off = (int64_t)all.size();
+    add_tiles(all, b, txo, tyo, [](const BScene& s, int& r, int& c) {
+      r = s.nlev > 1 ? s.H : 0;
+      c = s.nlev > 1 ? s.W : 0;
+    });
+    b->reg_n = (int)((int64_t)all.size() - b->reg_off);
   }
   if ((int64_t)all.size() > b->work_cap) return fail(SG_ERR_WORKSPACE, "work list exceeds its reserved area");
   cudaError_t e = cudaMemcpyAsync(b->ws + b->off_work, all.data(), all.size() * sizeof(BTile), cudaMemcpyHostToDevice, st);
@@ -709,8 +828,41 @@ static void level_post(const sg_batch* b, const BPools& P, int k, cudaStream_t s
 // the prolongation as separate tile-list launches (no halo work, and their data sit in L2).
 // Between them: the exact solve of the scenes whose coarsest level is k + 1 and the deeper
 // levels (twice for W).
+template <int SW>
+static void reg0_pre(const sg_batch* b, const BPools& P, cudaStream_t s) {
+  const unsigned g = (unsigned)std::max(1, std::min(b->reg_n, 148 * BReg::MINB));
+  SG_LAUNCH(k_b_reg_pre<SW><<<g, 32 * BReg::NWARP, 0, s>>>(P, work_at(b, b->reg_off), b->reg_n, b->omega));
+}
+
+template <int SW>
+static void reg0_post(const sg_batch* b, const BPools& P, cudaStream_t s) {
+  const unsigned g = (unsigned)std::max(1, std::min(b->reg_n, 148 * BReg::MINB_FINAL));
+  SG_LAUNCH(k_b_reg_post<SW><<<g, 32 * BReg::NWARP, 0, s>>>(P, work_at(b, b->reg_off), b->reg_n, b->omega));
+}
+
 template <int TX, int TY>
 static void cycle_at(const sg_batch* b, const BPools& P, int k, bool zero_init, cudaStream_t s) {
+  if (k == 0 && reg0_active(b)) {
+    // depth 0 on register tiles; the post kernel also corrects p64 and forms the next residual
+    switch (b->sweeps) {
+      case 1: reg0_pre<1>(b, P, s); break;
+      case 2: reg0_pre<2>(b, P, s); break;
+      default: reg0_pre<3>(b, P, s); break;
+    }
+    bool coarse1 = false;
+    for (const BScene& sc : b->scenes) coarse1 |= sc.nlev - 1 == 1;
+    if (coarse1) SG_LAUNCH(k_b_coarse<<<b->n, kBThreads, 0, s>>>(P, 1));
+    if (1 < b->max_depth) {
+      const int reps = b->wcycle ? 2 : 1;
+      for (int q = 0; q < reps; ++q) cycle_at<TX, TY>(b, P, 1, q == 0, s);
+    }
+    switch (b->sweeps) {
+      case 1: reg0_post<1>(b, P, s); break;
+      case 2: reg0_post<2>(b, P, s); break;
+      default: reg0_post<3>(b, P, s); break;
+    }
+    return;
+  }
   const bool fused = k >= SG_BATCH_FUSE_FROM;
   const BTile* lw = work_at(b, b->lev_off[k]);
   const int ln = b->lev_n[k];
@@ -752,7 +904,7 @@ template <int TX, int TY>
 static void step_head(const sg_batch* b, const BPools& P, int cur, long long step, cudaStream_t s) {
   const BTile* cw = work_at(b, 0);
   const BTile* fw = work_at(b, b->n_cells);
-  run<TX, TY>(fw, b->n_faces, OpPlume{P, cur, b->seed, step < 0 ? 0 : step}, s);
+  run<TX, TY>(work_at(b, b->src_off), b->src_n, OpPlume{P, cur, b->seed, step < 0 ? 0 : step}, s);
   run<TX, TY>(fw, b->n_faces, OpForces{P, cur}, s);
   run<TX, TY>(fw, b->n_faces, OpAdvectUV{P, cur}, s);
   run<TX, TY>(cw, b->n_cells, OpAdvectD{P, cur, b->dissipation}, s);
@@ -769,8 +921,10 @@ static void solve_body(const sg_batch* b, const BPools& P, cudaGraphConditionalH
   } else {
     cycle_at<TX, TY>(b, P, 0, true, s);
   }
-  run<TX, TY>(work_at(b, 0), b->n_cells, OpCorrect{P}, s);
-  run_sum<TX, TY>(work_at(b, 0), b->n_cells, P.rn2, OpFineResidual{P}, s);
+  if (!reg0_active(b)) {  // (the register-tiled depth 0 did both in its post kernel)
+    run<TX, TY>(work_at(b, 0), b->n_cells, OpCorrect{P}, s);
+    run_sum<TX, TY>(work_at(b, 0), b->n_cells, P.rn2, OpFineResidual{P}, s);
+  }
   SG_LAUNCH(k_b_after_cycle<<<1, 1024, 0, s>>>(P, ctl_ptr(b), h, use_handle));
 }
 
@@ -956,6 +1110,11 @@ int sg_batch_create(sg_batch** out, int n_scenes, const int* H, const int* W, co
     }
     c.opinv = shape_off[it - shapes.begin()];
   }
+  // depth 0 on register tiles: every scene smooths its fine level, and every width and cell
+  // count is even (the tiles' paired loads and stores need even element offsets)
+  b->reg0 = 1;
+  for (const BScene& c : b->scenes)
+    if (c.nlev < 2 || (c.W & 1) || ((int64_t)c.H * c.W) & 1) b->reg0 = 0;
   // work area: every scene's cell, face and level tiles under its most fragmenting shape
   b->work_cap = 0;
   for (const BScene& c : b->scenes) {
@@ -971,6 +1130,17 @@ int sg_batch_create(sg_batch** out, int n_scenes, const int* H, const int* W, co
     for (int k = 0; k + 1 < c.nlev; ++k) {  // the fused level kernels' 16 x 16 tiles
       const int h = k == 0 ? c.H : c.lH[k], w = k == 0 ? c.W : c.lW[k];
       b->work_cap += (int64_t)((h + kSY - 1) / kSY) * ((w + kSX - 1) / kSX);
+    }
+    {  // source tiles: at most every face tile of the scene, under the smallest tile shape
+      int64_t most = 0;
+      for (int t = 0; t < kNumTiles; ++t)
+        most = std::max(most, (int64_t)((c.H + kTiles[t][1]) / kTiles[t][1] + 1) * ((c.W + kTiles[t][0]) / kTiles[t][0] + 1));
+      b->work_cap += most;
+    }
+    {  // depth-0 register tiles at their smallest (3 sweeps)
+      int txo = 0, tyo = 0;
+      reg_tile(3, txo, tyo);
+      b->work_cap += (int64_t)((c.H + tyo - 1) / tyo) * ((c.W + txo - 1) / txo);
     }
   }
   int64_t off = 0;
@@ -993,6 +1163,8 @@ int sg_batch_create(sg_batch** out, int n_scenes, const int* H, const int* W, co
   b->off_b = take(4 * std::max<int64_t>(b->lev, 1));
   b->off_e2c = take(4 * b->cells);
   b->off_e2l = take(4 * std::max<int64_t>(b->lev, 1));
+  b->off_b1 = take(4 * b->cells);
+  b->off_r64 = take(8 * b->cells);
   b->off_pinv = take(8 * (int64_t)b->pinv.size());
   b->off_scenes = take((int64_t)sizeof(BScene) * n_scenes);
   b->off_sums = take(8 * 3 * (int64_t)n_scenes);

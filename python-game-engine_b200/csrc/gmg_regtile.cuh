@@ -1,5 +1,6 @@
 // Register-tiled level kernels of the convergent multigrid for large open-box levels
-// (included by gmg.cu inside namespace sg; uses w1 and rcp_open from there).
+// (included inside namespace sg by gmg.cu, and by batch.cu with SG_REGTILE_BODIES_ONLY for
+// the device bodies alone; uses w1 and rcp_open of gmg_weights.cuh).
 //
 // Same two launches per level and cycle as the shared-memory tiles (pre: sweeps + residual
 // + full weighting; post: prolongation + sweeps), but the cells stay in registers:
@@ -196,7 +197,8 @@ struct RegPost {
 template <typename T, int SW, int RPT, int NWARP, bool BOUNDED>
 __device__ __forceinline__ void reg_pre_body(RegXchg<T, NWARP>& x, const T* __restrict__ e_in, T* __restrict__ e_out,
                                              const T* __restrict__ bsrc, int64_t ld, int H, int W, T* __restrict__ bc,
-                                             int64_t ldc, int Hc, int Wc, T omega, int i0, int j0) {
+                                             int64_t ldc, int Hc, int Wc, T omega, int i0, int j0,
+                                             T* __restrict__ ec_zero = nullptr) {
   using S = RegPre<T, SW, RPT, NWARP>;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int i = i0 + 2 * lane, j = j0 + w * RPT;
@@ -294,6 +296,7 @@ __device__ __forceinline__ void reg_pre_body(RegXchg<T, NWARP>& x, const T* __re
       acc += wy2 * X[2 * m + 1];
       acc += wy3 * x3;
       bc[(int64_t)J * ldc + I] = acc;
+      if (ec_zero) ec_zero[(int64_t)J * ldc + I] = (T)0;  // the coarse correction starts at 0
     }
   }
   const int r_lo = S::HALO - w * RPT, r_hi = S::HALO + S::TYO - w * RPT;
@@ -301,6 +304,7 @@ __device__ __forceinline__ void reg_pre_body(RegXchg<T, NWARP>& x, const T* __re
                              r_hi);
 }
 
+#ifndef SG_REGTILE_BODIES_ONLY
 // pre: SW sweeps from e_in (NULL: zero initial guess), residual and its full weighting
 // into bc; the smoothed cells go to e_out.
 // b_alt (fine level of a fused solve only): the rhs alternates between b and b_alt from
@@ -321,6 +325,7 @@ __global__ void __launch_bounds__(32 * NWARP, MINB) k_gmg_pre_reg(const T* __res
   else
     reg_pre_body<T, SW, RPT, NWARP, true>(x, e_in, e_out, b, ld, H, W, bc, ldc, Hc, Wc, omega, i0, j0);
 }
+#endif
 
 // e = e_in + P ec on the thread's cells, then SW sweeps (e and b stay in registers).
 template <typename T, int SW, int RPT, int NWARP, bool BOUNDED>
@@ -401,6 +406,7 @@ __device__ __forceinline__ void reg_post_body(RegXchg<T, NWARP>& x, const T* __r
                              r_hi);
 }
 
+#ifndef SG_REGTILE_BODIES_ONLY
 // post: e_out = smoothed (e_in + P ec).
 template <typename T, int SW, int RPT, int NWARP, int MINB>
 __global__ void __launch_bounds__(32 * NWARP, MINB) k_gmg_post_reg(const T* __restrict__ e_in, T* __restrict__ e_out,
@@ -417,6 +423,7 @@ __global__ void __launch_bounds__(32 * NWARP, MINB) k_gmg_post_reg(const T* __re
   else
     reg_post_body<T, SW, RPT, NWARP, true>(x, e_in, e_out, b, ld, H, W, ec, ldc, Hc, Wc, omega, i0, j0);
 }
+#endif
 
 __device__ __forceinline__ void prefetch_l2(const void* ptr) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
@@ -530,6 +537,7 @@ __device__ __forceinline__ void reg_post_final_body(RegXchg<TC, NWARP>& x, const
   }
 }
 
+#ifndef SG_REGTILE_BODIES_ONLY
 template <typename TC, typename TP, int SW, int RPT, int NWARP, int MINB>
 __global__ void __launch_bounds__(32 * NWARP, MINB)
     k_gmg_post_final_reg(const TC* __restrict__ e_in, TC* __restrict__ b0, TC* __restrict__ b1,
@@ -554,6 +562,7 @@ __global__ void __launch_bounds__(32 * NWARP, MINB)
   const double s = block_sum(sq);
   if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
 }
+#endif
 
 // Rows per thread, warps per block and minimum resident blocks per SM of the register
 // tiles (the last caps the registers a thread may use); MINB_FINAL for the fused fine-level
