@@ -558,6 +558,54 @@ __global__ void __launch_bounds__(32 * BReg::NWARP, BReg::MINB_FINAL)
   }
 }
 
+// Depth k >= 1 on register tiles (the level kernels' bodies): pre from zero (or from the
+// level's correction, on the second visit of a W-cycle) into the level's second buffer,
+// zeroing level k + 1's correction; post from it plus the prolonged coarse correction into
+// the level's correction. The post's halo is two cells narrower, so it has its own tiles.
+template <int SW>
+__global__ void __launch_bounds__(32 * BReg::NWARP, BReg::MINB) k_b_reg_pre_lev(BPools P, const BTile* __restrict__ work,
+                                                                              int n, int k, float omega, int zero) {
+  using S = RegPre<float, SW, BReg::RPT, BReg::NWARP>;
+  __shared__ RegXchg<float, BReg::NWARP> x;
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    const BTile t = work[w];
+    if (!P.active[t.scene]) continue;
+    const BScene& sc = P.scenes[t.scene];
+    const BLevel L = level_of(P, sc, k), C = level_of(P, sc, k + 1);
+    const int i0 = t.tx * S::TXO - S::HALO, j0 = t.ty * S::TYO - S::HALO;
+    const bool inside = i0 >= 0 && i0 + kRW <= L.W && j0 >= 0 && j0 + BReg::NWARP * BReg::RPT <= L.H;
+    if (inside)
+      reg_pre_body<float, SW, BReg::RPT, BReg::NWARP, false>(x, zero ? nullptr : L.e, e2_of(P, sc, k), L.b, L.W, L.H,
+                                                             L.W, C.b, C.W, C.H, C.W, omega, i0, j0, C.e);
+    else
+      reg_pre_body<float, SW, BReg::RPT, BReg::NWARP, true>(x, zero ? nullptr : L.e, e2_of(P, sc, k), L.b, L.W, L.H,
+                                                            L.W, C.b, C.W, C.H, C.W, omega, i0, j0, C.e);
+    __syncthreads();
+  }
+}
+
+template <int SW>
+__global__ void __launch_bounds__(32 * BReg::NWARP, BReg::MINB) k_b_reg_post_lev(BPools P, const BTile* __restrict__ work,
+                                                                               int n, int k, float omega) {
+  using S = RegPost<float, SW, BReg::RPT, BReg::NWARP>;
+  __shared__ RegXchg<float, BReg::NWARP> x;
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    const BTile t = work[w];
+    if (!P.active[t.scene]) continue;
+    const BScene& sc = P.scenes[t.scene];
+    const BLevel L = level_of(P, sc, k), C = level_of(P, sc, k + 1);
+    const int i0 = t.tx * S::TXO - S::HALO, j0 = t.ty * S::TYO - S::HALO;
+    const bool inside = i0 >= 0 && i0 + kRW <= L.W && j0 >= 0 && j0 + BReg::NWARP * BReg::RPT <= L.H;
+    if (inside)
+      reg_post_body<float, SW, BReg::RPT, BReg::NWARP, false>(x, e2_of(P, sc, k), L.e, L.b, L.W, L.H, L.W, C.e, C.W,
+                                                              C.H, C.W, omega, i0, j0);
+    else
+      reg_post_body<float, SW, BReg::RPT, BReg::NWARP, true>(x, e2_of(P, sc, k), L.e, L.b, L.W, L.H, L.W, C.e, C.W,
+                                                             C.H, C.W, omega, i0, j0);
+    __syncthreads();
+  }
+}
+
 // After the rhs: ||b|| per scene, everyone starts active unless b = 0.
 __global__ void k_b_start(BPools P, BCtl* ctl, cudaGraphConditionalHandle h, int use_handle) {
   int any = 0;
@@ -646,6 +694,11 @@ struct sg_batch {
   int reg0 = 0;
   int64_t reg_off = 0;
   int reg_n = 0;
+  // depths 1 .. SG_BATCH_REG_TO - 1 on register tiles (every scene that smooths there has an
+  // even level width and offset): their pre and post tile lists
+  int regk[sg::kBMaxLev] = {0};
+  int64_t regk_pre_off[sg::kBMaxLev] = {0}, regk_post_off[sg::kBMaxLev] = {0};
+  int regk_pre_n[sg::kBMaxLev] = {0}, regk_post_n[sg::kBMaxLev] = {0};
   // the face tiles that can meet a scene's source disc (the sources' launch)
   int64_t src_off = 0;
   int src_n = 0;
@@ -713,18 +766,33 @@ static void add_tiles(std::vector<BTile>& out, const sg_batch* b, int TX, int TY
   }
 }
 
-// Owned cells of a depth-0 register tile for `sweeps` sweeps per side (1..3).
-static void reg_tile(int sweeps, int& txo, int& tyo) {
+// Owned cells of a register tile for `sweeps` sweeps per side (1..3): the pre shape (also
+// depth 0's fused post) or the plain post shape of the coarser depths.
+template <template <typename, int, int, int> class Shape>
+static void reg_tile_of(int sweeps, int& txo, int& tyo) {
   if (sweeps == 1) {
-    txo = RegPre<float, 1, BReg::RPT, BReg::NWARP>::TXO;
-    tyo = RegPre<float, 1, BReg::RPT, BReg::NWARP>::TYO;
+    txo = Shape<float, 1, BReg::RPT, BReg::NWARP>::TXO;
+    tyo = Shape<float, 1, BReg::RPT, BReg::NWARP>::TYO;
   } else if (sweeps == 2) {
-    txo = RegPre<float, 2, BReg::RPT, BReg::NWARP>::TXO;
-    tyo = RegPre<float, 2, BReg::RPT, BReg::NWARP>::TYO;
+    txo = Shape<float, 2, BReg::RPT, BReg::NWARP>::TXO;
+    tyo = Shape<float, 2, BReg::RPT, BReg::NWARP>::TYO;
   } else {
-    txo = RegPre<float, 3, BReg::RPT, BReg::NWARP>::TXO;
-    tyo = RegPre<float, 3, BReg::RPT, BReg::NWARP>::TYO;
+    txo = Shape<float, 3, BReg::RPT, BReg::NWARP>::TXO;
+    tyo = Shape<float, 3, BReg::RPT, BReg::NWARP>::TYO;
   }
+}
+static void reg_tile(int sweeps, int& txo, int& tyo) { reg_tile_of<RegPre>(sweeps, txo, tyo); }
+
+#ifndef SG_BATCH_REG_TO
+#define SG_BATCH_REG_TO 4
+#endif
+// Depth k >= 1 runs on register tiles when it is below SG_BATCH_REG_TO, depth 0 does, and its
+// levels allow it. (256 mixed scenes of 64..256 a side, 2 sweeps, V-cycle: 2.61 ms per step
+// with depth 0 alone on register tiles, 2.31 with depth 1 too, 2.18 through depth 3, and
+// no gain below: the deeper levels hold a few tiles per scene.)
+static bool regk_active(const sg_batch* b, int k) {
+  return k >= 1 && k < SG_BATCH_REG_TO && k < sg::kBMaxLev && b->regk[k] && b->reg0 && b->sweeps >= 1 &&
+         b->sweeps <= 3;
 }
 
 // Depth 0 runs on register tiles when the batch allows it and the sweeps are 1..3.
@@ -780,6 +848,23 @@ static int build_work(sg_batch* b, cudaStream_t st) {
     });
     b->reg_n = (int)((int64_t)all.size() - b->reg_off);
   }
+  for (int k = 1; k < sg::kBMaxLev; ++k) {
+    b->regk_pre_n[k] = b->regk_post_n[k] = 0;
+    if (!regk_active(b, k)) continue;
+    auto smooth_shape = [k](const BScene& s, int& r, int& c) {
+      r = k < s.nlev - 1 ? s.lH[k] : 0;
+      c = k < s.nlev - 1 ? s.lW[k] : 0;
+    };
+    int txo = 0, tyo = 0;
+    reg_tile_of<RegPre>(b->sweeps, txo, tyo);
+    b->regk_pre_off[k] = (int64_t)all.size();
+    add_tiles(all, b, txo, tyo, smooth_shape);
+    b->regk_pre_n[k] = (int)((int64_t)all.size() - b->regk_pre_off[k]);
+    reg_tile_of<RegPost>(b->sweeps, txo, tyo);
+    b->regk_post_off[k] = (int64_t)all.size();
+    add_tiles(all, b, txo, tyo, smooth_shape);
+    b->regk_post_n[k] = (int)((int64_t)all.size() - b->regk_post_off[k]);
+  }
   if ((int64_t)all.size() > b->work_cap) return fail(SG_ERR_WORKSPACE, "work list exceeds its reserved area");
   cudaError_t e = cudaMemcpyAsync(b->ws + b->off_work, all.data(), all.size() * sizeof(BTile), cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return fail(SG_ERR_CUDA, "work list upload: %s", cudaGetErrorString(e));
@@ -823,11 +908,6 @@ static void level_post(const sg_batch* b, const BPools& P, int k, cudaStream_t s
 #ifndef SG_BATCH_FUSE_FROM
 #define SG_BATCH_FUSE_FROM 3
 #endif
-// Depth k of one cycle. Levels k >= SG_BATCH_FUSE_FROM (small: launch-latency-bound) run the
-// fused pre and post kernels; the larger ones run grid-wide half sweeps, the restriction and
-// the prolongation as separate tile-list launches (no halo work, and their data sit in L2).
-// Between them: the exact solve of the scenes whose coarsest level is k + 1 and the deeper
-// levels (twice for W).
 template <int SW>
 static void reg0_pre(const sg_batch* b, const BPools& P, cudaStream_t s) {
   const unsigned g = (unsigned)std::max(1, std::min(b->reg_n, 148 * BReg::MINB));
@@ -840,8 +920,50 @@ static void reg0_post(const sg_batch* b, const BPools& P, cudaStream_t s) {
   SG_LAUNCH(k_b_reg_post<SW><<<g, 32 * BReg::NWARP, 0, s>>>(P, work_at(b, b->reg_off), b->reg_n, b->omega));
 }
 
+template <int SW>
+static void regk_pre(const sg_batch* b, const BPools& P, int k, bool zero_init, cudaStream_t s) {
+  const int n = b->regk_pre_n[k];
+  if (n > 0)
+    SG_LAUNCH(k_b_reg_pre_lev<SW><<<(unsigned)std::min(n, 148 * BReg::MINB), 32 * BReg::NWARP, 0, s>>>(
+        P, work_at(b, b->regk_pre_off[k]), n, k, b->omega, zero_init ? 1 : 0));
+}
+
+template <int SW>
+static void regk_post(const sg_batch* b, const BPools& P, int k, cudaStream_t s) {
+  const int n = b->regk_post_n[k];
+  if (n > 0)
+    SG_LAUNCH(k_b_reg_post_lev<SW><<<(unsigned)std::min(n, 148 * BReg::MINB), 32 * BReg::NWARP, 0, s>>>(
+        P, work_at(b, b->regk_post_off[k]), n, k, b->omega));
+}
+
+// Depth k of one cycle: a pre launch (sweeps, residual, restriction), the exact solve of the
+// scenes whose coarsest level is k + 1, the deeper levels (twice for W), a post launch
+// (prolongation, sweeps). Depth 0 and the depths below SG_BATCH_REG_TO run on register tiles
+// when the batch allows it; otherwise levels k >= SG_BATCH_FUSE_FROM run the fused 16 x 16
+// tile kernels, and the larger ones grid-wide half sweeps, the restriction and the
+// prolongation as separate tile-list launches.
 template <int TX, int TY>
 static void cycle_at(const sg_batch* b, const BPools& P, int k, bool zero_init, cudaStream_t s) {
+  if (regk_active(b, k)) {
+    switch (b->sweeps) {
+      case 1: regk_pre<1>(b, P, k, zero_init, s); break;
+      case 2: regk_pre<2>(b, P, k, zero_init, s); break;
+      default: regk_pre<3>(b, P, k, zero_init, s); break;
+    }
+    bool coarse_here = false;
+    for (const BScene& sc : b->scenes) coarse_here |= sc.nlev - 1 == k + 1;
+    if (coarse_here) SG_LAUNCH(k_b_coarse<<<b->n, kBThreads, 0, s>>>(P, k + 1));
+    if (k + 1 < b->max_depth) {
+      const int reps = b->wcycle ? 2 : 1;
+      for (int q = 0; q < reps; ++q) cycle_at<TX, TY>(b, P, k + 1, q == 0, s);
+    }
+    switch (b->sweeps) {
+      case 1: regk_post<1>(b, P, k, s); break;
+      case 2: regk_post<2>(b, P, k, s); break;
+      default: regk_post<3>(b, P, k, s); break;
+    }
+    return;
+  }
   if (k == 0 && reg0_active(b)) {
     // depth 0 on register tiles; the post kernel also corrects p64 and forms the next residual
     switch (b->sweeps) {
@@ -1115,6 +1237,11 @@ int sg_batch_create(sg_batch** out, int n_scenes, const int* H, const int* W, co
   b->reg0 = 1;
   for (const BScene& c : b->scenes)
     if (c.nlev < 2 || (c.W & 1) || ((int64_t)c.H * c.W) & 1) b->reg0 = 0;
+  for (int k = 1; k < kBMaxLev; ++k) {
+    b->regk[k] = k <= b->max_depth ? 1 : 0;
+    for (const BScene& c : b->scenes)
+      if (k < c.nlev - 1 && ((c.lW[k] & 1) || (c.olev[k] & 1))) b->regk[k] = 0;
+  }
   // work area: every scene's cell, face and level tiles under its most fragmenting shape
   b->work_cap = 0;
   for (const BScene& c : b->scenes) {
@@ -1137,10 +1264,12 @@ int sg_batch_create(sg_batch** out, int n_scenes, const int* H, const int* W, co
         most = std::max(most, (int64_t)((c.H + kTiles[t][1]) / kTiles[t][1] + 1) * ((c.W + kTiles[t][0]) / kTiles[t][0] + 1));
       b->work_cap += most;
     }
-    {  // depth-0 register tiles at their smallest (3 sweeps)
+    {  // register tiles at their smallest (3 sweeps; the pre shape bounds the post's too)
       int txo = 0, tyo = 0;
       reg_tile(3, txo, tyo);
       b->work_cap += (int64_t)((c.H + tyo - 1) / tyo) * ((c.W + txo - 1) / txo);
+      for (int k = 1; k + 1 < c.nlev && k < SG_BATCH_REG_TO; ++k)
+        b->work_cap += 2 * (int64_t)((c.lH[k] + tyo - 1) / tyo) * ((c.lW[k] + txo - 1) / txo);
     }
   }
   int64_t off = 0;

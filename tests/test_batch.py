@@ -48,7 +48,31 @@ def test_each_scene_steps_like_a_single_scene_simulation():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("tile,sweeps,cycle", [(1, 1, "V"), (2, 2, "W"), (3, 2, "V")])
+@pytest.mark.parametrize("shapes", [[(96, 70), (64, 64)], [(63, 77), (96, 96)]])
+def test_irregular_sizes_step_like_single_scenes(shapes):
+    """Odd level widths take depths off the register tiles (a fine width of 70 leaves depth 1
+    at 35 columns; an odd fine width leaves every depth to the tile-list kernels): the
+    batch must still step each scene like its single-scene simulation."""
+    scs = [S.Scene(f"irregular_{H}x{W}", H, W, 10, -1.0, [[0.5 * W, 0.15 * H, 0.1 * min(H, W), 1.0, 1.0, 0.0]],
+                   seed=7 + H) for H, W in shapes]
+    tol = 1e-6
+    b = B.BatchedSmoke(scs, tol=tol)
+    sims = [_single(sc, tol) for sc in scs]
+    for _ in range(5):
+        b.step()
+        for sim, sc in zip(sims, scs):
+            sim.substep(sc.dt)
+    torch.cuda.synchronize()
+    assert np.all(b.stats()[1] <= tol)
+    for k, sim in enumerate(sims):
+        d, u, v, _ = b.fields(k)
+        assert float((d - sim.density).abs().max()) <= 1e-4, k
+        assert float((u - sim.velocity_u).abs().max()) <= 1e-4 * max(float(sim.velocity_u.abs().max()), 1e-3), k
+        assert float((v - sim.velocity_v).abs().max()) <= 1e-4 * max(float(sim.velocity_v.abs().max()), 1e-3), k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tile,sweeps,cycle", [(1, 1, "V"), (2, 2, "W"), (3, 2, "V"), (0, 4, "W")])
 def test_configurations_agree(tile, sweeps, cycle):
     scs = _scenes(range(10, 18))
     ref = B.BatchedSmoke(scs, tol=1e-7)
