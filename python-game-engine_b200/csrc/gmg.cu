@@ -1025,10 +1025,13 @@ static int tail_launch(const sg_gmg_plan* p, bool zero_init, cudaStream_t s) {
 // The fused tiled kernels serve open-box level pairs with 1..3 sweeps per side.
 static bool fused_level(const sg_gmg_plan* p, int k) { return p->levels[k].fused != 0; }
 
-// Large tiles while a level fills the GPU with them (two blocks per SM), small tiles below:
-// a small level is latency-bound, and more blocks with less serial work each finish sooner.
+// Register tiles on levels of at least SG_GMG_REG_MIN_TILES 64 x 32 blocks, 16 x 16 shared-
+// memory tiles below: a small level is latency-bound, and more blocks with less serial work
+// each finish sooner. Per V-cycle at 2048^2 (32^2 exact coarsest; mixed / float64 / float32):
+// threshold 296 (512^2 on small tiles) 139 / 165 / 125 us, 100 (512^2 on register tiles)
+// 137 / 159 / 123, 30 (256^2 too) 141 / 160 / 127, every level 150 / 163 / 136.
 #ifndef SG_GMG_REG_MIN_TILES
-#define SG_GMG_REG_MIN_TILES (2 * 148)
+#define SG_GMG_REG_MIN_TILES 100
 #endif
 static bool small_tiles(const Level& L) {
   const int64_t large_blocks = (int64_t)((L.W + kTX - 1) / kTX) * ((L.H + kTY - 1) / kTY);
