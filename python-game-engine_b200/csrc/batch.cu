@@ -171,6 +171,11 @@ __device__ __forceinline__ void for_tiles_sum(const BTile* __restrict__ work, in
 }
 
 // -------------------------------------------------------------- step operators
+// Velocity buffers: the state lives in u/v[kVel] between steps; u/v[kVelAdv] holds the
+// advected (and forced) velocity until the projection writes the projected one back into
+// u/v[kVel]. Density ping-pongs between d[0] and d[1] by the step's parity.
+constexpr int kVel = 0, kVelAdv = 1;
+
 // Batched sources carry no noise (amplitude 0), so the step index the noise would hash is
 // not needed and the captured step graph can be replayed as is.
 struct OpPlume {
@@ -181,7 +186,7 @@ struct OpPlume {
   __device__ void operator()(int sc, int j, int i) const {
     const BScene& s = P.scenes[sc];
     if (j > s.H || i > s.W) return;
-    plume_point(j, i, s.H, s.W, P.d[cur] + s.oc, (int64_t)s.W, P.u[cur] + s.ou, (int64_t)s.W + 1, P.v[cur] + s.ov,
+    plume_point(j, i, s.H, s.W, P.d[cur] + s.oc, (int64_t)s.W, P.u[kVel] + s.ou, (int64_t)s.W + 1, P.v[kVel] + s.ov,
                 (int64_t)s.W, s.src, 1, seed + (uint64_t)sc, step);
   }
 };
@@ -192,27 +197,26 @@ struct OpForces {
   __device__ void operator()(int sc, int j, int i) const {
     const BScene& s = P.scenes[sc];
     if (j > s.H || i >= s.W) return;
-    forces_face(j, i, s.H, s.W, P.v[cur] + s.ov, (int64_t)s.W, (const float*)(P.d[cur] + s.oc), (int64_t)s.W,
+    forces_face(j, i, s.H, s.W, P.v[kVel] + s.ov, (int64_t)s.W, (const float*)(P.d[cur] + s.oc), (int64_t)s.W,
                 (const float*)nullptr, 0, s.dt, s.gravity, 0.0, s.dcoef, 0.0, 1);
   }
 };
 
 struct OpAdvectUV {
   BPools P;
-  int cur;
   __device__ void operator()(int sc, int j, int i) const {
     const BScene& s = P.scenes[sc];
     const int H = s.H, W = s.W;
     const MasksT<SG_MASK_OPEN> m = open_masks(H, W);
-    const float* us = P.u[cur] + s.ou;
-    const float* vs = P.v[cur] + s.ov;
+    const float* us = P.u[kVel] + s.ou;
+    const float* vs = P.v[kVel] + s.ov;
     if (j < H && i <= W)
-      P.u[1 - cur][s.ou + (int64_t)j * (W + 1) + i] =
+      P.u[kVelAdv][s.ou + (int64_t)j * (W + 1) + i] =
           m.u(j, i) ? advect_u_face(j, i, us, (int64_t)W + 1, (int64_t)H, (int64_t)W + 1, vs, (int64_t)H + 1,
                                     (int64_t)W, (int64_t)W, s.dt, s.inv)
                     : 0.0f;
     if (j <= H && i < W)
-      P.v[1 - cur][s.ov + (int64_t)j * W + i] =
+      P.v[kVelAdv][s.ov + (int64_t)j * W + i] =
           m.v(j, i) ? advect_v_face(j, i, vs, (int64_t)W, (int64_t)H + 1, (int64_t)W, us, (int64_t)H, (int64_t)W + 1,
                                     (int64_t)W + 1, s.dt, s.inv)
                     : 0.0f;
@@ -230,62 +234,76 @@ struct OpAdvectD {
     const MasksT<SG_MASK_OPEN> m = open_masks(H, W);
     P.d[1 - cur][s.oc + (int64_t)j * W + i] =
         advect_scalar_cell(j, i, H, W, (const float*)(P.d[cur] + s.oc), (int64_t)W,
-                           (const float*)(P.u[1 - cur] + s.ou), (int64_t)H, (int64_t)W + 1, (int64_t)W + 1,
-                           (const float*)(P.v[1 - cur] + s.ov), (int64_t)H + 1, (int64_t)W, (int64_t)W, m, s.dt,
+                           (const float*)(P.u[kVelAdv] + s.ou), (int64_t)H, (int64_t)W + 1, (int64_t)W + 1,
+                           (const float*)(P.v[kVelAdv] + s.ov), (int64_t)H + 1, (int64_t)W, (int64_t)W, m, s.dt,
                            s.inv, diss);
   }
 };
 
-struct OpDivergence {
-  BPools P;
-  int nxt;
-  __device__ void operator()(int sc, int j, int i) const {
-    const BScene& s = P.scenes[sc];
-    if (j >= s.H || i >= s.W) return;
-    const MasksT<SG_MASK_OPEN> m = open_masks(s.H, s.W);
-    P.div[s.oc + (int64_t)j * s.W + i] = divergence_cell(j, i, (const float*)(P.u[nxt] + s.ou), (int64_t)s.W + 1,
-                                                         (const float*)(P.v[nxt] + s.ov), (int64_t)s.W, m, s.inv);
-  }
-};
-
-struct OpProject {
-  BPools P;
-  int nxt;
-  __device__ void operator()(int sc, int j, int i) const {
-    const BScene& s = P.scenes[sc];
-    const MasksT<SG_MASK_OPEN> m = open_masks(s.H, s.W);
-    project_faces<float, MasksT<SG_MASK_OPEN>, SG_MASK_RING>(j, i, s.H, s.W, P.u[nxt] + s.ou, (int64_t)s.W + 1, P.v[nxt] + s.ov, (int64_t)s.W,
-                  (const float*)(P.p + s.oc), (int64_t)s.W, m, 1, SG_MASK_RING, (const uint8_t*)nullptr, 0, s.scale);
-  }
-};
-
-// metrics tail of the substep (simulation.py:251-265): the reference residual of p
-struct OpResidual {
+// The end of the step on one cell tile list (simulation.py:245-265): the pressure out of the
+// float64 solve, the gradient subtraction with the wall conditions written out of place into
+// the velocity state (each thread projects its cell's four faces from the advected velocity
+// and stores the lower and left ones, the last column and row also the outer ones), the
+// divergence of the projected faces and the reference residual of the pressure.
+struct OpTail {
   BPools P;
   __device__ void operator()(int sc, int j, int i) const {
     const BScene& s = P.scenes[sc];
-    if (j >= s.H || i >= s.W) return;
-    const MasksT<SG_MASK_OPEN> m = open_masks(s.H, s.W);
-    P.res[s.oc + (int64_t)j * s.W + i] =
-        residual_cell(j, i, s.H, s.W, (const float*)(P.p + s.oc), (int64_t)s.W, (const float*)(P.div + s.oc),
-                      (int64_t)s.W, m, s.alpha, 4.0);
+    const int H = s.H, W = s.W;
+    if (j >= H || i >= W) return;
+    using MK = MasksT<SG_MASK_OPEN>;
+    const MK m = open_masks(H, W);
+    const double* q = P.p64 + s.oc + (int64_t)j * W + i;
+    const float c = (float)q[0];
+    const float pl = i > 0 ? (float)q[-1] : c, pr = i < W - 1 ? (float)q[1] : c;
+    const float pd = j > 0 ? (float)q[-W] : c, pu = j < H - 1 ? (float)q[W] : c;
+    const float* ua = P.u[kVelAdv] + s.ou + (int64_t)j * (W + 1) + i;
+    const float* va = P.v[kVelAdv] + s.ov + (int64_t)j * W + i;
+    const float ul = projected_u_pv<float, MK, SG_MASK_RING>(j, i, H, W, ua[0], c, pl, m, SG_MASK_RING, nullptr, 0,
+                                                           s.scale);
+    const float ur = projected_u_pv<float, MK, SG_MASK_RING>(j, i + 1, H, W, ua[1], pr, c, m, SG_MASK_RING, nullptr,
+                                                           0, s.scale);
+    const float vd = projected_v_pv<float, MK, SG_MASK_RING>(j, i, H, W, va[0], c, pd, m, SG_MASK_RING, nullptr, 0,
+                                                           s.scale);
+    const float vu = projected_v_pv<float, MK, SG_MASK_RING>(j + 1, i, H, W, va[W], pu, c, m, SG_MASK_RING, nullptr,
+                                                           0, s.scale);
+    float* u = P.u[kVel] + s.ou + (int64_t)j * (W + 1) + i;
+    float* v = P.v[kVel] + s.ov + (int64_t)j * W + i;
+    u[0] = ul;
+    if (i == W - 1) u[1] = ur;
+    v[0] = vd;
+    if (j == H - 1) v[W] = vu;
+    const int64_t o = s.oc + (int64_t)j * W + i;
+    const float dv = divergence_from_faces(j, i, ul, ur, vd, vu, m, s.inv);
+    P.p[o] = c;
+    P.div[o] = dv;
+    P.res[o] = residual_from_values(j, i, H, W, c, pl, pr, pd, pu, dv, m, s.alpha, 4.0);
   }
 };
 
 // -------------------------------------------------------------- solver operators
-// b = alpha div: the first cycle's rhs (the residual of p = 0) in float32, p = 0 and the
-// correction 0, ||b||^2 per scene.
+// The divergence of the advected velocity and b = alpha div: the first cycle's rhs (the
+// residual of p = 0) in float32 and float64, p64 = 0, ||b||^2 per scene. With depth 0 on
+// the tile-list kernels (tiles0), p is that depth's correction (zeroed here) and div feeds
+// the fine residual (stored here).
 struct OpRhs {
   BPools P;
+  int tiles0;
   __device__ double operator()(int sc, int j, int i) const {
     const BScene& s = P.scenes[sc];
     if (j >= s.H || i >= s.W) return 0.0;
+    const MasksT<SG_MASK_OPEN> m = open_masks(s.H, s.W);
+    const float dv = divergence_cell(j, i, (const float*)(P.u[kVelAdv] + s.ou), (int64_t)s.W + 1,
+                                     (const float*)(P.v[kVelAdv] + s.ov), (int64_t)s.W, m, s.inv);
     const int64_t o = s.oc + (int64_t)j * s.W + i;
-    const double b = s.alpha * (double)P.div[o];
+    const double b = s.alpha * (double)dv;
     P.b0[o] = (float)b;
     P.r64[o] = b;
-    P.p[o] = 0.0f;
     P.p64[o] = 0.0;
+    if (tiles0) {
+      P.div[o] = dv;
+      P.p[o] = 0.0f;
+    }
     return b * b;
   }
 };
@@ -300,17 +318,6 @@ struct OpCorrect {
     const int64_t o = s.oc + (int64_t)j * s.W + i;
     P.p64[o] += (double)P.p[o];
     P.p[o] = 0.0f;
-  }
-};
-
-// The pressure the projection uses.
-struct OpPressureOut {
-  BPools P;
-  __device__ void operator()(int sc, int j, int i) const {
-    const BScene& s = P.scenes[sc];
-    if (j >= s.H || i >= s.W) return;
-    const int64_t o = s.oc + (int64_t)j * s.W + i;
-    P.p[o] = (float)P.p64[o];
   }
 };
 
@@ -873,6 +880,8 @@ static int build_work(sg_batch* b, cudaStream_t st) {
 
 static const BTile* work_at(const sg_batch* b, int64_t first) { return wsp<BTile>(b, b->off_work) + first; }
 
+// Tile-list launches: one resident wave of blocks walking the list (four waves measured the
+// same, a block per tile 5 % slower over the step: these tiles are short).
 static unsigned grid_for(int n) {
   const int cap = 148 * (2048 / kBThreads);
   return (unsigned)std::max(1, std::min(n, cap));
@@ -908,15 +917,21 @@ static void level_post(const sg_batch* b, const BPools& P, int k, cudaStream_t s
 #ifndef SG_BATCH_FUSE_FROM
 #define SG_BATCH_FUSE_FROM 3
 #endif
+// Blocks of a register-tile launch: one per tile (the kernels keep a grid-stride loop). The
+// batch step measured 2.18 ms with one resident wave of blocks walking the list, 2.11 with
+// two, 2.08 with four and 2.06 with a block per tile: a block that retires early frees its
+// SM slot for the next tile, where a walking block waits on its own tiles' latency.
+static unsigned reg_grid(int n, int /*minb*/) { return (unsigned)std::max(1, n); }
+
 template <int SW>
 static void reg0_pre(const sg_batch* b, const BPools& P, cudaStream_t s) {
-  const unsigned g = (unsigned)std::max(1, std::min(b->reg_n, 148 * BReg::MINB));
+  const unsigned g = reg_grid(b->reg_n, BReg::MINB);
   SG_LAUNCH(k_b_reg_pre<SW><<<g, 32 * BReg::NWARP, 0, s>>>(P, work_at(b, b->reg_off), b->reg_n, b->omega));
 }
 
 template <int SW>
 static void reg0_post(const sg_batch* b, const BPools& P, cudaStream_t s) {
-  const unsigned g = (unsigned)std::max(1, std::min(b->reg_n, 148 * BReg::MINB_FINAL));
+  const unsigned g = reg_grid(b->reg_n, BReg::MINB_FINAL);
   SG_LAUNCH(k_b_reg_post<SW><<<g, 32 * BReg::NWARP, 0, s>>>(P, work_at(b, b->reg_off), b->reg_n, b->omega));
 }
 
@@ -924,7 +939,7 @@ template <int SW>
 static void regk_pre(const sg_batch* b, const BPools& P, int k, bool zero_init, cudaStream_t s) {
   const int n = b->regk_pre_n[k];
   if (n > 0)
-    SG_LAUNCH(k_b_reg_pre_lev<SW><<<(unsigned)std::min(n, 148 * BReg::MINB), 32 * BReg::NWARP, 0, s>>>(
+    SG_LAUNCH(k_b_reg_pre_lev<SW><<<reg_grid(n, BReg::MINB), 32 * BReg::NWARP, 0, s>>>(
         P, work_at(b, b->regk_pre_off[k]), n, k, b->omega, zero_init ? 1 : 0));
 }
 
@@ -932,7 +947,7 @@ template <int SW>
 static void regk_post(const sg_batch* b, const BPools& P, int k, cudaStream_t s) {
   const int n = b->regk_post_n[k];
   if (n > 0)
-    SG_LAUNCH(k_b_reg_post_lev<SW><<<(unsigned)std::min(n, 148 * BReg::MINB), 32 * BReg::NWARP, 0, s>>>(
+    SG_LAUNCH(k_b_reg_post_lev<SW><<<reg_grid(n, BReg::MINB), 32 * BReg::NWARP, 0, s>>>(
         P, work_at(b, b->regk_post_off[k]), n, k, b->omega));
 }
 
@@ -1028,11 +1043,10 @@ static void step_head(const sg_batch* b, const BPools& P, int cur, long long ste
   const BTile* fw = work_at(b, b->n_cells);
   run<TX, TY>(work_at(b, b->src_off), b->src_n, OpPlume{P, cur, b->seed, step < 0 ? 0 : step}, s);
   run<TX, TY>(fw, b->n_faces, OpForces{P, cur}, s);
-  run<TX, TY>(fw, b->n_faces, OpAdvectUV{P, cur}, s);
+  run<TX, TY>(fw, b->n_faces, OpAdvectUV{P}, s);
   run<TX, TY>(cw, b->n_cells, OpAdvectD{P, cur, b->dissipation}, s);
-  run<TX, TY>(cw, b->n_cells, OpDivergence{P, 1 - cur}, s);
   SG_LAUNCH(k_b_clear_sums<<<1, 1024, 0, s>>>(P, b->n));
-  run_sum<TX, TY>(cw, b->n_cells, P.bn2, OpRhs{P}, s);
+  run_sum<TX, TY>(cw, b->n_cells, P.bn2, OpRhs{P, reg0_active(b) ? 0 : 1}, s);
 }
 
 template <int TX, int TY>
@@ -1051,13 +1065,8 @@ static void solve_body(const sg_batch* b, const BPools& P, cudaGraphConditionalH
 }
 
 template <int TX, int TY>
-static void step_tail(const sg_batch* b, const BPools& P, int cur, cudaStream_t s) {
-  const BTile* cw = work_at(b, 0);
-  const BTile* fw = work_at(b, b->n_cells);
-  run<TX, TY>(cw, b->n_cells, OpPressureOut{P}, s);
-  run<TX, TY>(fw, b->n_faces, OpProject{P, 1 - cur}, s);
-  run<TX, TY>(cw, b->n_cells, OpDivergence{P, 1 - cur}, s);
-  run<TX, TY>(cw, b->n_cells, OpResidual{P}, s);
+static void step_tail(const sg_batch* b, const BPools& P, cudaStream_t s) {
+  run<TX, TY>(work_at(b, 0), b->n_cells, OpTail{P}, s);
 }
 
 #define SG_BTRY(x, what)                                                                  \
@@ -1096,7 +1105,7 @@ static int build_step_graph(sg_batch* b, int cur, cudaGraphExec_t* out) {
   SG_BTRY(cudaGraphAddNode(&cnode, cg, deps, ndeps, &cp), "conditional node");
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   SG_BTRY(cudaStreamUpdateCaptureDependencies(cs, &cnode, 1, cudaStreamSetCaptureDependencies), "deps");
-  step_tail<TX, TY>(b, P, cur, cs);
+  step_tail<TX, TY>(b, P, cs);
   unsigned long long c1 = launch_count();
   SG_BTRY(cudaStreamEndCapture(cs, &g), "end capture");
   SG_BTRY(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
@@ -1321,8 +1330,8 @@ int sg_batch_layout(const sg_batch* b, int scene, int64_t* off_density, int64_t*
   const BScene& c = b->scenes[scene];
   const int q = b->cur;
   if (off_density) *off_density = b->off_d[q] + 4 * c.oc;
-  if (off_u) *off_u = b->off_u[q] + 4 * c.ou;
-  if (off_v) *off_v = b->off_v[q] + 4 * c.ov;
+  if (off_u) *off_u = b->off_u[kVel] + 4 * c.ou;
+  if (off_v) *off_v = b->off_v[kVel] + 4 * c.ov;
   if (off_pressure) *off_pressure = b->off_p + 4 * c.oc;
   return SG_OK;
 }
