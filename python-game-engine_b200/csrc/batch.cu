@@ -881,29 +881,83 @@ static int build_work(sg_batch* b, cudaStream_t st) {
 static const BTile* work_at(const sg_batch* b, int64_t first) { return wsp<BTile>(b, b->off_work) + first; }
 
 // Tile-list launches: one resident wave of blocks walking the list (four waves measured the
-// same, a block per tile 5 % slower over the step: these tiles are short).
-static unsigned grid_for(int n) {
-  const int cap = 148 * (2048 / kBThreads);
-  return (unsigned)std::max(1, std::min(n, cap));
+// same, a block per tile 5 % slower over the step: these tiles are short). The wave is the
+// kernel's own occupancy times the SMs: with more blocks than fit at once, the rest would
+// run as a second, partial wave (the tail op's 40 registers fit six blocks of 256 threads
+// per SM, the scalar advection's 48 five).
+template <class K>
+static int resident_blocks(K kernel, int threads, size_t smem) {
+  int per_sm = 0, dev = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1 ||
+      cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) {
+    (void)cudaGetLastError();
+    return 148 * (2048 / threads);
+  }
+  return per_sm * sms;
 }
+
+template <int TX, int TY, class F>
+static int tiles_cap() {
+  static const int cap = resident_blocks(k_b_tiles<TX, TY, F>, kBThreads, 0);
+  return cap;
+}
+
+template <int TX, int TY, class F>
+static int tiles_sum_cap() {
+  static const int cap = resident_blocks(k_b_tiles_sum<TX, TY, F>, kBThreads, 0);
+  return cap;
+}
+
+static unsigned grid_of(int n, int cap) { return (unsigned)std::max(1, std::min(n, cap)); }
 
 template <int TX, int TY, class F>
 static void run(const BTile* work, int n, const F& f, cudaStream_t s) {
   if (n <= 0) return;
-  SG_LAUNCH(k_b_tiles<TX, TY, F><<<grid_for(n), kBThreads, 0, s>>>(work, n, f));
+  SG_LAUNCH(k_b_tiles<TX, TY, F><<<grid_of(n, tiles_cap<TX, TY, F>()), kBThreads, 0, s>>>(work, n, f));
 }
 
 template <int TX, int TY, class F>
 static void run_sum(const BTile* work, int n, double* out, const F& f, cudaStream_t s) {
   if (n <= 0) return;
-  SG_LAUNCH(k_b_tiles_sum<TX, TY, F><<<grid_for(n), kBThreads, 0, s>>>(work, n, out, f));
+  SG_LAUNCH(k_b_tiles_sum<TX, TY, F><<<grid_of(n, tiles_sum_cap<TX, TY, F>()), kBThreads, 0, s>>>(work, n, out, f));
+}
+
+template <int SW>
+static int pre16_cap() {
+  static const int cap = resident_blocks(k_b_pre16<SW>, kTBX * kTBY, 0);
+  return cap;
+}
+
+template <int SW>
+static int post16_cap() {
+  static const int cap = resident_blocks(k_b_post16<SW>, kTBX * kTBY, 0);
+  return cap;
+}
+
+// The occupancy queries run once per kernel, before any stream capture.
+template <int TX, int TY>
+static void prime_caps() {
+  tiles_cap<TX, TY, OpPlume>();
+  tiles_cap<TX, TY, OpForces>();
+  tiles_cap<TX, TY, OpAdvectUV>();
+  tiles_cap<TX, TY, OpAdvectD>();
+  tiles_cap<TX, TY, OpTail>();
+  tiles_cap<TX, TY, OpRelax>();
+  tiles_cap<TX, TY, OpRestrict>();
+  tiles_cap<TX, TY, OpProlong>();
+  tiles_cap<TX, TY, OpCorrect>();
+  tiles_sum_cap<TX, TY, OpRhs>();
+  tiles_sum_cap<TX, TY, OpFineResidual>();
+  pre16_cap<1>(), pre16_cap<2>(), pre16_cap<3>(), pre16_cap<4>();
+  post16_cap<1>(), post16_cap<2>(), post16_cap<3>(), post16_cap<4>();
 }
 
 template <int SW>
 static void level_pre(const sg_batch* b, const BPools& P, int k, bool zero_init, cudaStream_t s) {
   const int n = b->lev16_n[k];
   if (n > 0)
-    SG_LAUNCH(k_b_pre16<SW><<<grid_for(n), dim3(kTBX, kTBY), 0, s>>>(P, work_at(b, b->lev16_off[k]), n, k, b->omega,
+    SG_LAUNCH(k_b_pre16<SW><<<grid_of(n, pre16_cap<SW>()), dim3(kTBX, kTBY), 0, s>>>(P, work_at(b, b->lev16_off[k]), n, k, b->omega,
                                                              zero_init ? 1 : 0));
 }
 
@@ -911,7 +965,7 @@ template <int SW>
 static void level_post(const sg_batch* b, const BPools& P, int k, cudaStream_t s) {
   const int n = b->lev16_n[k];
   if (n > 0)
-    SG_LAUNCH(k_b_post16<SW><<<grid_for(n), dim3(kTBX, kTBY), 0, s>>>(P, work_at(b, b->lev16_off[k]), n, k, b->omega));
+    SG_LAUNCH(k_b_post16<SW><<<grid_of(n, post16_cap<SW>()), dim3(kTBX, kTBY), 0, s>>>(P, work_at(b, b->lev16_off[k]), n, k, b->omega));
 }
 
 #ifndef SG_BATCH_FUSE_FROM
@@ -1078,6 +1132,7 @@ static void step_tail(const sg_batch* b, const BPools& P, cudaStream_t s) {
 // Graph of one step starting from buffer `cur`: head, WHILE(any scene active) cycle, tail.
 template <int TX, int TY>
 static int build_step_graph(sg_batch* b, int cur, cudaGraphExec_t* out) {
+  prime_caps<TX, TY>();
   BPools P = pools(b);
   cudaStream_t cs = b->cs;
   cudaGraph_t g = nullptr;
