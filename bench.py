@@ -4,7 +4,7 @@
 
 Workload ``mixed_2048``: one SmokeSimulation2D substep of the 2048^2 four-source
 scene (float32 state), pressure solved by the convergent multigrid (V(2,2),
-red-black Gauss-Seidel omega 1.4, full weighting, bilinear prolongation, the 32^2
+red-black Gauss-Seidel omega 1.3, full weighting, bilinear prolongation, the 32^2
 coarsest level solved exactly by the cosine transform) with FP32 cycles inside FP64
 iterative refinement to a relative residual of 1e-8 (and, in a short second run, 1e-10), then projection and the reference's metrics tail. The same scene is also
 timed with a float64 state and an all-FP64 solve to the same residual ("fp64_gpu").
@@ -41,6 +41,7 @@ UNIT = "cell-steps/s"
 TOL = 1e-8
 TOL_TIGHT = 1e-10  # the workload's second residual target
 COARSEST = 32  # exact coarsest level (open box: cosine transform); the hierarchy is 2048^2 .. 32^2
+OMEGA = 1.3  # red-black Gauss-Seidel over-relaxation of the multigrid (GPU arms and the oracle)
 
 
 def _peaks():
@@ -119,7 +120,7 @@ def cpu_oracle_steps(n_steps, warmup, fields=None):
     sc = sg.scenes.mixed_2048(steps=n_steps + warmup)
     fmu, fmv = O.face_masks_from_solid(np.zeros((sc.H, sc.W), bool))
     fl = O.is_fluid_from_faces(fmu, fmv)
-    gmg = O.GMGOracle(fmu, fmv, fl, coarsest=COARSEST, omega=1.4)  # the GPU arm's hierarchy
+    gmg = O.GMGOracle(fmu, fmv, fl, coarsest=COARSEST, omega=OMEGA)  # the GPU arm's hierarchy
     cycles = []
 
     def solver(p, div, fmu_, fmv_, rho, h, dt, **_):
@@ -157,7 +158,7 @@ def cpu_oracle_batch(scenes, steps):
     for sc in scenes:
         fmu, fmv = O.face_masks_from_solid(np.zeros((sc.H, sc.W), bool))
         fl = O.is_fluid_from_faces(fmu, fmv)
-        gmg = O.GMGOracle(fmu, fmv, fl, coarsest=8, omega=1.4)
+        gmg = O.GMGOracle(fmu, fmv, fl, coarsest=8, omega=OMEGA)
 
         def solver(p, div, fmu_, fmv_, rho, h, dt, gmg=gmg, fl=fl, **_):
             b = O.alpha_coeff(h, rho, dt) * div.astype(np.float64) * fl
@@ -193,7 +194,7 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 state, f64/f32 mixed solve", "data": "synthetic",
         "config": {"workload": "mixed_2048", "grid": [2048, 2048],
-                   "solver": f"multigrid V(2,2) RBGS w=1.4, full weighting, bilinear, {COARSEST}x{COARSEST} exact "
+                   "solver": f"multigrid V(2,2) RBGS w={OMEGA}, full weighting, bilinear, {COARSEST}x{COARSEST} exact "
                              f"coarsest; FP32 cycles in FP64 iterative refinement",
                    "tol": TOL, "mean_cycles": sum(cycles) / max(len(cycles), 1)},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
@@ -304,7 +305,7 @@ def run_ours(args):
         return float(t.item())
 
     def make(dtype, precision, tol=TOL, remove_mean=False):
-        params = sg.GeometricMultigridParams(tol=tol, max_cycles=40, precision=precision, omega=1.4,
+        params = sg.GeometricMultigridParams(tol=tol, max_cycles=40, precision=precision, omega=OMEGA,
                                              coarsest=COARSEST, fixed_cycles=args.fixed_cycles,
                                              remove_mean=remove_mean)
         return sg.scenes.make_sim(sc, "geometric_multigrid", params, dtype=dtype, device=dev)
@@ -496,7 +497,7 @@ def run_ours(args):
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 state + f64/f32 mixed solve", "data": "synthetic",
         "config": {"workload": "mixed_2048", "grid": [2048, 2048], "sources": 4, "solver":
-                   "multigrid V(2,2) RBGS w=1.4, full weighting, bilinear, 32x32 exact coarsest (cosine transform); "
+                   f"multigrid V(2,2) RBGS w={OMEGA}, full weighting, bilinear, 32x32 exact coarsest (cosine transform); "
                    "FP32 cycles in FP64 "
                    "iterative refinement", "tol": TOL, "mean_cycles_per_step": info["cycles"] / max(info["solves"], 1),
                    "converged": bool(relres_ok), "l2": "working set > 126 MB L2; no flush",

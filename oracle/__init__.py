@@ -554,7 +554,7 @@ class GMGOracle:
     pseudo-inverse of its operator after removing the rhs mean.
     """
 
-    def __init__(self, fmu, fmv, fluid, coarsest=8, omega=1.4, pre=2, post=2, cycle="V"):
+    def __init__(self, fmu, fmv, fluid, coarsest=8, omega=1.3, pre=2, post=2, cycle="V"):
         self.levels = []
         f, cu, cv = fluid.astype(bool), fmu.astype(bool), fmv.astype(bool)
         while True:

@@ -90,7 +90,7 @@ class GeometricMultigridParams:
     cycle: str = "V"            # "V" or "W"
     pre_sweeps: int = 2
     post_sweeps: int = 2
-    omega: float = 1.4          # red-black Gauss-Seidel over-relaxation (1.0 = plain GS)
+    omega: float = 1.3          # red-black Gauss-Seidel over-relaxation (1.0 = plain GS)
     coarsest: int = 8           # coarsen until both extents <= coarsest
     precision: str = "fp64"     # "fp32" | "fp64" | "mixed" (FP32 cycles in FP64 refinement)
     check_every: int = 1        # host convergence check interval (cycles)

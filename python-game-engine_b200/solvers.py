@@ -225,7 +225,7 @@ _PRECISION = {"fp32": L.SG_GMG_FP32, "fp64": L.SG_GMG_FP64, "mixed": L.SG_GMG_MI
 class GMGPlan:
     """A bound multigrid plan (host plan + device workspace) for one grid and mask."""
 
-    def __init__(self, H, W, fmu, fmv, device, coarsest=8, omega=1.4, pre=2, post=2, cycle="V", precision="fp64",
+    def __init__(self, H, W, fmu, fmv, device, coarsest=8, omega=1.3, pre=2, post=2, cycle="V", precision="fp64",
                  remove_mean=False):
         lib = L.load()
         self.H, self.W, self.precision = H, W, precision
@@ -369,7 +369,7 @@ class GeometricMultigridSolver:
         return plan
 
     def __call__(self, pressure, divergence, face_mask_u, face_mask_v, fluid_density, cell_size, dt, tol=1e-6,
-                 max_cycles=50, cycle="V", pre_sweeps=2, post_sweeps=2, omega=1.4, coarsest=8, precision="fp64",
+                 max_cycles=50, cycle="V", pre_sweeps=2, post_sweeps=2, omega=1.3, coarsest=8, precision="fp64",
                  check_every=1, fixed_cycles=0, rebuild_masks=False, strict=False, zero_initial_guess=False,
                  remove_mean=False, **_ignored):
         H, W = pressure.shape

@@ -25,6 +25,7 @@ from cuda_adapter import dev  # noqa: E402
 
 sg = package()
 scenes = sg.scenes
+OMEGA = 1.3  # the red-black over-relaxation of both the CUDA multigrid and the oracle's
 
 
 def _oracle_sim(scene, solver, kw, dtype):
@@ -86,7 +87,7 @@ def test_gmg_one_cycle_vs_oracle(shape, obstacles, cycle, precision):
     H, W = shape
     fmu, fmv, fl, div = _problem(H, W, obstacles, 1)
     alpha = -0.7
-    g = O.GMGOracle(fmu, fmv, fl, coarsest=8, omega=1.4, cycle=cycle)
+    g = O.GMGOracle(fmu, fmv, fl, coarsest=8, omega=OMEGA, cycle=cycle)
     pe = np.zeros((H, W))
     g.vcycle(0, pe, alpha * div)
     solver = sg.GeometricMultigridSolver()
@@ -94,7 +95,7 @@ def test_gmg_one_cycle_vs_oracle(shape, obstacles, cycle, precision):
     p = torch.zeros((H, W), dtype=torch.float32 if precision == "fp32" else torch.float64, device="cuda")
     # cell_size, rho, dt chosen so that alpha = -(h^2) rho / dt = -0.7
     solver(p, dev(div.astype(np.float64 if precision == "fp64" else np.float32)), masks[0], masks[1], 0.7, 1.0, 1.0,
-           precision=precision, fixed_cycles=1, cycle=cycle)
+           precision=precision, fixed_cycles=1, cycle=cycle, omega=OMEGA)
     got = p.double().cpu().numpy()
     tol = 1e-10 if precision == "fp64" else 2e-5
     assert np.max(np.abs(got - pe)) <= tol * np.max(np.abs(pe))
@@ -110,13 +111,13 @@ def test_gmg_one_cycle_cosine_coarsest_vs_oracle(shape, cycle, precision):
     H, W = shape
     fmu, fmv, fl, div = _problem(H, W, False, 3)
     alpha = -0.7
-    g = O.GMGOracle(fmu, fmv, fl, coarsest=32, omega=1.4, cycle=cycle)
+    g = O.GMGOracle(fmu, fmv, fl, coarsest=32, omega=OMEGA, cycle=cycle)
     pe = np.zeros((H, W))
     g.vcycle(0, pe, alpha * div)
     solver = sg.GeometricMultigridSolver()
     p = torch.zeros((H, W), dtype=torch.float32 if precision == "fp32" else torch.float64, device="cuda")
     solver(p, dev(div.astype(np.float64 if precision == "fp64" else np.float32)), sg.OPEN_BOX, sg.OPEN_BOX, 0.7,
-           1.0, 1.0, precision=precision, fixed_cycles=1, cycle=cycle, coarsest=32)
+           1.0, 1.0, precision=precision, fixed_cycles=1, cycle=cycle, coarsest=32, omega=OMEGA)
     got = p.double().cpu().numpy()
     tol = 1e-10 if precision == "fp64" else 2e-5
     assert np.max(np.abs(got - pe)) <= tol * np.max(np.abs(pe))
