@@ -403,7 +403,7 @@ int sg_batch_graph_nodes(const sg_batch* batch, int* step_nodes, int* cycle_node
 int sg_batch_stats(sg_batch* batch, int* cycles, double* relres, long long* total_cycles, void* stream);
 /* Scratch bytes the autotuner needs for its snapshot of the state. */
 int64_t sg_batch_snapshot_bytes(const sg_batch* batch);
-/* Time `steps` steps of every (tile, sweeps in 1..2, V/W) candidate from the current state
+/* Time `steps` steps of every (tile, sweeps in 1..3, V/W) candidate from the current state
  * (restored each time), configure the fastest whose scenes all converged. */
 int sg_batch_autotune(sg_batch* batch, int steps, void* scratch, int64_t scratch_bytes, void* stream, int* tile,
                       int* sweeps, int* wcycle, double* ms_per_step);

@@ -1498,7 +1498,7 @@ int sg_batch_autotune(sg_batch* b, int steps, void* scratch, int64_t scratch_byt
   int rc = SG_OK;
   std::vector<int> cyc(b->n);
   for (int t = 0; t < kNumTiles && rc == SG_OK; ++t)
-    for (int sw = 1; sw <= 2 && rc == SG_OK; ++sw)
+    for (int sw = 1; sw <= 3 && rc == SG_OK; ++sw)
       for (int w = 0; w <= 1 && rc == SG_OK; ++w) {
         b->tile = t;
         b->sweeps = sw;
