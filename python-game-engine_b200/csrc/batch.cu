@@ -5,15 +5,16 @@
 // own buoyancy coefficient, cell size and time step. All scenes' fields live in shared
 // pools (one per field kind, scene by scene, row stride = row length). Each operator of the
 // step is ONE persistent launch over a work list of tiles (scene, tile row, tile column):
-// blocks of 256 threads stride over the list, each tile being TX x TY cells of one scene, so
-// small and large scenes fill the GPU together. The per-cell arithmetic is the single-grid
+// one resident wave of 256-thread blocks strides over the list, each tile being TX x TY
+// cells of one scene, so small and large scenes fill the GPU together. The per-cell arithmetic is the single-grid
 // operators' own (cell_ops.cuh); this unit is compiled with -fmad=false like theirs.
 //
 // The pressure solve is the convergent multigrid of the single-grid solver (red-black
 // Gauss-Seidel with omega, full-weighting restriction, bilinear prolongation, exact solve
 // on the coarsest level <= 8 x 8 through its pseudo-inverse; each side of a level is one
-// launch over 16 x 16 tiles of all scenes, with the single-grid shared-memory tile bodies
-// of gmg_tiled.cuh: sweeps, residual and restriction in shared memory) in the single-grid solver's
+// launch over a tile list of all scenes: the single-grid register-tile bodies of
+// gmg_regtile.cuh on depths 0-3, the shared-memory 16 x 16 tile bodies of gmg_tiled.cuh
+// below, sweeps, residual and restriction on chip) in the single-grid solver's
 // mixed precision: float32 cycles on the correction equation inside float64 iterative
 // refinement (p and the residual b - A p in float64), until each scene's relative residual
 // ||b - A p|| / ||b|| is <= tol; the pressure the projection uses is p rounded to float32.
