@@ -212,3 +212,59 @@ def test_product_path_does_not_import_the_oracle():
             with open(os.path.join(pkg, fn)) as f:
                 src = f.read()
             assert not re.search(r"^\s*(import|from)\s+oracle\b", src, re.M), fn
+
+
+def _batch_create(scenes, tol=1e-6):
+    from importlib import import_module
+
+    B = import_module("python-game-engine_b200.batch")
+    n = len(scenes)
+    H = (ctypes.c_int * n)(*[s.H for s in scenes])
+    W = (ctypes.c_int * n)(*[s.W for s in scenes])
+    params = np.ascontiguousarray(np.asarray([B.scene_params(s) for s in scenes], dtype=np.float64))
+    h = ctypes.c_void_p()
+    rc = L.load().sg_batch_create(ctypes.byref(h), n, H, W, params.ctypes.data_as(ctypes.c_void_p), tol, 50, 0)
+    return rc, h
+
+
+def test_batch_plan_layout_on_the_host():
+    """A batch's pools, offsets and workspace are laid out on the host (no GPU): fields scene
+    by scene, the velocity state in one fixed buffer, and every tile shape known."""
+    lib = L.load()
+    scenes = sg.scenes.batch_256(16)
+    rc, h = _batch_create(scenes)
+    assert rc == L.SG_OK
+    try:
+        cells = sum(s.H * s.W for s in scenes)
+        nbytes = lib.sg_batch_workspace_bytes(h)
+        # at least: two density buffers, two u and v buffers, p, p64, rhs (x2), r64, div, res
+        assert nbytes >= 4 * cells * 14 and nbytes < 64 * cells * 20
+        offs = [[ctypes.c_int64() for _ in range(4)] for _ in scenes]
+        for k, o in enumerate(offs):
+            assert lib.sg_batch_layout(h, k, *[ctypes.byref(x) for x in o]) == L.SG_OK
+        for k in range(1, len(scenes)):
+            a, b = scenes[k - 1], scenes[k]
+            assert offs[k][0].value - offs[k - 1][0].value == 4 * a.H * a.W  # density
+            assert offs[k][1].value - offs[k - 1][1].value == 4 * a.H * (a.W + 1)  # u faces
+            assert offs[k][2].value - offs[k - 1][2].value == 4 * (a.H + 1) * a.W  # v faces
+            assert offs[k][3].value - offs[k - 1][3].value == 4 * a.H * a.W  # pressure
+        assert all(x.value % 4 == 0 and 0 <= x.value < nbytes for o in offs for x in o)
+        assert lib.sg_batch_layout(h, len(scenes), None, None, None, None) == L.SG_ERR_ARG
+    finally:
+        lib.sg_batch_destroy(h)
+    tx, ty = ctypes.c_int(), ctypes.c_int()
+    shapes = []
+    for t in range(4):
+        assert lib.sg_batch_tile_shape(t, ctypes.byref(tx), ctypes.byref(ty)) == L.SG_OK
+        shapes.append(f"{tx.value}x{ty.value}")
+    assert shapes == sg.batch.TILE_NAMES
+    assert lib.sg_batch_tile_shape(4, ctypes.byref(tx), ctypes.byref(ty)) == L.SG_ERR_ARG
+
+
+def test_batch_create_rejects_bad_scenes():
+    sc = sg.scenes.batch_scene(0)
+    tiny = sg.scenes.Scene("tiny", 1, 64, 10, -1.0, [[32.0, 0.5, 0.4, 1.0, 1.0, 0.0]])
+    rc, h = _batch_create([sc, tiny])
+    assert rc == L.SG_ERR_ARG and not h.value and b"grid" in L.load().sg_last_error()
+    rc, h = _batch_create([sc], tol=0.0)
+    assert rc == L.SG_ERR_ARG and not h.value
