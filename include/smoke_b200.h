@@ -394,7 +394,8 @@ int sg_batch_step(sg_batch* batch, int n_steps, void* stream);
  * v ((H+1) x W) and pressure (H x W), float32, row stride = row length. */
 int sg_batch_layout(const sg_batch* batch, int scene, int64_t* off_density, int64_t* off_u, int64_t* off_v,
                     int64_t* off_pressure);
-/* Which of the two field buffers holds the current state (0 / 1). */
+/* Which of the two density buffers holds the current state (0 / 1); the velocity state
+ * always lives in the first velocity buffer (the projection writes it back there). */
 int sg_batch_current(const sg_batch* batch);
 /* Cycle-loop iterations (one per cycle of all scenes together) since bind; synchronises. */
 int sg_batch_loops(sg_batch* batch, long long* loops, void* stream);
