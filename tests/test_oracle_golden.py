@@ -183,3 +183,22 @@ def test_gmg_oracle_converges_on_box():
     p2 = np.zeros((H, W))
     cycles2, hist2 = g.solve(p2, b, tol=1e-8, max_cycles=30, precision="mixed")
     assert hist2[-1] <= 1e-8 and cycles2 <= 15
+
+
+def test_gmg_oracle_default_over_relaxation():
+    """The default red-black over-relaxation (1.3) takes fewer V(2,2) cycles to 1e-10 on an
+    open box than 1.2 or 1.4 (128^2: 6 against 7 and 8)."""
+    H = W = 128
+    fmu, fmv = O.face_masks_from_solid(np.zeros((H, W), bool))
+    fl = O.is_fluid_from_faces(fmu, fmv)
+    rng = np.random.default_rng(1)
+    b = rng.standard_normal((H, W)) * fl
+    b[fl] -= b[fl].mean()
+    cycles = {}
+    for omega in (1.2, 1.3, 1.4):
+        g = O.GMGOracle(fmu, fmv, fl, omega=omega)
+        p = np.zeros((H, W))
+        cycles[omega], hist = g.solve(p, b, tol=1e-10, max_cycles=40)
+        assert hist[-1] <= 1e-10
+    assert O.GMGOracle(fmu, fmv, fl).omega == 1.3
+    assert cycles[1.3] <= 6 and cycles[1.3] < cycles[1.2] and cycles[1.3] < cycles[1.4]
