@@ -1,0 +1,27 @@
+"""The benchmark's reference arm runs on the host cores alone (the CPU oracle of the path):
+its JSON line must carry the contract's keys, on the same metric, unit and workload as the
+CUDA arm."""
+import json
+import os
+import subprocess
+import sys
+
+from conftest import ROOT
+
+
+def test_reference_arm_prints_one_contract_line():
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "1"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "cell-steps/s" and d["value"] > 0
+    assert d["metric"].startswith("cell-steps/s at 2048")
+    assert d["config"]["workload"] == "mixed_2048" and d["config"]["grid"] == [2048, 2048]
+    assert d["higher_is_better"] is True and d["steps"] == 1 and d["warmup"] == 1
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"] and cb["value"] == d["value"]
+    e2e = d["e2e"]
+    assert e2e["value"] == d["value"] and e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
