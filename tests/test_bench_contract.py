@@ -1,6 +1,6 @@
 """The benchmark's reference arm runs on the host cores alone (the CPU oracle of the path):
 its JSON line must carry the contract's keys, on the same metric, unit and workload as the
-CUDA arm."""
+CUDA arm (the 2048^2 step, or a bounded sample of the batch of 256 scenes)."""
 import json
 import os
 import subprocess
@@ -25,3 +25,17 @@ def test_reference_arm_prints_one_contract_line():
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"] and cb["value"] == d["value"]
     e2e = d["e2e"]
     assert e2e["value"] == d["value"] and e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+
+
+def test_batch_reference_arm_uses_the_batch_metric():
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
+                          "batch_256", "--steps", "1", "--warmup", "1"], cwd=ROOT, env=env, capture_output=True,
+                         text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["workload"] == "batch_256" and d["value"] > 0
+    assert d["metric"].startswith("cell-steps/s, 256 batched scenes") and d["config"]["workload"] == "batch_256"
+    assert d["cpu_baseline"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
