@@ -108,6 +108,15 @@ def _dist():
     return world, rank, local
 
 
+def mixed_config(mean_cycles, converged, parallelism):
+    """The `config` object of the mixed_2048 line, the same keys in both arms."""
+    return {"workload": "mixed_2048", "grid": [2048, 2048], "sources": 4,
+            "solver": f"multigrid V(2,2) RBGS w={OMEGA}, full weighting, bilinear, {COARSEST}x{COARSEST} exact "
+                      f"coarsest (cosine transform); FP32 cycles in FP64 iterative refinement",
+            "tol": TOL, "mean_cycles_per_step": mean_cycles, "converged": bool(converged),
+            "l2": "working set > 126 MB L2; no flush", "parallelism": parallelism}
+
+
 # ----------------------------------------------------------------------------- reference arm
 def cpu_oracle_steps(n_steps, warmup, fields=None):
     """Time the CPU oracle on the same scene: returns (seconds per step list, cycles, threads).
@@ -148,15 +157,27 @@ def cpu_oracle_steps(n_steps, warmup, fields=None):
     return times, cycles[warmup:], threads
 
 
-def cpu_oracle_batch(scenes, steps):
-    """The CPU oracle on a sample of the batch: each scene stepped `steps` times (after one
-    warm-up step) with the oracle's multigrid in mixed precision to 1e-6."""
+def batch_sample(scenes, per_size=1):
+    """A sample of the batch stratified by grid size: the first `per_size` scenes of each size."""
+    picked, seen = [], {}
+    for sc in scenes:
+        if seen.get(sc.W, 0) < per_size:
+            picked.append(sc)
+            seen[sc.W] = seen.get(sc.W, 0) + 1
+    return picked
+
+
+def cpu_oracle_batch(scenes, sample, steps, warmup=1):
+    """The CPU oracle on a size-stratified `sample` of the batch `scenes`: each sampled scene
+    is stepped `warmup` untimed then `steps` timed substeps with the oracle's multigrid in mixed
+    precision to 1e-6. The time per cell-step measured for each grid size is weighted by that
+    size's share of the whole batch's cells, so the figure estimates the whole batch's rate."""
     import numpy as np
 
     import oracle as O
 
-    total_cells, total_s = 0, 0.0
-    for sc in scenes:
+    per_size = {}
+    for sc in sample:
         fmu, fmv = O.face_masks_from_solid(np.zeros((sc.H, sc.W), bool))
         fl = O.is_fluid_from_faces(fmu, fmv)
         gmg = O.GMGOracle(fmu, fmv, fl, coarsest=8, omega=OMEGA)
@@ -170,16 +191,26 @@ def cpu_oracle_batch(scenes, steps):
         sim = O.OracleSim(sc.H, sc.W, sc.cell_size, solver, {}, dtype=np.float32)
         sim.dt, sim.gravity = sc.dt, sc.gravity
         sim.plumes = [O.PlumeSpec(*row, seed=sc.seed) for row in sc.plumes]
-        sim.substep(sc.dt)
+        for _ in range(warmup):
+            sim.substep(sc.dt)
         t0 = time.perf_counter()
         for _ in range(steps):
             sim.substep(sc.dt)
-        total_s += time.perf_counter() - t0
-        total_cells += sc.H * sc.W * steps
+        dt_s = time.perf_counter() - t0
+        acc = per_size.setdefault(sc.W, [0.0, 0])
+        acc[0] += dt_s
+        acc[1] += sc.H * sc.W * steps
+    batch_cells = {}
+    for sc in scenes:
+        batch_cells[sc.W] = batch_cells.get(sc.W, 0) + sc.H * sc.W
+    est_s = sum(batch_cells[w] * per_size[w][0] / per_size[w][1] for w in batch_cells)
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": total_cells / total_s, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{len(scenes)} of the batch's scenes x {steps} substeps each on the CPU oracle (C/OpenMP "
-                      f"restatement of the reference kernels + the same multigrid to 1e-6), after 1 warm-up step"}
+    sizes = sorted(per_size)
+    return {"value": sum(batch_cells.values()) / est_s, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(sample)} scenes of the batch (the first of each size {sizes}) x {steps} substeps each "
+                      f"on the CPU oracle (C/OpenMP restatement of the reference kernels + the same multigrid to "
+                      f"1e-6), after {warmup} warm-up substep(s); time per cell-step per size weighted by that "
+                      f"size's share of the batch's {sum(batch_cells.values())} cells"}
 
 
 def run_reference(args):
@@ -196,10 +227,8 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
         "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 state, f64/f32 mixed solve", "data": "synthetic",
-        "config": {"workload": "mixed_2048", "grid": [2048, 2048],
-                   "solver": f"multigrid V(2,2) RBGS w={OMEGA}, full weighting, bilinear, {COARSEST}x{COARSEST} exact "
-                             f"coarsest; FP32 cycles in FP64 iterative refinement",
-                   "tol": TOL, "mean_cycles": sum(cycles) / max(len(cycles), 1)},
+        "config": mixed_config(sum(cycles) / max(len(cycles), 1), len(cycles) == len(times),
+                               f"replicas x{args.gpus} (host cores of rank 0)"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{len(times)} substeps of mixed_2048 on the CPU oracle (C/OpenMP restatement of "
                                    f"the reference kernels + the same multigrid), after {args.warmup} warm-up"},
@@ -210,21 +239,22 @@ def run_reference(args):
 
 
 def run_reference_batch(args):
-    """The batch workload's reference arm: the CPU oracle steps a bounded sample of the batch
-    (its first 8 scenes, each stepped `steps` times after one warm-up step) on the host cores."""
+    """The batch workload's reference arm: the CPU oracle steps a size-stratified sample of the
+    batch (one scene of each grid size, `warmup` untimed and `steps` timed substeps each) on the
+    host cores, and the per-size rates are weighted by the batch's size mix."""
     sg = importlib.import_module("python-game-engine_b200")
-    scenes = sg.scenes.batch_256(256, steps=args.steps)[:8]
+    scenes = sg.scenes.batch_256(256, steps=args.steps)
     steps = max(1, args.steps)
-    cpu = cpu_oracle_batch(scenes, steps)
-    sample_cells = sum(sc.H * sc.W for sc in scenes)
+    cpu = cpu_oracle_batch(scenes, batch_sample(scenes), steps, warmup=max(0, args.warmup))
+    total_cells = sum(sc.H * sc.W for sc in scenes)
     value = cpu["value"]
     line = {
         "impl": "reference", "metric": BATCH_METRIC, "workload": "batch_256", "value": value, "unit": UNIT,
-        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * sample_cells / value,
+        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_cells / value,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32 state, f64/f32 mixed solve",
         "data": "synthetic",
-        "config": {"workload": "batch_256", "scenes": len(scenes), "cells": sample_cells, "tol": 1e-6,
-                   "sample": "the batch's first 8 scenes"},
+        "config": {"workload": "batch_256", "scenes": len(scenes), "cells": total_cells, "tol": 1e-6,
+                   "sample": cpu["sample"]},
         "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -522,12 +552,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 state + f64/f32 mixed solve", "data": "synthetic",
-        "config": {"workload": "mixed_2048", "grid": [2048, 2048], "sources": 4, "solver":
-                   f"multigrid V(2,2) RBGS w={OMEGA}, full weighting, bilinear, 32x32 exact coarsest (cosine transform); "
-                   "FP32 cycles in FP64 "
-                   "iterative refinement", "tol": TOL, "mean_cycles_per_step": info["cycles"] / max(info["solves"], 1),
-                   "converged": bool(relres_ok), "l2": "working set > 126 MB L2; no flush",
-                   "parallelism": f"replicas x{world}"},
+        "config": mixed_config(info["cycles"] / max(info["solves"], 1), bool(relres_ok), f"replicas x{world}"),
         "fp64_gpu": {"value": value64, "ms_per_step": ms64 / args.steps,
                      "mean_cycles_per_step": info64["cycles"] / max(info64["solves"], 1), "converged": bool(fp64_ok),
                      "mixed_speedup": value / value64},
@@ -622,7 +647,7 @@ def run_batch(args):
     peak, peak_kind = _peaks()
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_oracle_batch(scenes[:8], 2)
+        cpu = cpu_oracle_batch(scenes, batch_sample(scenes), 2)
     # algorithmic bytes per cell and step outside the solver (float32): forces 12, advect u/v
     # 12 + 12, advect density + dissipation 16, divergence 12, projection 20, metrics
     # divergence 12 + residual 12 = 108 B; per cycle the solver moves >= the fine level's

@@ -188,7 +188,9 @@ int sg_jacobi_solve(int dtype, int64_t H, int64_t W, void* p, int64_t ld_p, cons
  * must not exceed it (1024 x 1024 float32, 724 x 724 float64); larger grids return
  * SG_ERR_CAPACITY. The first call on each device looks the array's address up
  * (cudaGetSymbolAddress) with that device current; make that first call before any
- * stream capture. All calls share the one array: calls that overlap on the GPU (other
+ * stream capture. The address is kept for the life of the process: after a
+ * cudaDeviceReset on a device, do not call this entry point on that device again until
+ * the library has been unloaded and loaded again. All calls share the one array: calls that overlap on the GPU (other
  * streams, other host threads) race and must be serialised by the caller. Nothing in
  * the array needs clearing: the first sweep writes every cell before it is read.
  * Allocates nothing and calls no allocating routine. */
@@ -203,6 +205,64 @@ int sg_jacobi_solve_noalloc(int dtype, int64_t H, int64_t W, void* p, int64_t ld
 int sg_rbsor_solve(int dtype, int64_t H, int64_t W, void* p, int64_t ld_p, const void* div, int64_t ld_div,
                    int mask_mode, const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv, int64_t ld_fmv,
                    double alpha, double reciprocal_beta, double omega, int iterations, void* stream);
+
+/* Red-black SOR on a checkerboard-split layout (red_black_sor_gauss_seidel.py:8-42; the
+ * tolerance loop has no reference counterpart: the reference runs a fixed sweep count).
+ * Cell (j, i) of colour c = (i + j) & 1 lives in plane c at row j, column i >> 1, so each
+ * colour streams contiguously. The iterates equal sg_rbsor_solve's bit for bit.
+ * Workspace (256-byte aligned, sg_rbsor_split_workspace_bytes): two state buffers of two
+ * planes each, the two divergence planes and the residual partial sums.
+ *   pack:   which = 0 copies the pressure into the state, 1 the divergence
+ *   sweeps: `iterations` sweeps (colour 0 then 1) on the state; variant 0 launches one
+ *           streaming kernel per half sweep, variant 1 sweeps 32 x 64 tiles staged in shared
+ *           memory up to 4 sweeps per launch (same iterates), -1 picks the tiles while
+ *           2 * H * W * sizeof(dtype) <= 8 MiB (L2-resident, launch-bound) and the
+ *           streaming launches above (bandwidth-bound)
+ *   sumsq:  *out (device) = sum over fluid cells of the squared reference residual
+ *           (residual.py:39-40) of the state, or of p = 0 when zero_p is set
+ *   unpack: the state back to a natural-layout field
+ *   tol_solve: pack, then sweeps in chunks of check_every until ||r(p)|| <= tol ||r(0)||
+ *           (fluid cells) or max_iterations, then unpack into p; synchronises the stream
+ *           after every chunk to read the residual. Returns SG_ERR_NOT_CONVERGED (p still
+ *           written, *out_iterations / *out_relres set) when the tolerance is not reached. */
+int64_t sg_rbsor_split_workspace_bytes(int dtype, int64_t H, int64_t W);
+int sg_rbsor_split_pack(int dtype, int64_t H, int64_t W, const void* src, int64_t ld_src, int which,
+                        void* workspace, int64_t workspace_bytes, void* stream);
+int sg_rbsor_split_unpack(int dtype, int64_t H, int64_t W, const void* workspace, int64_t workspace_bytes,
+                          void* dst, int64_t ld_dst, void* stream);
+int sg_rbsor_split_sweeps(int dtype, int64_t H, int64_t W, void* workspace, int64_t workspace_bytes,
+                          int mask_mode, const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv,
+                          int64_t ld_fmv, double alpha, double reciprocal_beta, double omega,
+                          int64_t iterations, int variant, void* stream);
+int sg_rbsor_split_sumsq(int dtype, int64_t H, int64_t W, void* workspace, int64_t workspace_bytes,
+                         int mask_mode, const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv,
+                         int64_t ld_fmv, double alpha, double reciprocal_beta, int zero_p, double* out,
+                         void* stream);
+int sg_rbsor_tol_solve(int dtype, int64_t H, int64_t W, void* p, int64_t ld_p, const void* div,
+                       int64_t ld_div, int mask_mode, const uint8_t* fmu, int64_t ld_fmu,
+                       const uint8_t* fmv, int64_t ld_fmv, double alpha, double reciprocal_beta,
+                       double omega, double tol, int64_t max_iterations, int64_t check_every,
+                       int variant, void* workspace, int64_t workspace_bytes, int64_t* out_iterations,
+                       double* out_relres, void* stream);
+
+/* Mixed-precision red-black SOR (no reference counterpart): float64 iterative refinement
+ * around the split-layout float32 sweeps, for a float32 pressure and divergence that must
+ * reach a residual below float32's floor (~1e-4 relative on a 512^2 plume). The pressure is
+ * accumulated in float64; each refinement forms the float64 reference residual
+ * (residual.py:39-40) and solves A e = float32(r) from e = 0 with float32 sweeps
+ * (red_black_sor_gauss_seidel.py:8-27 with alpha = 1) in chunks of check_every, to
+ * max(1e-3, tol / (2 relres)) (at most 0.5) or until three chunks in a row gain < 1 %;
+ * then p += e. Stops at ||r(p)|| <= tol ||r(0)|| (fluid cells) or max_iterations sweeps.
+ * variant as for sg_rbsor_split_sweeps. Workspace: sg_rbsor_mixed_workspace_bytes
+ * (256-byte aligned). Synchronises the stream after every chunk. SG_ERR_NOT_CONVERGED when
+ * the tolerance is not reached (p written). */
+int64_t sg_rbsor_mixed_workspace_bytes(int64_t H, int64_t W);
+int sg_rbsor_mixed_solve(int64_t H, int64_t W, void* p, int64_t ld_p, const void* div, int64_t ld_div,
+                         int mask_mode, const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv,
+                         int64_t ld_fmv, double alpha, double reciprocal_beta, double omega, double tol,
+                         int64_t max_iterations, int64_t check_every, int variant, void* workspace,
+                         int64_t workspace_bytes, int64_t* out_iterations, double* out_relres,
+                         int64_t* out_refinements, void* stream);
 
 /* backends/numba/solvers/gauss_seidel.py:8-48 (lexicographic order), run as an
  * anti-diagonal wavefront in one thread block; intended for small grids. */

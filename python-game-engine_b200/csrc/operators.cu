@@ -424,7 +424,8 @@ static int check_mask_mode(int mode, const void* a, const void* b) {
 
 // Ping-pong buffer of sg_jacobi_solve_noalloc: a fixed array in device memory, so the
 // entry point allocates nothing. Host code cannot use the name as a device address;
-// its address is looked up once per device with that device current.
+// its address is looked up once per device with that device current and kept for the
+// life of the process (a cudaDeviceReset invalidates it until the library is reloaded).
 static __device__ __align__(256) unsigned char g_jacobi_noalloc_scratch[SG_JACOBI_NOALLOC_MAX_BYTES];
 
 static std::mutex g_noalloc_mu;

@@ -1,7 +1,8 @@
 """Generate golden fixtures by running the reference's own Numba kernels.
 
 Run in a container that holds the reference source (it is not needed anywhere
-else):  python tests/golden/make_golden.py [path/to/reference/src]
+else):  python tests/golden/make_golden.py path/to/reference/src
+(or with REFERENCE_SRC set to that path)
 
 The reference (LCEBurton/python-game-engine, src/cfd) is imported read-only; numba's
 on-disk cache is redirected to tests/golden/_numba_cache (git-ignored) because the
@@ -15,7 +16,9 @@ import os
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
+REF_SRC = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REFERENCE_SRC")
+if not REF_SRC:
+    sys.exit("usage: python tests/golden/make_golden.py path/to/reference/src (or set REFERENCE_SRC)")
 os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(HERE, "_numba_cache"))
 sys.path.insert(0, REF_SRC)
 

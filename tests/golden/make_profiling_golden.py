@@ -1,7 +1,8 @@
 """Generate the profiling / cfd-bench golden fixtures with the reference's own code.
 
 Run in a container that holds the reference source (it is not needed anywhere else):
-    python tests/golden/make_profiling_golden.py [path/to/reference/src]
+    python tests/golden/make_profiling_golden.py path/to/reference/src
+(or with REFERENCE_SRC set to that path)
 
 Outputs (consumed by tests/test_profiling.py):
   * profiling_metrics.npz: seeded float32 / float64 fields and, for each, the values the
@@ -18,7 +19,9 @@ import os
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
+REF_SRC = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REFERENCE_SRC")
+if not REF_SRC:
+    sys.exit("usage: python tests/golden/make_profiling_golden.py path/to/reference/src (or set REFERENCE_SRC)")
 os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(HERE, "_numba_cache"))
 sys.path.insert(0, REF_SRC)
 

@@ -74,13 +74,22 @@ def test_noalloc_rejects_grids_above_its_capacity():
     lib = L.load()
     n = 1024
     p = torch.zeros((n, n), dtype=torch.float64, device="cuda")  # 8 MiB > 4 MiB of float64 scratch
-    rc = lib.sg_jacobi_solve_noalloc(L.SG_F64, n, n, p.data_ptr(), n, p.data_ptr(), n, L.SG_MASK_OPEN, None, 0, None, 0,
-                                     -1.0, 0.25, 3, L.stream_ptr())
+    div = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    rc = lib.sg_jacobi_solve_noalloc(L.SG_F64, n, n, p.data_ptr(), n, div.data_ptr(), n, L.SG_MASK_OPEN, None, 0, None,
+                                     0, -1.0, 0.25, 3, L.stream_ptr())
     assert rc == L.SG_ERR_CAPACITY
     assert b"static" in lib.sg_last_error()
-    # the largest float32 grid that fits is accepted
-    q = torch.zeros((n, n), dtype=torch.float32, device="cuda")
-    rc = lib.sg_jacobi_solve_noalloc(L.SG_F32, n, n, q.data_ptr(), n, q.data_ptr(), n, L.SG_MASK_OPEN, None, 0, None, 0,
-                                     -1.0, 0.25, 3, L.stream_ptr())
+    # the largest float32 grid that fits is accepted, and its result equals the allocating entry's
+    rng = np.random.default_rng(7)
+    q0 = torch.from_numpy(rng.uniform(-1, 1, (n, n)).astype(np.float32)).cuda()
+    qdiv = torch.from_numpy(rng.uniform(-1, 1, (n, n)).astype(np.float32)).cuda()
+    got, expected = q0.clone(), q0.clone()
+    scratch = torch.empty((n, n), dtype=torch.float32, device="cuda")
+    rc = lib.sg_jacobi_solve_noalloc(L.SG_F32, n, n, got.data_ptr(), n, qdiv.data_ptr(), n, L.SG_MASK_OPEN, None, 0,
+                                     None, 0, -1.0, 0.25, 3, L.stream_ptr())
+    assert rc == L.SG_OK, lib.sg_last_error()
+    rc = lib.sg_jacobi_solve(L.SG_F32, n, n, expected.data_ptr(), n, qdiv.data_ptr(), n, L.SG_MASK_OPEN, None, 0, None,
+                             0, -1.0, 0.25, 3, scratch.data_ptr(), L.stream_ptr())
     assert rc == L.SG_OK, lib.sg_last_error()
     torch.cuda.synchronize()
+    assert torch.equal(got, expected)
