@@ -273,6 +273,95 @@ def gauss_seidel_pressure_solver(p, div, fmu, fmv, fluid_density, cell_size, dt,
                                      _ptr(_mask(fmv)), H, W, alpha, reciprocal_beta(), iterations)
 
 
+def rb_sor_tolerance(p, div, fmu, fmv, fluid_density, cell_size, dt, omega=1.9, tol=1e-6, max_iterations=200000,
+                     check_every=100):
+    """The CUDA SORToleranceSolver's loop (no reference counterpart; the reference runs a
+    fixed sweep count): red_black_sor_gauss_seidel.py:8-27 sweeps in chunks of `check_every`
+    until ||r(p)|| <= tol ||r(0)|| over fluid cells, r the reference residual
+    (residual.py:39-40) rounded to the field's dtype, squares summed in float64.
+    Returns (sweeps, relative residual)."""
+    alpha = alpha_coeff(cell_size, fluid_density, dt)
+    fl = is_fluid_from_faces(fmu, fmv)
+    out = np.empty_like(p)
+
+    def norm(q):
+        compute_residual(q, div, fl, fmu, fmv, alpha, reciprocal_beta(), out)
+        return float(np.sqrt(np.sum(out.astype(np.float64) ** 2)))
+
+    r0 = norm(np.zeros_like(p))
+    rel = norm(p) / r0 if r0 > 0 else 0.0
+    it = 0
+    while rel > tol and it < max_iterations:
+        n = min(check_every, max_iterations - it)
+        _fn("or_rbsor", p.dtype)(_ptr(p), _ptr(div), _ptr(_mask(fl)), _ptr(_mask(fmu)), _ptr(_mask(fmv)),
+                                  p.shape[0], p.shape[1], alpha, reciprocal_beta(), omega, n)
+        it += n
+        rel = norm(p) / r0 if r0 > 0 else 0.0
+    return it, rel
+
+
+def rb_sor_mixed(p, div, fmu, fmv, fluid_density, cell_size, dt, omega=1.9, tol=1e-6, max_iterations=200000,
+                 check_every=100):
+    """The CUDA mixed-precision SOR (no reference counterpart): float64 iterative refinement
+    around float32 red-black SOR sweeps (red_black_sor_gauss_seidel.py:8-27). The pressure
+    is accumulated in float64; each refinement forms the float64 reference residual r
+    (residual.py:39-40) and solves A e = float32(r) from e = 0 with float32 sweeps (alpha = 1)
+    in chunks of `check_every`, until the correction's relative residual reaches
+    max(1e-3, tol / (2 ||r|| / ||r0||)) (at most 0.5) or three chunks in a row gain less than
+    1 %; then p += e. Stops when ||r(p)|| <= tol ||r(0)||. `p` and `div` are float32.
+    Returns (sweeps, relative residual, refinements)."""
+    alpha = alpha_coeff(cell_size, fluid_density, dt)
+    fl = is_fluid_from_faces(fmu, fmv)
+    H, W = p.shape
+    p64 = p.astype(np.float64)
+    d64 = div.astype(np.float64)
+    out64 = np.empty_like(p64)
+    out32 = np.empty((H, W), np.float32)
+
+    def res64(q):
+        return compute_residual(q, d64, fl, fmu, fmv, alpha, reciprocal_beta(), out64)
+
+    r0 = float(np.sqrt(np.sum(res64(np.zeros_like(p64)) ** 2)))
+    it = outer = 0
+    while True:
+        r = res64(p64)
+        rel = float(np.sqrt(np.sum(r ** 2))) / r0 if r0 > 0 else 0.0
+        if not np.isfinite(rel) or rel <= tol or it >= max_iterations:
+            break
+        inner_tol = min(0.5, max(1e-3, 0.5 * tol / rel))
+        r32 = r.astype(np.float32)
+        e = np.zeros((H, W), np.float32)
+
+        def inorm(q):
+            compute_residual(q, r32, fl, fmu, fmv, 1.0, reciprocal_beta(), out32)
+            return float(np.sqrt(np.sum(out32.astype(np.float64) ** 2)))
+
+        ir0 = inorm(np.zeros_like(e))
+        irel = best = 1.0
+        stalls = 0
+        while irel > inner_tol and it < max_iterations:
+            n = min(check_every, max_iterations - it)
+            _fn("or_rbsor", np.float32)(_ptr(e), _ptr(r32), _ptr(_mask(fl)), _ptr(_mask(fmu)), _ptr(_mask(fmv)),
+                                         H, W, 1.0, reciprocal_beta(), omega, n)
+            it += n
+            irel = inorm(e) / ir0 if ir0 > 0 else 0.0
+            if not np.isfinite(irel):
+                break
+            if irel < 0.99 * best:
+                best, stalls = irel, 0
+            else:
+                stalls += 1
+                if stalls >= 3:
+                    break
+        p64 += e.astype(np.float64)
+        outer += 1
+        if not np.isfinite(irel):
+            rel = irel
+            break
+    p[:] = p64.astype(np.float32)
+    return it, rel, outer
+
+
 SMOOTHERS = {
     "jacobi": jacobi_pressure_solver,
     "rb_sor_gauss_seidel": rb_sor_pressure_solver,

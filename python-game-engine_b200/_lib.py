@@ -47,6 +47,16 @@ SIGNATURES = {
     "sg_jacobi_solve_noalloc": [I, I64, I64, P, I64, P, I64, I, P, I64, P, I64, D, D, I, P],
     "sg_rbsor_solve": [I, I64, I64, P, I64, P, I64, I, P, I64, P, I64, D, D, D, I, P],
     "sg_gauss_seidel_solve": [I, I64, I64, P, I64, P, I64, I, P, I64, P, I64, D, D, I, P],
+    "sg_rbsor_split_workspace_bytes": [I, I64, I64],
+    "sg_rbsor_split_pack": [I, I64, I64, P, I64, I, P, I64, P],
+    "sg_rbsor_split_unpack": [I, I64, I64, P, I64, P, I64, P],
+    "sg_rbsor_split_sweeps": [I, I64, I64, P, I64, I, P, I64, P, I64, D, D, D, I64, I, P],
+    "sg_rbsor_split_sumsq": [I, I64, I64, P, I64, I, P, I64, P, I64, D, D, I, P, P],
+    "sg_rbsor_tol_solve": [I, I64, I64, P, I64, P, I64, I, P, I64, P, I64, D, D, D, D, I64, I64, I, P, I64,
+                           ctypes.POINTER(ctypes.c_int64), PD, P],
+    "sg_rbsor_mixed_workspace_bytes": [I64, I64],
+    "sg_rbsor_mixed_solve": [I64, I64, P, I64, P, I64, I, P, I64, P, I64, D, D, D, D, I64, I64, I, P, I64,
+                             ctypes.POINTER(ctypes.c_int64), PD, ctypes.POINTER(ctypes.c_int64), P],
     "sg_mg_restrict_average": [I, I64, I64, P, I64, I, P, I64, P, I64, I64, I64, D, P],
     "sg_mg_prolong": [I, I64, I64, P, I64, I64, I64, I, P, I64, P, I64, I, P],
     "sg_mg_coarsen_solid": [I64, I64, P, I64, P, I64, P],
@@ -113,6 +123,8 @@ _RESTYPE = {
     "sg_batch_workspace_bytes": ctypes.c_int64,
     "sg_batch_snapshot_bytes": ctypes.c_int64,
     "sg_field_stats_workspace_bytes": ctypes.c_int64,
+    "sg_rbsor_split_workspace_bytes": ctypes.c_int64,
+    "sg_rbsor_mixed_workspace_bytes": ctypes.c_int64,
 }
 
 _lib = None

@@ -25,7 +25,7 @@ LIB = os.path.join(LIBDIR, "libsmoke_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
           "--expt-relaxed-constexpr", "-I" + INCLUDE, "-I" + CSRC]
-PER_FILE = {"operators.cu": ["-fmad=false"], "batch.cu": ["-fmad=false"]}
+PER_FILE = {"operators.cu": ["-fmad=false"], "batch.cu": ["-fmad=false"], "rbsor_split.cu": ["-fmad=false"]}
 
 
 def _nvcc():

@@ -69,17 +69,21 @@ class MultigridParams:
 
 @dataclass
 class SORToleranceParams:
-    """Red-black SOR run until ||r|| / ||r(0)|| <= tol (checked every check_every sweeps)."""
+    """Red-black SOR run until ||r|| / ||r(0)|| <= tol (checked every check_every sweeps).
+    precision: "native" (the field's dtype) or "mixed" (float32 sweeps in float64 refinement)."""
     omega: float = 1.9
     tol: float = 1e-6
     max_iterations: int = 200000
     check_every: int = 100
+    precision: str = "native"
 
     def string(self):
-        return f"SORToleranceParams_omega_{self.omega}_tol_{self.tol}"
+        suffix = "" if self.precision == "native" else f"_{self.precision}"
+        return f"SORToleranceParams_omega_{self.omega}_tol_{self.tol}{suffix}"
 
     def to_fn(self):
-        return f"o_{self.omega}_t_{self.tol}"
+        suffix = "" if self.precision == "native" else f"_{self.precision}"
+        return f"o_{self.omega}_t_{self.tol}{suffix}"
 
 
 @dataclass

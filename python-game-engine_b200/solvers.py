@@ -180,43 +180,75 @@ class MultigridSolver:
 
 
 # ---------------------------------------------------------------- new methods
-def _relres(pressure, divergence, fmu, fmv, fl, alpha, out, r0):
-    sq = torch.zeros(1, dtype=torch.float64, device=pressure.device)
-    compute_residual(pressure, divergence, fl, fmu, fmv, alpha, 0.25, out, sumsq=sq)
-    return math.sqrt(float(sq.item())) / r0 if r0 > 0 else 0.0
-
-
 class SORToleranceSolver:
     """Red-black SOR until ||r(p)|| / ||r(0)|| <= tol over fluid cells, with r the
-    reference residual (residual.py:39-40); checked on the host every check_every
-    sweeps. No reference counterpart (the reference runs a fixed sweep count)."""
+    reference residual (residual.py:39-40), on the checkerboard-split layout: red and
+    black cells in separate contiguous planes, the residual norm checked every
+    ``check_every`` sweeps. The iterates are the reference kernel's
+    (red_black_sor_gauss_seidel.py:8-27) bit for bit; the tolerance loop has no reference
+    counterpart (the reference runs a fixed sweep count). ``variant``: 1 sweeps
+    shared-memory tiles up to four sweeps per launch, 0 launches one streaming kernel per
+    half sweep, -1 (default) picks the tiles for grids that sit in L2 and the streaming
+    kernel above.
+
+    ``precision="mixed"`` (float32 fields): float64 iterative refinement around float32
+    sweeps (``sg_rbsor_mixed_solve``), which reaches tolerances below float32's residual
+    floor; ``last_refinements`` counts the refinements."""
 
     def __init__(self):
         self.last_iterations = 0
         self.last_relres = None
+        self.last_refinements = 0
         self.converged = None
+        self._ws = None
+
+    def workspace(self, nbytes, device):
+        if self._ws is None or self._ws.numel() < nbytes + 256 or self._ws.device != torch.device(device):
+            self._ws = torch.empty(nbytes + 256, dtype=torch.uint8, device=device)
+        base = self._ws.data_ptr()
+        off = (-base) % 256
+        return ctypes.c_void_p(base + off), self._ws.numel() - off
 
     def __call__(self, pressure, divergence, face_mask_u, face_mask_v, fluid_density, cell_size, dt, omega=1.9,
-                 tol=1e-6, max_iterations=200000, check_every=100, strict=False, **_ignored):
+                 tol=1e-6, max_iterations=200000, check_every=100, strict=False, variant=-1, precision="native",
+                 **_ignored):
         H, W = pressure.shape
         alpha = calculate_alpha(cell_size, fluid_density, dt)
-        fl = face_mask_u if isinstance(face_mask_u, AnalyticMask) else is_fluid_from_faces(face_mask_u, face_mask_v)
-        out = torch.empty_like(pressure)
-        zero = torch.zeros_like(pressure)
-        r0 = _relres(zero, divergence, face_mask_u, face_mask_v, fl, alpha, out, 1.0)
-        rel = _relres(pressure, divergence, face_mask_u, face_mask_v, fl, alpha, out, r0)
-        it = 0
-        while rel > tol and it < max_iterations:
-            n = min(check_every, max_iterations - it)
-            red_black_sor_gauss_seidel_pressure_solver(pressure, divergence, face_mask_u, face_mask_v, fluid_density,
-                                                       cell_size, dt, n, omega=omega)
-            it += n
-            rel = _relres(pressure, divergence, face_mask_u, face_mask_v, fl, alpha, out, r0)
-            if not math.isfinite(rel):
-                raise L.SmokeCudaError(f"non-finite residual after {it} SOR sweeps")
-        self.last_iterations, self.last_relres, self.converged = it, rel, rel <= tol
-        if strict and rel > tol:
-            raise L.NotConverged(f"SOR relative residual {rel:.3e} > {tol:.3e} after {it} sweeps", it, rel)
+        mode, pu, lu, pv, lv = _face_pair(face_mask_u, face_mask_v, H, W)
+        p, ldp = L.field(pressure, "pressure")
+        d, ldd = L.field(divergence, "divergence", dtype=pressure.dtype)
+        lib = L.load()
+        its = ctypes.c_int64(0)
+        refs = ctypes.c_int64(0)
+        rel = ctypes.c_double(0.0)
+        if precision == "mixed":
+            if pressure.dtype != torch.float32:
+                raise TypeError("precision='mixed' refines a float32 pressure; a float64 one needs no refinement")
+            ws, nbytes = self.workspace(int(lib.sg_rbsor_mixed_workspace_bytes(H, W)), pressure.device)
+            rc = lib.sg_rbsor_mixed_solve(H, W, p, ldp, d, ldd, mode, pu, lu, pv, lv, alpha,
+                                          calculate_reciprocal_beta(), float(omega), float(tol), int(max_iterations),
+                                          int(check_every), int(variant), ws, nbytes, ctypes.byref(its),
+                                          ctypes.byref(rel), ctypes.byref(refs), L.stream_ptr())
+            name = "sg_rbsor_mixed_solve"
+        elif precision == "native":
+            code = L.dtype_code(pressure)
+            ws, nbytes = self.workspace(int(lib.sg_rbsor_split_workspace_bytes(code, H, W)), pressure.device)
+            rc = lib.sg_rbsor_tol_solve(code, H, W, p, ldp, d, ldd, mode, pu, lu, pv, lv, alpha,
+                                        calculate_reciprocal_beta(), float(omega), float(tol), int(max_iterations),
+                                        int(check_every), int(variant), ws, nbytes, ctypes.byref(its),
+                                        ctypes.byref(rel), L.stream_ptr())
+            name = "sg_rbsor_tol_solve"
+        else:
+            raise ValueError(f"precision must be 'native' or 'mixed', got {precision!r}")
+        self.last_iterations, self.last_relres = int(its.value), float(rel.value)
+        self.last_refinements = int(refs.value)
+        self.converged = rc == L.SG_OK
+        if rc == L.SG_ERR_NOT_CONVERGED:
+            if strict:
+                raise L.NotConverged(f"SOR relative residual {self.last_relres:.3e} > {tol:.3e} after "
+                                     f"{self.last_iterations} sweeps", self.last_iterations, self.last_relres)
+            return
+        L.check(rc, name)
 
 
 _PRECISION = {"fp32": L.SG_GMG_FP32, "fp64": L.SG_GMG_FP64, "mixed": L.SG_GMG_MIXED}

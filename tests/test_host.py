@@ -57,6 +57,23 @@ def test_abi_rejects_bad_arguments_without_a_gpu():
     rc = lib.sg_compute_divergence(L.SG_F64, 4, 4, fake, 5, fake, 4, fake, 4, L.SG_MASK_OPEN, null, 0, null, 0, 0.0,
                                    null)
     assert rc == L.SG_ERR_ARG
+    # split-layout SOR: workspace must be aligned and large enough, dtype known
+    n = lib.sg_rbsor_split_workspace_bytes(L.SG_F32, 64, 64)
+    assert n > 6 * 64 * 32 * 4 and lib.sg_rbsor_split_workspace_bytes(9, 64, 64) == -1
+    rc = lib.sg_rbsor_split_pack(L.SG_F32, 64, 64, fake, 64, 0, ctypes.c_void_p(256 + 16), n, null)
+    assert rc == L.SG_ERR_ARG and b"aligned" in lib.sg_last_error()
+    rc = lib.sg_rbsor_split_sweeps(L.SG_F32, 64, 64, ctypes.c_void_p(256), n - 1, L.SG_MASK_OPEN, null, 0, null, 0,
+                                   1.0, 0.25, 1.9, 3, 1, null)
+    assert rc == L.SG_ERR_ARG and b"workspace" in lib.sg_last_error()
+    rc = lib.sg_rbsor_split_sweeps(L.SG_F64, 64, 64, ctypes.c_void_p(256), 1 << 30, L.SG_MASK_OPEN, null, 0, null, 0,
+                                   1.0, 0.25, 1.9, 3, 2, null)
+    assert rc == L.SG_ERR_ARG and b"variant" in lib.sg_last_error()
+    rc = lib.sg_rbsor_tol_solve(7, 64, 64, fake, 64, fake, 64, L.SG_MASK_OPEN, null, 0, null, 0, 1.0, 0.25, 1.9,
+                                1e-6, 10, 5, 1, ctypes.c_void_p(256), 1 << 30, null, null, null)
+    assert rc == L.SG_ERR_DTYPE
+    rc = lib.sg_rbsor_mixed_solve(64, 64, fake, 64, fake, 64, L.SG_MASK_OPEN, null, 0, null, 0, 1.0, 0.25, 1.9, 1e-6,
+                                  10, 5, -1, ctypes.c_void_p(256), 16, null, null, null, null)
+    assert rc == L.SG_ERR_ARG and b"workspace" in lib.sg_last_error()
     # the Python layer turns codes into exceptions
     with pytest.raises(ValueError):
         L.check(L.SG_ERR_ARG, "x")

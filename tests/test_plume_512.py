@@ -1,0 +1,223 @@
+"""512^2 plume scenes (variant 0: source r=32 at x=0.5; variants 1, 2: seeded inflow x on the
+bottom edge), pressure by red-black SOR omega=1.9 and by multigrid V(2,2) (red-black
+Gauss-Seidel, omega = 1, full weighting, bilinear prolongation, exact 8^2 coarsest level),
+both to a relative residual of 1e-6, float64 and float32 states, against the CPU oracle.
+
+Stated tolerances (relative L2 unless noted; pressure with its mean removed):
+* SOR, float64: the CUDA sweeps and the oracle's are the reference kernel's expression in
+  IEEE order on both sides, so the sweep counts of every tolerance loop are equal and the
+  fields bit-identical.
+* SOR, float32 state: float32 sweeps stall near 1e-4 relative residual on this scene, so
+  the float32 run refines in float64 (precision="mixed"); it equals the oracle's mixed
+  refinement bit for bit (same sweeps, same decisions), and differs from the float64 run by
+  what two solves that each stop at 1e-6 may differ by: <= 1e-3 on pressure, <= 1e-5 on
+  density and velocity after 2 steps.
+* Multigrid, float64: the CUDA solver contracts multiply-adds, the oracle does not, so
+  iterates differ by rounding; cycle counts are equal and fields agree to 1e-9.
+* Multigrid, float32 state (mixed-precision solve): float32 cycles round differently on the
+  two sides; density and velocity agree with the oracle's mixed run to 1e-4 and with the
+  float64 oracle to 1e-3, pressure to 1e-4 / 2e-3.
+* Post-projection divergence: on cells two or more cells from the wall ring it equals
+  r / alpha (r the solve's residual), so its norm there is at most tol * ||divergence before
+  the solve|| plus the rounding of the float32 faces (8 eps32 max|u| / h per cell); asserted
+  on every step of every multigrid run. (The post-projection divergence itself is the
+  difference of nearly cancelling terms, so it is compared through this bound rather than
+  relative to the oracle's.)
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import package
+
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():
+    pytest.skip("CUDA device required", allow_module_level=True)
+
+import oracle as O  # noqa: E402
+
+sg = package()
+scenes = sg.scenes
+TOL = 1e-6
+SOR_CHECK = 200
+_RECORDED = {}
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / nb) if nb > 0 else float(np.linalg.norm(a))
+
+
+def _prel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return _rel(a - a.mean(), b - b.mean())
+
+
+def recording(method):
+    """The CUDA solver `method` registered once more under a test name that first records the
+    norm of the divergence it is handed (the pre-projection divergence)."""
+    name = f"test_recorded_{method}"
+    if name not in _RECORDED:
+        inner = sg.get_solver(method, "cuda")
+        norms = []
+
+        def fn(pressure, divergence, *args, **kw):
+            norms.append(float(divergence.double().norm()))
+            inner(pressure, divergence, *args, **kw)
+
+        sg.register_solver(name, "cuda", fn)
+        _RECORDED[name] = norms
+    return name, _RECORDED[name]
+
+
+def check_divergence_bound(sim, div_before, tol):
+    """||div after projection|| on cells >= 2 from the ring <= tol ||div before|| + rounding."""
+    d = sim.divergence.double()[2:-2, 2:-2]
+    eps = 6e-8 if sim.divergence.dtype == torch.float32 else 1.2e-16
+    vmax = max(float(sim.velocity_u.abs().max()), float(sim.velocity_v.abs().max()))
+    rounding = 8 * eps * vmax / sim.cell_size * np.sqrt(d.numel())
+    got = float(d.norm())
+    assert got <= tol * div_before * 1.001 + rounding, (got, tol * div_before, rounding)
+    return got
+
+
+def _oracle(sc, solver, dtype):
+    s = O.OracleSim(sc.H, sc.W, sc.cell_size, solver, {}, dtype=dtype)
+    s.dt, s.gravity = sc.dt, sc.gravity
+    s.plumes = [O.PlumeSpec(*row, seed=sc.seed) for row in sc.plumes]
+    return s
+
+
+def _fields(sim, numpy_side=False):
+    names = ("density", "velocity_u", "velocity_v", "pressure", "divergence")
+    if numpy_side:
+        return {n: getattr(sim, n).copy() for n in names}
+    return {n: getattr(sim, n).cpu().numpy() for n in names}
+
+
+def _gmg_oracle_solver(sc, precision, record):
+    fmu, fmv = O.face_masks_from_solid(np.zeros((sc.H, sc.W), bool))
+    fl = O.is_fluid_from_faces(fmu, fmv)
+    gmg = O.GMGOracle(fmu, fmv, fl, coarsest=8, omega=1.0)
+
+    def solver(p, div, fmu_, fmv_, rho, h, dt, **_):
+        b = O.alpha_coeff(h, rho, dt) * div.astype(np.float64) * fl
+        p64 = np.zeros(p.shape)
+        c, hist = gmg.solve(p64, b, tol=TOL, max_cycles=60, precision=precision)
+        record.append((c, hist[-1]))
+        p[:] = p64.astype(p.dtype)
+
+    return solver
+
+
+def _gmg_params(precision):
+    return sg.GeometricMultigridParams(tol=TOL, max_cycles=60, omega=1.0, coarsest=8, pre_sweeps=2, post_sweeps=2,
+                                       cycle="V", precision=precision)
+
+
+# ---------------------------------------------------------------- red-black SOR
+def test_sor_fp64_matches_oracle_bit_for_bit():
+    sc = scenes.plume_512(0, steps=2)
+    cu = scenes.make_sim(sc, "rb_sor_tolerance", sg.SORToleranceParams(omega=1.9, tol=TOL, check_every=SOR_CHECK),
+                         dtype=torch.float64)
+    solver = sg.get_solver("rb_sor_tolerance", "cuda")
+    rec = []
+
+    def ora_sor(p, div, fmu, fmv, rho, h, dt, **_):
+        rec.append(O.rb_sor_tolerance(p, div, fmu, fmv, rho, h, dt, omega=1.9, tol=TOL, check_every=SOR_CHECK))
+
+    ora = _oracle(sc, ora_sor, np.float64)
+    for k in range(sc.steps):
+        cu.substep(sc.dt)
+        ora.substep(sc.dt)
+        assert solver.converged and solver.last_relres <= TOL
+        assert solver.last_iterations == rec[k][0], (k, solver.last_iterations, rec[k])
+    g, o = _fields(cu), _fields(ora, True)
+    for n in g:
+        assert np.array_equal(g[n], o[n]), n
+    assert rec[-1][0] > 10000  # the scene needs tens of thousands of sweeps per solve at omega = 1.9
+
+
+def test_sor_fp32_mixed_matches_oracle_and_fp64():
+    sc = scenes.plume_512(0, steps=2)
+    cu = scenes.make_sim(sc, "rb_sor_tolerance",
+                         sg.SORToleranceParams(omega=1.9, tol=TOL, check_every=SOR_CHECK, precision="mixed"),
+                         dtype=torch.float32)
+    solver = sg.get_solver("rb_sor_tolerance", "cuda")
+    rec, rec64 = [], []
+
+    def ora_mixed(p, div, fmu, fmv, rho, h, dt, **_):
+        rec.append(O.rb_sor_mixed(p, div, fmu, fmv, rho, h, dt, omega=1.9, tol=TOL, check_every=SOR_CHECK))
+
+    def ora_fp64(p, div, fmu, fmv, rho, h, dt, **_):
+        rec64.append(O.rb_sor_tolerance(p, div, fmu, fmv, rho, h, dt, omega=1.9, tol=TOL, check_every=SOR_CHECK))
+
+    ora = _oracle(sc, ora_mixed, np.float32)
+    ora64 = _oracle(sc, ora_fp64, np.float64)
+    for k in range(sc.steps):
+        cu.substep(sc.dt)
+        ora.substep(sc.dt)
+        ora64.substep(sc.dt)
+        assert solver.converged and solver.last_relres <= TOL
+        assert (solver.last_iterations, solver.last_refinements) == (rec[k][0], rec[k][2]), (k, rec[k])
+    g, o, o64 = _fields(cu), _fields(ora, True), _fields(ora64, True)
+    for n in g:
+        assert np.array_equal(g[n], o[n]), n
+    assert _prel(g["pressure"], o64["pressure"]) <= 1e-3
+    for n in ("density", "velocity_u", "velocity_v"):
+        assert _rel(g[n], o64[n]) <= 1e-5, n
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_sor_50_steps_every_solve_converges(variant):
+    sc = scenes.plume_512(variant, steps=50)
+    solver = sg.get_solver("rb_sor_tolerance", "cuda")
+    runs = {}
+    for name, dtype, precision in (("fp64", torch.float64, "native"), ("fp32", torch.float32, "mixed")):
+        sim = scenes.make_sim(sc, "rb_sor_tolerance", sg.SORToleranceParams(omega=1.9, tol=TOL, check_every=SOR_CHECK,
+                                                                            precision=precision), dtype=dtype)
+        for _ in range(sc.steps):
+            sim.substep(sc.dt)
+            assert solver.converged and solver.last_relres <= TOL
+        runs[name] = _fields(sim)
+    a, b = runs["fp32"], runs["fp64"]
+    assert np.max(b["density"]) > 0.5
+    assert _rel(a["density"], b["density"]) <= 1e-3
+    assert _rel(a["velocity_v"], b["velocity_v"]) <= 1e-3
+
+
+# ---------------------------------------------------------------- multigrid V(2,2)
+@pytest.mark.parametrize("variant,steps", [(0, 50), (1, 10), (2, 10)])
+def test_multigrid_fp64_and_fp32_vs_oracle(variant, steps):
+    sc = scenes.plume_512(variant, steps=steps)
+    solver = sg.get_solver("geometric_multigrid", "cuda")
+    name_rec, norms = recording("geometric_multigrid")
+    out = {}
+    for name, dtype, npdt, precision in (("fp64", torch.float64, np.float64, "fp64"),
+                                         ("fp32", torch.float32, np.float32, "mixed")):
+        cu = scenes.make_sim(sc, "geometric_multigrid", _gmg_params(precision), dtype=dtype)
+        cu.pressure_solver_method = name_rec
+        rec = []
+        ora = _oracle(sc, _gmg_oracle_solver(sc, precision, rec), npdt)
+        for k in range(sc.steps):
+            norms.clear()
+            cu.substep(sc.dt)
+            ora.substep(sc.dt)
+            assert solver.converged and solver.last_relres <= TOL, (name, k)
+            assert rec[k][1] <= TOL
+            if name == "fp64":
+                assert solver.last_cycles == rec[k][0], (k, solver.last_cycles, rec[k])
+            check_divergence_bound(cu, norms[-1], TOL)
+        out[name] = (_fields(cu), _fields(ora, True))
+    g64, o64 = out["fp64"]
+    g32, o32 = out["fp32"]
+    assert np.max(o64["density"]) > 0.5
+    for n in ("density", "velocity_u", "velocity_v"):
+        assert _rel(g64[n], o64[n]) <= 1e-9, n
+        assert _rel(g32[n], o32[n]) <= 1e-4, n
+        assert _rel(g32[n], o64[n]) <= 1e-3, n
+    assert _prel(g64["pressure"], o64["pressure"]) <= 1e-9
+    assert _prel(g32["pressure"], o32["pressure"]) <= 1e-4
+    assert _prel(g32["pressure"], o64["pressure"]) <= 2e-3
