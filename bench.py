@@ -213,6 +213,109 @@ def cpu_oracle_batch(scenes, sample, steps, warmup=1):
                       f"size's share of the batch's {sum(batch_cells.values())} cells"}
 
 
+def reference_numba(n=2048, steps=2, warmup=2, cycles=5):
+    """The reference's own Numba code on the host cores, as context beside the oracle port
+    (the reference cannot reach the 1e-8 target: its multigrid stalls near 0.1). Imports
+    the reference installed under baseline/_ref (or REFERENCE_SRC). Measures
+    (a) SmokeSimulation2D substeps (float32, the reference's only dtype) at n^2 with its
+        multigrid (Jacobi smoother, log2(n / 8) + 1 levels, 2 V(2,2) cycles), the 4 sources
+        of the scene as the reference's additive emitters, after `warmup` substeps (JIT);
+    (b) float64 calls of its kernels on the scene's first divergence: one multigrid V(2,2)
+        cycle (Jacobi smoother) repeated `cycles` times with the relative residual after each,
+        and one Jacobi sweep."""
+    ref = os.environ.get("REFERENCE_SRC") or os.path.join(ROOT, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(ref, "cfd")):
+        return {"unavailable": "the reference package is not installed under baseline/_ref"}
+    try:
+        import numba
+    except ImportError:
+        return {"unavailable": "numba is not installed"}
+    import numpy as np
+
+    os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(tempfile.gettempdir(), "sg_reference_numba_cache"))
+    if ref not in sys.path:
+        sys.path.insert(0, ref)
+    import cfd.solvers  # noqa: F401  (registries first: the reference's import order)
+    import cfd.operators  # noqa: F401
+    from cfd.backends.numba.operators.divergence import compute_divergence
+    from cfd.backends.numba.operators.residual import compute_residual
+    from cfd.backends.numba.solvers.jacobi import jacobi_pressure_solver
+    from cfd.backends.numba.solvers.multigrid.solver import MultigridSolver
+    from cfd.common.config import GridConfig, PressureSolverConfig, SimulationConfig
+    from cfd.common.emitters import Emitter2D
+    from cfd.common.simulation import SmokeSimulation2D
+    from cfd.profiling import ProfileSession
+    from cfd.solvers.params import MultigridParams
+
+    sg = importlib.import_module("python-game-engine_b200")
+    sc = sg.scenes.mixed_2048(steps=steps + warmup)
+    levels = int(np.log2(n // 8)) + 1
+    mgp = MultigridParams(smoother_type="jacobi", num_levels=levels, v_cycles=2, smoother_iterations=2,
+                          coarsest_iterations=30)
+    cfg = SimulationConfig(grid=GridConfig(size=(n, n), cell_size=1.0 / n),
+                           pressure_solver=PressureSolverConfig(method="multigrid", params=mgp))
+    import contextlib
+
+    with contextlib.redirect_stdout(sys.stderr):  # the reference prints a banner; stdout carries the JSON line
+        sim = SmokeSimulation2D(cfg, profiler=ProfileSession.disabled((n, n)))
+    sim.dt, sim.gravity = 0.5 / n, sc.gravity
+    k = n / sc.W
+    for cx, cy, r, dens, vin, _ in sc.plumes:
+        sim.add_emitter(Emitter2D(position=(cx * k, cy * k), radius=r * k, density_value=dens / sim.dt,
+                                  velocity_value=(0.0, vin / sim.dt), approach="hard_cutoff", numba_optimized=True))
+    t_jit = time.perf_counter()
+    for _ in range(warmup):
+        sim.substep(sim.dt)
+    t_jit = time.perf_counter() - t_jit
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.substep(sim.dt)
+    t_step = (time.perf_counter() - t0) / steps
+    # float64 kernels on the current divergence (recomputed from the state)
+    u = sim.velocity_u.astype(np.float64)
+    v = sim.velocity_v.astype(np.float64)
+    fmu, fmv = sim._face_mask_u, sim._face_mask_v
+    fl = sim.is_fluid
+    div = np.zeros((n, n))
+    compute_divergence(u, v, div, fmu, fmv, sim.cell_size)
+    alpha = -(sim.cell_size ** 2) * sim.fluid_density / sim.dt
+    res = np.zeros((n, n))
+
+    def relres(p):
+        compute_residual(p, div, fl, fmu, fmv, alpha, 0.25, res)
+        return float(np.linalg.norm(res))
+
+    r0 = relres(np.zeros((n, n)))
+    mg = MultigridSolver()
+    p = np.zeros((n, n))
+    mg(p, div, fmu, fmv, sim.fluid_density, sim.cell_size, sim.dt, v_cycles=1, smoother_type="jacobi",
+       smoother_backend="numba", num_levels=levels, smoother_iterations=2, coarsest_iterations=30,
+       profiler=ProfileSession.disabled((n, n)))  # JIT and hierarchy
+    p[:] = 0.0
+    hist, t_cyc = [], 0.0
+    for _ in range(cycles):
+        t0 = time.perf_counter()
+        mg(p, div, fmu, fmv, sim.fluid_density, sim.cell_size, sim.dt, v_cycles=1, smoother_type="jacobi",
+           smoother_backend="numba", num_levels=levels, smoother_iterations=2, coarsest_iterations=30,
+           profiler=ProfileSession.disabled((n, n)))
+        t_cyc += time.perf_counter() - t0
+        hist.append(relres(p) / r0 if r0 > 0 else 0.0)
+    q = np.zeros((n, n))
+    jacobi_pressure_solver(q, div, fmu, fmv, sim.fluid_density, sim.cell_size, sim.dt, iterations=1)
+    t0 = time.perf_counter()
+    jacobi_pressure_solver(q, div, fmu, fmv, sim.fluid_density, sim.cell_size, sim.dt, iterations=10)
+    t_jac = (time.perf_counter() - t0) / 10
+    return {"threads": int(numba.get_num_threads()), "numba": numba.__version__,
+            "substep_fp32": {"ms_per_step": 1e3 * t_step, "cell_steps_per_s": n * n / t_step, "steps": steps,
+                             "solver": f"reference multigrid, {levels} levels, Jacobi smoother, 2 x V(2,2) "
+                                       "(fixed cycles: it has no tolerance loop)",
+                             "warmup_s_with_jit": t_jit},
+            "vcycle_fp64": {"ms_per_cycle": 1e3 * t_cyc / cycles, "relres_after_each_cycle": hist},
+            "jacobi_sweep_fp64_ms": 1e3 * t_jac,
+            "sources": "the scene's 4 sources as additive hard-cutoff emitters (the reference has no overwriting "
+                       "source)"}
+
+
 def run_reference(args):
     world, rank, _ = _dist()
     if rank != 0:
@@ -234,6 +337,11 @@ def run_reference(args):
                                    f"the reference kernels + the same multigrid), after {args.warmup} warm-up"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_reference_numba:
+        try:
+            line["reference_numba"] = reference_numba()
+        except Exception as e:  # context only: the timed arm above stands on its own
+            line["reference_numba"] = {"unavailable": f"{type(e).__name__}: {e}"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -360,11 +468,15 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def make(dtype, precision, tol=TOL, remove_mean=False):
+    def make(dtype, precision, tol=TOL, remove_mean=False, inner=1):
         params = sg.GeometricMultigridParams(tol=tol, max_cycles=40, precision=precision, omega=OMEGA,
                                              coarsest=COARSEST, fixed_cycles=args.fixed_cycles,
-                                             remove_mean=remove_mean)
-        return sg.scenes.make_sim(sc, "geometric_multigrid", params, dtype=dtype, device=dev)
+                                             remove_mean=remove_mean, inner_cycles=inner)
+        sim = sg.scenes.make_sim(sc, "geometric_multigrid", params, dtype=dtype, device=dev)
+        # float32 states advect in the arithmetic chosen for the run; float64 states in the
+        # reference's float64 arithmetic
+        sim.advection_arithmetic = args.advection if dtype == torch.float32 else "reference"
+        return sim
 
     solver = sg.get_solver("geometric_multigrid", "cuda")
 
@@ -533,6 +645,23 @@ def run_ours(args):
                        "converged": bool(info_t["failures"] == 0 and info_t["solves"] == k_tight)}
         del st
     tight["mixed_speedup"] = tight["mixed"]["value"] / tight["fp64"]["value"]
+    # ---- classical iterative refinement: k FP32 cycles on the correction between two FP64
+    # passes (p += e, residual), against the headline's per-cycle correction in the fused fine
+    # kernel (k = 1); same scene, residual and cycle type
+    refinement = {"fused_per_cycle (inner 1)": {"value": value, "ms_per_step": ms_max / args.steps,
+                                                "mean_cycles_per_step": info["cycles"] / max(info["solves"], 1)}}
+    for k in (2, 3, 4):
+        st = make(torch.float32, "mixed", inner=k)
+        ms_k, info_k, _, _ = timed(st, k_tight, args.warmup)
+        ms_k = max_over_ranks(ms_k)
+        refinement[f"inner {k}"] = {"value": world * cells * k_tight / (ms_k / 1e3), "ms_per_step": ms_k / k_tight,
+                                    "mean_cycles_per_step": info_k["cycles"] / max(info_k["solves"], 1),
+                                    "converged": bool(info_k["failures"] == 0 and info_k["solves"] == k_tight)}
+        del st
+    torch.cuda.empty_cache()
+    extras = None
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras = other_workloads(sg, dev, lib, peak_gbs=_peaks()[0])
     # ---- CPU baseline on a bounded sample (rank 0, one GPU only)
     cpu = None
     cpu_error = None
@@ -557,6 +686,7 @@ def run_ours(args):
                      "mean_cycles_per_step": info64["cycles"] / max(info64["solves"], 1), "converged": bool(fp64_ok),
                      "mixed_speedup": value / value64},
         "tol_1e-10": tight,
+        "advection_arithmetic": {"float32_state": args.advection, "float64_state": "reference"},
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h + 8},
         "gpu_launches": int(launches),
@@ -576,10 +706,121 @@ def run_ours(args):
                          "frac": pre_bytes / (pre_ms / 1e3) / 1e9 / peak}}},
         "error_vs_fp64": errors,
         "error_vs_cpu_oracle": cpu_error,
+        "refinement_modes": refinement,
+        "workloads": extras,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _time_steps(torch, fn, steps, warmup):
+    """CUDA-event time of `steps` calls of fn() after `warmup` calls (ms per call)."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def other_workloads(sg, dev, lib, peak_gbs):
+    """Bounded runs of the other configurations, as sub-objects of the line:
+    plume_512  512^2 plume: red-black SOR omega 1.9 (float64; float32 state with float64
+               refinement) and multigrid V(2,2) RBGS omega 1, 8^2 coarsest (float64; float32
+               state with the mixed solve), each to 1e-6; plus the split-layout SOR sweep kernel
+               alone at 4096^2 (streaming half sweeps, 4 S bytes per cell and sweep moved)
+    plume_128  128^2 plume, Jacobi x 100 per step, float64 (the reference's iterates)
+    batch_256  the 256 batched scenes, mixed multigrid to 1e-6, autotuned, graph step"""
+    import torch
+
+    out = {}
+    # ---- 512^2
+    sc = sg.scenes.plume_512(0, steps=20)
+    p512 = {"grid": [512, 512], "tol": 1e-6}
+    runs = (("sor_fp64", "rb_sor_tolerance", sg.SORToleranceParams(omega=1.9, tol=1e-6, check_every=200),
+             torch.float64, 3),
+            ("sor_fp32_mixed", "rb_sor_tolerance",
+             sg.SORToleranceParams(omega=1.9, tol=1e-6, check_every=200, precision="mixed"), torch.float32, 3),
+            ("mg_fp64", "geometric_multigrid",
+             sg.GeometricMultigridParams(tol=1e-6, max_cycles=60, omega=1.0, coarsest=8, precision="fp64"),
+             torch.float64, 10),
+            ("mg_fp32_mixed", "geometric_multigrid",
+             sg.GeometricMultigridParams(tol=1e-6, max_cycles=60, omega=1.0, coarsest=8, precision="mixed"),
+             torch.float32, 10))
+    for name, method, params, dtype, steps in runs:
+        sim = sg.scenes.make_sim(sc, method, params, dtype=dtype, device=dev)
+        solver = sg.get_solver(method, "cuda")
+        work = []
+
+        def step(sim=sim, solver=solver, work=work, method=method):
+            sim.substep(sc.dt)
+            if method == "rb_sor_tolerance":
+                work.append(solver.last_iterations)
+                assert solver.converged
+        ms = _time_steps(torch, step, steps, 2)
+        entry = {"value": sc.cells / (ms / 1e3), "unit": "cell-steps/s", "ms_per_step": ms, "steps": steps}
+        if method == "rb_sor_tolerance":
+            entry["mean_sweeps_per_step"] = sum(work[2:]) / max(len(work) - 2, 1)
+            entry["timing"] = "host-synchronised tolerance loop (residual read every 200 sweeps)"
+        else:
+            cyc, rel, ok = solver.last_cycles, solver.last_relres, solver.converged
+            entry["last_cycles"], entry["last_relres"], entry["converged"] = cyc, rel, bool(ok)
+        p512[name] = entry
+        del sim
+    # the split-layout sweep kernel alone, at a size well above L2
+    kern = {}
+    for dtype in (torch.float32, torch.float64):
+        n = 4096
+        code = sg._lib.dtype_code(torch.empty((), dtype=dtype))
+        nb = int(lib.sg_rbsor_split_workspace_bytes(code, n, n))
+        ws = torch.zeros(nb, dtype=torch.uint8, device=dev)
+        s = sg._lib.stream_ptr()
+
+        def sweeps(k, code=code, nb=nb, ws=ws, s=s):
+            rc = lib.sg_rbsor_split_sweeps(code, n, n, ws.data_ptr(), nb, sg._lib.SG_MASK_OPEN, None, 0, None, 0,
+                                           -1e-3, 0.25, 1.9, k, 0, s)
+            assert rc == 0, lib.sg_last_error()
+        ms = _time_steps(torch, lambda: sweeps(10), 3, 1) / 10
+        S = dtype.itemsize
+        gbs = 4 * S * n * n / (ms / 1e3) / 1e9
+        kern[str(dtype).replace("torch.", "")] = {"grid": [n, n], "us_per_sweep": ms * 1e3,
+                                                  "bytes_per_cell_sweep": 4 * S, "achieved_gbs": gbs,
+                                                  "frac": gbs / peak_gbs}
+        del ws
+    p512["sor_split_kernel"] = kern
+    out["plume_512"] = p512
+    torch.cuda.empty_cache()
+    # ---- 128^2, Jacobi x 100, float64
+    sc = sg.scenes.plume_128(steps=40)
+    sim = sg.scenes.make_sim(sc, "jacobi", sg.JacobiParams(iterations=100), dtype=torch.float64, device=dev)
+    ms = _time_steps(torch, lambda: sim.substep(sc.dt), 20, 3)
+    out["plume_128"] = {"value": sc.cells / (ms / 1e3), "unit": "cell-steps/s", "ms_per_step": ms, "steps": 20,
+                        "solver": "Jacobi x 100 (reference iterates), float64",
+                        "hbm_ceiling_cell_steps_per_s": peak_gbs * 1e9 / 2568,
+                        "note": "ceiling at (21 + 100 x 3) x 8 B per cell-step; 16384 cells sit in L2 and the step "
+                                "is launch-bound (one launch per sweep)"}
+    del sim
+    # ---- batch of 256 scenes
+    scenes = sg.scenes.batch_256(256, steps=10)
+    b = sg.batch.BatchedSmoke(scenes, tol=1e-6, max_cycles=50, seed=1000, device=dev)
+    b.step(2)
+    choice = b.autotune(steps=2)
+    b.step(3)
+    _, _, tot0 = b.stats()
+    ms = _time_steps(torch, lambda: b.step(1), 10, 0)
+    _, rel, tot1 = b.stats()
+    out["batch_256"] = {"value": b.cells / (ms / 1e3), "unit": "cell-steps/s", "ms_per_step": ms, "steps": 10,
+                        "scenes": len(scenes), "cells": b.cells, "autotuned": choice,
+                        "mean_cycles_per_scene_step": float((tot1 - tot0).sum()) / (len(scenes) * 10),
+                        "scenes_not_converged_last_step": int((rel > 1e-6).sum())}
+    del b
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_batch(args):
@@ -686,6 +927,12 @@ def main():
     ap.add_argument("--fixed-cycles", type=int, default=0,
                     help="profiling: run this many cycles per solve kernel by kernel instead of the graph loop")
     ap.add_argument("--workload", choices=["mixed_2048", "batch_256"], default="mixed_2048")
+    ap.add_argument("--advection", choices=["float32", "reference"], default="float32",
+                    help="arithmetic of the float32 state's advection: float32 (relative to the cell) or the "
+                         "reference's float64 positions and weights (bit for bit)")
+    ap.add_argument("--no-extras", action="store_true", help="skip the other workloads' sub-objects")
+    ap.add_argument("--no-reference-numba", action="store_true",
+                    help="reference arm: skip timing the reference's own Numba code beside the oracle port")
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="time one path only, without e2e / roofline / CPU parts (for profiler runs)")
     args = ap.parse_args()

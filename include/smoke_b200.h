@@ -87,6 +87,21 @@ int sg_advect_velocity(int dtype, int64_t H, int64_t W, const void* u_src, int64
                        int mask_mode, const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv,
                        int64_t ld_fmv, double dt, double cell_size, void* stream);
 
+/* float32 fields advected in float32 arithmetic (advection.py:112-180: same backtrace,
+ * clamped bilinear sampling, masks and dissipation). The reference evaluates positions and
+ * weights in float64; here the backtrace offset -vel * dt / h is taken relative to the
+ * sampling point's cell, so the weights keep float32's relative precision, and the result
+ * equals the reference's up to rounding (not bit for bit). Velocity fields in MAC shapes
+ * (H x (W+1), (H+1) x W); masks as for sg_advect_velocity / sg_advect_scalar. */
+int sg_advect_velocity_f32(int64_t H, int64_t W, const void* u_src, int64_t ld_us, void* u_dst, int64_t ld_ud,
+                           const void* v_src, int64_t ld_vs, void* v_dst, int64_t ld_vd, int mask_mode,
+                           const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv, int64_t ld_fmv, double dt,
+                           double cell_size, void* stream);
+int sg_advect_scalar_f32(int64_t H, int64_t W, const void* src, int64_t ld_src, void* dst, int64_t ld_dst,
+                         const void* u, int64_t ld_u, const void* v, int64_t ld_v, int mask_mode,
+                         const uint8_t* is_fluid, int64_t ld_fluid, double dt, double cell_size, double dissipation,
+                         void* stream);
+
 /* backends/numba/operators/forces.py:78-105 (apply_forces). v is (H+1) x W; density and
  * temperature are H x W. temperature may be NULL (treated as ambient everywhere).
  * f32_temporaries=1 rounds both force terms to float32 as the reference does
@@ -342,6 +357,13 @@ int sg_gmg_solve_from_zero_async(sg_gmg_plan* plan, void* p, int64_t ld_p, const
  * sets a floor under the relative residual (near 1e-10 for a float32 state at 2048^2).
  * No counterpart in the reference. */
 int sg_gmg_set_remove_mean(sg_gmg_plan* plan, int on);
+/* Cycles per refinement step, 1..8 (default 1). With 1, a plan whose fine level runs the
+ * fused kernels corrects p and updates the fine-precision residual inside every cycle's
+ * post-smoothing kernel. With k >= 2 (classical iterative refinement) each step of the
+ * tolerance loop runs k cycles on the cycle-precision correction from zero, then p += e and
+ * one fine-precision residual pass; the cycle count grows by k per step. No counterpart in
+ * the reference. */
+int sg_gmg_set_inner_cycles(sg_gmg_plan* plan, int inner);
 /* Outcome of the last solve (synchronises stream): cycles run, last relative residual,
  * status (1 converged, 2 cycle cap reached, 3 non-finite residual) and the number of
  * cycles run by all solves since sg_gmg_bind. Any output may be NULL. */

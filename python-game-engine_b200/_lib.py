@@ -33,6 +33,8 @@ SIGNATURES = {
     "sg_advect_velocity_u": [I, I64, I64, P, I64, P, I64, P, I64, I64, I64, I, P, I64, D, D, P],
     "sg_advect_velocity_v": [I, I64, I64, P, I64, P, I64, P, I64, I64, I64, I, P, I64, D, D, P],
     "sg_advect_velocity": [I, I64, I64, P, I64, P, I64, P, I64, P, I64, I, P, I64, P, I64, D, D, P],
+    "sg_advect_velocity_f32": [I64, I64, P, I64, P, I64, P, I64, P, I64, I, P, I64, P, I64, D, D, P],
+    "sg_advect_scalar_f32": [I64, I64, P, I64, P, I64, P, I64, P, I64, I, P, I64, D, D, D, P],
     "sg_apply_forces": [I, I64, I64, P, I64, P, I64, P, I64, D, D, D, D, D, I, P],
     "sg_cool_temperature": [I, I64, I64, P, I64, D, D, D, P],
     "sg_compute_divergence": [I, I64, I64, P, I64, P, I64, P, I64, I, P, I64, P, I64, D, P],
@@ -106,6 +108,7 @@ SIGNATURES = {
     "sg_batch_snapshot_bytes": [P],
     "sg_batch_autotune": [P, I, P, I64, P, PI, PI, PI, PD],
     "sg_gmg_set_remove_mean": [P, I],
+    "sg_gmg_set_inner_cycles": [P, I],
     "sg_field_stats_workspace_bytes": [],
     "sg_field_stats": [I, I64, I64, P, I64, P, P, P],
     "sg_version": [],

@@ -356,16 +356,16 @@ __global__ void k_gmg_finalize_norm(const double* __restrict__ partial, int n, G
   if (threadIdx.x == 0) st->bnorm = sqrt(s);
 }
 
-// Relative residual after the prologue (body = 0) or a cycle (body = 1); decides whether
+// Relative residual after the prologue (body = 0) or a body of `body` cycles; decides whether
 // the WHILE node runs another cycle (when use_handle) and records the status.
 __device__ void finalize_rel_state(double s, GmgState* st, cudaGraphConditionalHandle h, int use_handle, int body) {
   double nb = st->bnorm;
   double rel = sqrt(s);
   if (!(nb == nb) || isinf(nb)) rel = nb + rel;  // a non-finite ||b|| makes the ratio non-finite
   else rel = nb > 0.0 ? rel / nb : 0.0;
-  if (body) {
-    st->cycles += 1;
-    st->total_cycles += 1;
+  if (body) {  // body = the number of V/W-cycles the graph body ran
+    st->cycles += body;
+    st->total_cycles += body;
   }
   int c = st->cycles;
   st->relres = rel;
@@ -764,6 +764,10 @@ struct sg_gmg_plan {
   // the residual in the precision of p when that differs from the cycle precision
   int fused_ir = 0;
   int64_t off_b2 = 0, off_r64 = 0;
+  // cycles per refinement step (classical iterative refinement): with inner >= 2 the body
+  // runs `inner` cycles on the cycle-precision correction from zero, then one p += e and one
+  // fine-precision residual, instead of the fused fine level's per-cycle correction
+  int inner = 1;
   // remove the fluid mean of the rhs before solving (a Neumann problem's rhs must sum to
   // zero; float rounding of a telescoping divergence sum leaves a component no p removes)
   int remove_mean = 0;
@@ -1228,7 +1232,7 @@ static void prologue(const sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div, i
   }
   // from a zero guess the fused fine level carries the residual from here on (b0 / r64), so
   // the FP64 rhs itself is not kept
-  TP* bkeep = (zero_guess && p->fused_ir) ? nullptr : bf;
+  TP* bkeep = (zero_guess && p->fused_ir && p->inner <= 1) ? nullptr : bf;
   SG_LAUNCH(k_gmg_rhs<TD, TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, div, ldd, st, m, bkeep, p->ld_bfine, part,
                                                           zero_guess ? pp : nullptr, ldp, ws_ptr<TC>(p, L.off_b), L.ld,
                                                           r64, p->remove_mean));
@@ -1251,7 +1255,7 @@ static void body(const sg_gmg_plan* p, TP* pp, int64_t ldp, cudaGraphConditional
   LevelMask m = level_mask(p, 0);
   double* part = (double*)(p->ws + p->off_partial);
   GmgState* st = state_ptr(p);
-  if (p->fused_ir) {
+  if (p->fused_ir && p->inner <= 1) {
     // pre (rhs by cycle parity) -> coarse levels -> post + correction + next residual
     const TC* b_alt = ws_ptr<TC>(p, p->off_b2);
     switch (p->pre) {
@@ -1272,12 +1276,13 @@ static void body(const sg_gmg_plan* p, TP* pp, int64_t ldp, cudaGraphConditional
     return;
   }
   dim3 g = grid_wide(L.W, L.H);
-  cycle<TC>(p, 0, true, s);
+  const int inner = p->inner < 1 ? 1 : p->inner;
+  for (int q = 0; q < inner; ++q) cycle<TC>(p, 0, q == 0, s);
   SG_LAUNCH(k_gmg_correct<TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, pp, ldp, ws_ptr<TC>(p, L.off_e), L.ld));
   SG_LAUNCH(k_gmg_fine_residual<TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, pp, ldp, (const TP*)(p->ws + p->off_bfine),
                                                                    p->ld_bfine, m, ws_ptr<TC>(p, L.off_b), L.ld,
                                                                    (TP*)nullptr, part));
-  SG_LAUNCH(k_gmg_finalize_rel<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st, h, use_handle, 1));
+  SG_LAUNCH(k_gmg_finalize_rel<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st, h, use_handle, inner));
 }
 
 static unsigned long long counter() { return launch_count(); }
@@ -1762,6 +1767,17 @@ int sg_gmg_set_remove_mean(sg_gmg_plan* plan, int on) {
     plan->exec = nullptr;
   }
   plan->remove_mean = on;
+  return SG_OK;
+}
+
+int sg_gmg_set_inner_cycles(sg_gmg_plan* plan, int inner) {
+  SG_REQUIRE(plan, "null plan");
+  SG_REQUIRE(inner >= 1 && inner <= 8, "inner cycles must be in 1..8");
+  if (plan->inner != inner && plan->exec) {  // the cached solve graph has the old body
+    cudaGraphExecDestroy(plan->exec);
+    plan->exec = nullptr;
+  }
+  plan->inner = inner;
   return SG_OK;
 }
 

@@ -51,6 +51,26 @@ struct RegXchg {
   T xbot[NWARP][32];
 };
 
+// Synchronisation of the row exchange. With SG_REG_PAIR_SYNC (the default) each pair of
+// adjacent warps shares one named barrier (id w for warps w - 1 and w, 64 threads), so a
+// warp waits for its two neighbours only, not for the slowest warp of the block. A warp
+// takes its upper barrier before its lower one: warp 0 has no upper one, so the chain always
+// completes. Double buffering stays safe: a warp rewrites buffer buf only after the next
+// exchange's barriers with both neighbours, which they reach after reading buf.
+#ifndef SG_REG_PAIR_SYNC
+#define SG_REG_PAIR_SYNC 1
+#endif
+template <int NWARP>
+__device__ __forceinline__ void sync_neighbour_warps(int w) {
+#if SG_REG_PAIR_SYNC
+  static_assert(NWARP <= 16, "one named barrier per warp edge (ids 1 .. NWARP - 1)");
+  if (w > 0) asm volatile("bar.sync %0, 64;" ::"r"(w) : "memory");
+  if (w < NWARP - 1) asm volatile("bar.sync %0, 64;" ::"r"(w + 1) : "memory");
+#else
+  __syncthreads();
+#endif
+}
+
 // Publish the warp's edge rows into buffer buf, wait, and fetch the neighbouring warps'
 // edges: above = row w RPT - 1 (last row of warp w - 1), below = row (w + 1) RPT (first row
 // of warp w + 1). The outermost warps get their own rows back (halo cells, never used).
@@ -65,7 +85,7 @@ __device__ __forceinline__ void exchange_rows(RegXchg<T, NWARP>& x, int buf, con
   bo.y = e[RPT - 1][1];
   x.top[buf][w][lane] = t;
   x.bot[buf][w][lane] = bo;
-  __syncthreads();
+  sync_neighbour_warps<NWARP>(w);
   const V a = x.bot[buf][w > 0 ? w - 1 : w][lane];
   const V b = x.top[buf][w < NWARP - 1 ? w + 1 : w][lane];
   above[0] = a.x;

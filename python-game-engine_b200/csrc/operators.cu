@@ -317,6 +317,68 @@ __global__ void k_jacobi(int H, int W, const T* __restrict__ p, int64_t ldp, T* 
   o[(int64_t)j * ldo + i] = (T)(((double)s + alpha * (double)div[(int64_t)j * ldd + i]) * rb);
 }
 
+// jacobi.py:8-24, several sweeps per launch on grids that sit in L2 (where one launch per
+// sweep is launch-bound). A block stages a 16 x 32 tile plus a halo of kJG cells in shared
+// memory, sweeps there with the valid region shrinking by one cell per sweep along region
+// edges that are not the grid's edges, and writes its own cells: after `sweeps` <= kJG sweeps
+// they hold exactly the grid-wide iterates (each update is k_jacobi's expression, in the
+// same order, on the same values). Reads src, writes dst (different buffers).
+constexpr int kJTR = 16, kJTC = 32, kJG = 8, kJT = 256;
+
+template <typename T, int MM>
+__global__ void __launch_bounds__(kJT) k_jacobi_tiles(int H, int W, const T* __restrict__ src, int64_t lds,
+                                                      T* __restrict__ dst, int64_t ldd, const T* __restrict__ div,
+                                                      int64_t lddv, MasksT<MM> m, double alpha, double rb,
+                                                      int sweeps) {
+  constexpr int RR = kJTR + 2 * kJG, CC = kJTC + 2 * kJG;
+  __shared__ T sa[RR * CC], sb[RR * CC], sdv[RR * CC];
+  const int j0 = blockIdx.y * kJTR, i0 = blockIdx.x * kJTC;
+  const int R0 = max(j0 - kJG, 0), R1 = min(j0 + kJTR + kJG, H);
+  const int C0 = max(i0 - kJG, 0), C1 = min(i0 + kJTC + kJG, W);
+  const int nc = C1 - C0;
+  for (int e = threadIdx.x; e < (R1 - R0) * nc; e += kJT) {
+    const int rr = e / nc, cc = e - rr * nc;
+    sa[rr * CC + cc] = src[(int64_t)(R0 + rr) * lds + C0 + cc];
+    sdv[rr * CC + cc] = div[(int64_t)(R0 + rr) * lddv + C0 + cc];
+  }
+  __syncthreads();
+  T* a = sa;
+  T* b = sb;
+  for (int sw = 0; sw < sweeps; ++sw) {
+    const int rlo = R0 + (R0 > 0 ? sw + 1 : 0), rhi = R1 - (R1 < H ? sw + 1 : 0);
+    const int clo = C0 + (C0 > 0 ? sw + 1 : 0), chi = C1 - (C1 < W ? sw + 1 : 0);
+    const int w = chi - clo;
+    for (int e = threadIdx.x; e < (rhi - rlo) * w; e += kJT) {
+      const int j = rlo + e / w, i = clo + e % w;
+      const int rr = j - R0, cc = i - C0;
+      const T c = a[rr * CC + cc];
+      T out = c;
+      if (m.fluid(j, i)) {
+        // nbsum_ref's neighbours (clamped indices) and order, on the staged tile
+        const T l = m.u(j, i) ? a[rr * CC + (max(i - 1, 0) - C0)] : c;
+        const T r = m.u(j, i + 1) ? a[rr * CC + (min(i + 1, W - 1) - C0)] : c;
+        const T d = m.v(j, i) ? a[(max(j - 1, 0) - R0) * CC + cc] : c;
+        const T u = m.v(j + 1, i) ? a[(min(j + 1, H - 1) - R0) * CC + cc] : c;
+        T sum = l + r;
+        sum = sum + d;
+        sum = sum + u;
+        out = (T)(((double)sum + alpha * (double)sdv[rr * CC + cc]) * rb);
+      }
+      b[rr * CC + cc] = out;
+    }
+    __syncthreads();
+    T* t = a;
+    a = b;
+    b = t;
+  }
+  const int jh = min(j0 + kJTR, H), ih = min(i0 + kJTC, W);
+  const int ow = ih - i0;
+  for (int e = threadIdx.x; e < (jh - j0) * ow; e += kJT) {
+    const int j = j0 + e / ow, i = i0 + e % ow;
+    dst[(int64_t)j * ldd + i] = a[(j - R0) * CC + (i - C0)];
+  }
+}
+
 // red_black_sor_gauss_seidel.py:8-27, one colour: cells with (i + j) % 2 == color.
 template <typename T>
 __global__ void k_rbsor_half(int H, int W, T* __restrict__ p, int64_t ldp, const T* __restrict__ div, int64_t ldd,
@@ -408,6 +470,9 @@ __global__ void k_coarsen_solid(int Hc, int Wc, const uint8_t* __restrict__ s, i
 using namespace sg;
 
 // ------------------------------------------------------------------ argument checks
+// largest grid (bytes of one field) solved by the multi-sweep Jacobi tiles
+constexpr int64_t kJacobiTileMaxBytes = (int64_t)8 << 20;
+
 static int check_grid(int64_t H, int64_t W) {
   if (H < 1 || W < 1 || H > (1 << 28) || W > (1 << 28)) return fail(SG_ERR_ARG, "bad grid %lld x %lld", (long long)H, (long long)W);
   return SG_OK;
@@ -759,7 +824,25 @@ int sg_jacobi_solve(int dtype, int64_t H, int64_t W, void* p, int64_t ld_p, cons
     int64_t lda = ld_p;
     T* b = (T*)scratch;
     int64_t ldb = W;
-    for (int it = 0; it < iterations; ++it) {
+    // grids that sit in L2: kJG sweeps per launch on shared-memory tiles (same iterates)
+    const bool tiles = H * W * (int64_t)sizeof(T) <= kJacobiTileMaxBytes;
+    const int per = tiles ? kJG : 1;
+    for (int it = 0; it < iterations; it += per) {
+      if (tiles) {
+        const int n = iterations - it < kJG ? iterations - it : kJG;
+        SG_MASK_DISPATCH(mask_mode, {
+          SG_LAUNCH(k_jacobi_tiles<T, MM><<<dim3((unsigned)((W + kJTC - 1) / kJTC), (unsigned)((H + kJTR - 1) / kJTR)),
+                                           kJT, 0, s>>>((int)H, (int)W, a, lda, b, ldb, (const T*)div, ld_div,
+                                                        m.as<MM>(), alpha, reciprocal_beta, n));
+        });
+        T* t = a;
+        a = b;
+        b = t;
+        int64_t tl = lda;
+        lda = ldb;
+        ldb = tl;
+        continue;
+      }
       SG_LAUNCH(k_jacobi<T><<<grid2d(W, H), block2d(), 0, s>>>((int)H, (int)W, a, lda, b, ldb, (const T*)div, ld_div, m, alpha,
                                                      reciprocal_beta));
       T* t = a;

@@ -85,7 +85,9 @@ def main():
     out = {"problem": f"inverse {args.n}^2 x {args.steps} steps", "checkpoint_every": 8}
     if args.fd:
         t0 = time.perf_counter()
-        out["fd_check_fp64"] = fd_check(args.n, args.steps, args.fd)
+        # the step sizes bracket the rounding floor: below ~1e-5 the error of the differences
+        # grows like 1 / eps (rounding of the rollouts), above it like eps^2 (truncation)
+        out["fd_check_fp64"] = fd_check(args.n, args.steps, args.fd, eps=(1e-7, 1e-6, 1e-5, 1e-4))
         out["fd_check_fp64"]["seconds"] = time.perf_counter() - t0
     model, force, target = A.inverse_problem(n=args.n, steps=args.steps, dtype=torch.float32, precision="fp32",
                                              tol=1e-6)

@@ -60,9 +60,22 @@ def _same_dtype(*ts):
     return L.dtype_code(ts[0])
 
 
+def _arithmetic(arithmetic, dt_code):
+    if arithmetic == "reference":
+        return False
+    if arithmetic == "float32":
+        if dt_code != L.SG_F32:
+            raise TypeError("arithmetic='float32' advects float32 fields")
+        return True
+    raise ValueError(f"arithmetic must be 'reference' or 'float32', got {arithmetic!r}")
+
+
 def advect_scalar_field(field_source, field_dest, velocity_u, velocity_v, is_fluid, dt, cell_size,
-                        dissipation: float = 1.0, **_ignored):
-    """advection.py:112-128; ``dissipation`` fuses simulation.py:232 (density *= 0.999)."""
+                        dissipation: float = 1.0, arithmetic: str = "reference", **_ignored):
+    """advection.py:112-128; ``dissipation`` fuses simulation.py:232 (density *= 0.999).
+    ``arithmetic="float32"`` (float32 fields): backtrace and interpolation in float32
+    relative to the cell (``sg_advect_scalar_f32``), equal to the reference's float64
+    arithmetic up to rounding; "reference" (default) reproduces it bit for bit."""
     dt_code = _same_dtype(field_source, field_dest, velocity_u, velocity_v)
     H, W = field_source.shape
     if tuple(field_dest.shape) != (H, W):
@@ -72,6 +85,12 @@ def advect_scalar_field(field_source, field_dest, velocity_u, velocity_v, is_flu
     u, ldu = L.field(velocity_u, "velocity_u")
     v, ldv = L.field(velocity_v, "velocity_v")
     mode, pf, ldf = _masks(is_fluid, "is_fluid", (H, W))
+    if _arithmetic(arithmetic, dt_code):
+        if tuple(velocity_u.shape) != (H, W + 1) or tuple(velocity_v.shape) != (H + 1, W):
+            raise ValueError("velocity fields must have MAC shapes (H, W+1) and (H+1, W)")
+        L.call("sg_advect_scalar_f32", H, W, s, lds, d, ldd, u, ldu, v, ldv, mode, pf, ldf, float(dt),
+               float(cell_size), float(dissipation), L.stream_ptr())
+        return
     L.call("sg_advect_scalar", dt_code, H, W, s, lds, d, ldd, u, velocity_u.shape[0], velocity_u.shape[1], ldu,
            v, velocity_v.shape[0], velocity_v.shape[1], ldv, mode, pf, ldf, float(dt), float(cell_size),
            float(dissipation), L.stream_ptr())
@@ -101,8 +120,9 @@ def advect_velocity_v(velocity_v_source, velocity_v_dest, velocity_u, face_mask_
            mode, pm, ldm, float(dt), float(cell_size), L.stream_ptr())
 
 
-def advect_velocity(u_src, u_dst, v_src, v_dst, face_mask_u, face_mask_v, dt, cell_size):
-    """Both velocity advections of simulation.py:280-286 in one launch (MAC shapes)."""
+def advect_velocity(u_src, u_dst, v_src, v_dst, face_mask_u, face_mask_v, dt, cell_size, arithmetic="reference"):
+    """Both velocity advections of simulation.py:280-286 in one launch (MAC shapes);
+    ``arithmetic`` as for advect_scalar_field."""
     dt_code = _same_dtype(u_src, u_dst, v_src, v_dst)
     H, W1 = u_src.shape
     W = W1 - 1
@@ -113,6 +133,10 @@ def advect_velocity(u_src, u_dst, v_src, v_dst, face_mask_u, face_mask_v, dt, ce
     b, ldb = L.field(u_dst, "u_dst")
     c, ldc = L.field(v_src, "v_src")
     d, ldd = L.field(v_dst, "v_dst")
+    if _arithmetic(arithmetic, dt_code):
+        L.call("sg_advect_velocity_f32", H, W, a, lda, b, ldb, c, ldc, d, ldd, mode, pu, lu, pv, lv, float(dt),
+               float(cell_size), L.stream_ptr())
+        return
     L.call("sg_advect_velocity", dt_code, H, W, a, lda, b, ldb, c, ldc, d, ldd, mode, pu, lu, pv, lv, float(dt),
            float(cell_size), L.stream_ptr())
 

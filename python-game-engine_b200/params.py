@@ -101,6 +101,7 @@ class GeometricMultigridParams:
     fixed_cycles: int = 0       # > 0: run exactly this many cycles without host checks
     rebuild_masks: bool = False
     remove_mean: bool = False   # subtract the fluid mean of the rhs (rounding of sum(div)) before solving
+    inner_cycles: int = 1       # >= 2: classical refinement, that many FP32 cycles per FP64 residual
 
     def string(self):
         return (f"GeometricMultigridParams_{self.cycle}{self.pre_sweeps}{self.post_sweeps}_w{self.omega}"

@@ -226,6 +226,9 @@ class SmokeSimulation2D:
         self.step_index = 0
         self.debug = getattr(config, "debug", False)
         self.profiler = profiler if profiler is not None else NullProfileSession()
+        # "reference": the reference's float64 sampling arithmetic, bit for bit; "float32":
+        # float32 fields advected in float32 arithmetic (equal up to rounding, faster)
+        self.advection_arithmetic = "reference"
 
     def _init_boundaries(self):
         self._solid_mask[0, :] = True
@@ -359,20 +362,21 @@ class SmokeSimulation2D:
     def _advect_velocity(self, dt):
         fmu, fmv, _ = self._kmasks
         ops.advect_velocity(self.velocity_u, self.velocity_u_temp, self.velocity_v, self.velocity_v_temp, fmu, fmv, dt,
-                            self.cell_size)
+                            self.cell_size, arithmetic=self.advection_arithmetic)
         self.velocity_u, self.velocity_u_temp = self.velocity_u_temp, self.velocity_u
         self.velocity_v, self.velocity_v_temp = self.velocity_v_temp, self.velocity_v
 
     def _advect_density(self, dt):
         _, _, fl = self._kmasks
         ops.advect_scalar_field(self.density, self.density_temp, self.velocity_u, self.velocity_v, fl, dt,
-                                self.cell_size, dissipation=self.density_dissipation)
+                                self.cell_size, dissipation=self.density_dissipation,
+                                arithmetic=self.advection_arithmetic)
         self.density, self.density_temp = self.density_temp, self.density
 
     def _advect_temperature(self, dt):
         _, _, fl = self._kmasks
         ops.advect_scalar_field(self._temperature, self.temperature_temp, self.velocity_u, self.velocity_v, fl, dt,
-                                self.cell_size)
+                                self.cell_size, arithmetic=self.advection_arithmetic)
         self._temperature, self.temperature_temp = self.temperature_temp, self._temperature
 
     def _compute_divergence(self):

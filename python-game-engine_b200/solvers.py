@@ -258,7 +258,7 @@ class GMGPlan:
     """A bound multigrid plan (host plan + device workspace) for one grid and mask."""
 
     def __init__(self, H, W, fmu, fmv, device, coarsest=8, omega=1.3, pre=2, post=2, cycle="V", precision="fp64",
-                 remove_mean=False):
+                 remove_mean=False, inner_cycles=1):
         lib = L.load()
         self.H, self.W, self.precision = H, W, precision
         handle = ctypes.c_void_p()
@@ -277,6 +277,7 @@ class GMGPlan:
                 "sg_gmg_plan_create")
         self.handle = handle
         L.check(lib.sg_gmg_set_remove_mean(handle, 1 if remove_mean else 0), "sg_gmg_set_remove_mean")
+        L.check(lib.sg_gmg_set_inner_cycles(handle, int(inner_cycles)), "sg_gmg_set_inner_cycles")
         nbytes = lib.sg_gmg_workspace_bytes(handle)
         self.workspace = torch.empty(int(nbytes), dtype=torch.uint8, device=device)
         L.check(lib.sg_gmg_bind(handle, self.workspace.data_ptr(), L.stream_ptr()), "sg_gmg_bind")
@@ -353,6 +354,10 @@ class GeometricMultigridSolver:
     ``strict=True`` reads it at once and raises NotConverged / SmokeCudaError. With
     ``fixed_cycles > 0`` exactly that many cycles run kernel by kernel (capturable);
     per-cycle relative residuals then stay on the device in ``last_relres_dev``.
+    ``inner_cycles`` k >= 2 (mixed precision): classical iterative refinement, k FP32 cycles
+    on the correction from zero between two FP64 passes (p += e, residual), instead of the
+    fused fine level that corrects p and updates the FP64 residual every cycle; the cycle
+    counts then grow in steps of k.
     """
 
     def __init__(self):
@@ -388,25 +393,27 @@ class GeometricMultigridSolver:
         return next(iter(self._plans.values()), None)
 
     def plan_for(self, H, W, fmu, fmv, device, coarsest, omega, pre, post, cycle, precision, rebuild=False,
-                 remove_mean=False):
+                 remove_mean=False, inner_cycles=1):
         if isinstance(fmu, AnalyticMask):
             mkey = ("analytic", fmu.mode)
         else:
             mkey = (fmu.data_ptr(), fmu._version, fmv.data_ptr(), fmv._version)
-        key = (H, W, mkey, coarsest, omega, pre, post, cycle, precision, str(device), bool(remove_mean))
+        key = (H, W, mkey, coarsest, omega, pre, post, cycle, precision, str(device), bool(remove_mean),
+               int(inner_cycles))
         plan = self._plans.get(key)
         if plan is None or rebuild:
-            plan = GMGPlan(H, W, fmu, fmv, device, coarsest, omega, pre, post, cycle, precision, remove_mean)
+            plan = GMGPlan(H, W, fmu, fmv, device, coarsest, omega, pre, post, cycle, precision, remove_mean,
+                           inner_cycles)
             self._plans = {key: plan}
         return plan
 
     def __call__(self, pressure, divergence, face_mask_u, face_mask_v, fluid_density, cell_size, dt, tol=1e-6,
                  max_cycles=50, cycle="V", pre_sweeps=2, post_sweeps=2, omega=1.3, coarsest=8, precision="fp64",
                  check_every=1, fixed_cycles=0, rebuild_masks=False, strict=False, zero_initial_guess=False,
-                 remove_mean=False, **_ignored):
+                 remove_mean=False, inner_cycles=1, **_ignored):
         H, W = pressure.shape
         plan = self.plan_for(H, W, face_mask_u, face_mask_v, pressure.device, coarsest, omega, pre_sweeps, post_sweeps,
-                             cycle, precision, rebuild_masks, remove_mean)
+                             cycle, precision, rebuild_masks, remove_mean, inner_cycles)
         want = torch.float32 if precision == "fp32" else torch.float64
         if pressure.dtype == want:
             p = pressure

@@ -1,8 +1,8 @@
 """Generate golden fixtures by running the reference's own Numba kernels.
 
 Run in a container that holds the reference source (it is not needed anywhere
-else):  python tests/golden/make_golden.py path/to/reference/src
-(or with REFERENCE_SRC set to that path)
+else):  python tests/golden/make_golden.py path/to/reference/src [generator ...]
+(or with REFERENCE_SRC set to that path; generator names select a subset, default all)
 
 The reference (LCEBurton/python-game-engine, src/cfd) is imported read-only; numba's
 on-disk cache is redirected to tests/golden/_numba_cache (git-ignored) because the
@@ -232,9 +232,55 @@ def gen_sim():
     save("sim", **d)
 
 
+def obstacle_solid(H, W):
+    """The 1-cell wall ring plus a rectangle and a disc inside (set_solid_mask replaces the
+    whole solid mask, so the ring is part of it, as a caller of the reference would pass)."""
+    j, i = np.indices((H, W))
+    solid = np.zeros((H, W), bool)
+    solid[0, :] = solid[-1, :] = True
+    solid[:, 0] = solid[:, -1] = True
+    solid[14:18, 6:13] = True
+    solid |= (i + 0.5 - 22.0) ** 2 + (j + 0.5 - 20.0) ** 2 < 3.2 ** 2
+    return solid
+
+
+def gen_sim_obstacles():
+    """SmokeSimulation2D substeps after set_solid_mask with interior obstacles (the masks are
+    rebuilt at the next substep, simulation.py:133-143, :198-204; the reference multigrid
+    rebuilds its hierarchy with rebuild_masks=True)."""
+    d = {}
+    H = W = 32
+    solid = obstacle_solid(H, W)
+    d["solid"] = solid
+    for name, method, params in (
+        ("jacobi", "jacobi", JacobiParams(iterations=30)),
+        ("mg", "multigrid", MultigridParams(smoother_type="jacobi", num_levels=3, v_cycles=2,
+                                            smoother_iterations=2, coarsest_iterations=20, rebuild_masks=True)),
+    ):
+        cfg = SimulationConfig(grid=GridConfig(size=(W, H), cell_size=1.0 / H),
+                               pressure_solver=PressureSolverConfig(method=method, params=params))
+        sim = SmokeSimulation2D(cfg, profiler=ProfileSession.disabled((H, W)))
+        sim.add_emitter(Emitter2D(position=(16, 6), radius=4.0, density_value=3.0, temperature_value=2.0,
+                                  velocity_value=(0.3, 2.0), approach="linear", numba_optimized=True))
+        for step in range(8):
+            if step == 2:
+                sim.set_solid_mask(solid.astype(np.uint8))
+            sim.substep(sim.dt)
+            if step in (1, 2, 7):
+                d[f"{name}_s{step}_density"] = sim.density.copy()
+                d[f"{name}_s{step}_u"] = sim.velocity_u.copy()
+                d[f"{name}_s{step}_v"] = sim.velocity_v.copy()
+                d[f"{name}_s{step}_p"] = sim.pressure.copy()
+                d[f"{name}_s{step}_t"] = sim.temperature.copy()
+                d[f"{name}_s{step}_div"] = sim.divergence.copy()
+                d[f"{name}_s{step}_res"] = sim.pressure_residual.copy()
+    save("sim_obstacles", **d)
+
+
+GENERATORS = {"operators": gen_operators, "kat_shapes": gen_kat_shapes, "multigrid": gen_multigrid,
+              "emitters": gen_emitters, "sim": gen_sim, "sim_obstacles": gen_sim_obstacles}
+
 if __name__ == "__main__":
-    gen_operators()
-    gen_kat_shapes()
-    gen_multigrid()
-    gen_emitters()
-    gen_sim()
+    # optional generator names after the reference path select a subset (default: all)
+    for name in (sys.argv[2:] or list(GENERATORS)):
+        GENERATORS[name]()

@@ -140,3 +140,77 @@ def test_two_gloo_ranks_agree_on_the_shards():
     scs = S.batch_256(64)
     assert sorted(gathered[0] + gathered[1]) == list(range(64))
     assert cells == sum(s.H * s.W for s in scs)
+
+
+# ---------------------------------------------------------------- against the CPU oracle
+_ORACLE_RUNS = {}
+ORACLE_STEPS = 5
+
+
+def _oracle_batch(sweeps, cycle, scs):
+    """The CPU oracle (the reference kernels restated in C, and the same multigrid: red-black
+    over-relaxation 1.3, full weighting, bilinear prolongation, exact coarsest <= 8 a side,
+    FP32 cycles in FP64 refinement to 1e-6) stepping every scene of `scs`; cached per
+    (sweeps, cycle), which is all the autotuner's choices change in the arithmetic."""
+    import oracle as O
+
+    key = (sweeps, cycle)
+    if key not in _ORACLE_RUNS:
+        out = []
+        for sc in scs:
+            fmu, fmv = O.face_masks_from_solid(np.zeros((sc.H, sc.W), bool))
+            fl = O.is_fluid_from_faces(fmu, fmv)
+            gmg = O.GMGOracle(fmu, fmv, fl, coarsest=8, omega=1.3, pre=sweeps, post=sweeps, cycle=cycle)
+            rels = []
+
+            def solver(p, div, fmu_, fmv_, rho, h, dt, gmg=gmg, fl=fl, rels=rels, **_):
+                b = O.alpha_coeff(h, rho, dt) * div.astype(np.float64) * fl
+                p64 = np.zeros(p.shape)
+                _, hist = gmg.solve(p64, b, tol=1e-6, max_cycles=50, precision="mixed")
+                rels.append(hist[-1])
+                p[:] = p64.astype(p.dtype)
+
+            sim = O.OracleSim(sc.H, sc.W, sc.cell_size, solver, {}, dtype=np.float32)
+            sim.dt, sim.gravity = sc.dt, sc.gravity
+            sim.plumes = [O.PlumeSpec(*row, seed=sc.seed) for row in sc.plumes]
+            for _ in range(ORACLE_STEPS):
+                sim.substep(sc.dt)
+            assert max(rels) <= 1e-6
+            out.append((sim.density.copy(), sim.velocity_u.copy(), sim.velocity_v.copy(), sim.pressure.copy()))
+        _ORACLE_RUNS[key] = out
+    return _ORACLE_RUNS[key]
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cycle", ["V", "W"])
+@pytest.mark.parametrize("sweeps", [1, 2, 3])
+@pytest.mark.parametrize("tile", [0, 1, 2, 3])
+def test_batch_matches_the_cpu_oracle_for_every_autotuner_choice(tile, sweeps, cycle):
+    """Seven scenes of four sizes (64 .. 256), every (tile, sweeps, V/W) candidate of the
+    autotuner, 5 steps, against the oracle stepping each scene on its own.
+    Stated tolerance: 1e-5 relative L2 on density, u, v and the pressure (mean removed). The
+    operators are bit-exact; the solves run the same cycles and stop at the same 1e-6, and
+    differ only by the rounding of their float32 cycles (the GPU contracts multiply-adds,
+    the oracle does not), ~1e-7 of the pressure per solve."""
+    scs = _scenes(range(7))
+    assert len({s.H for s in scs}) >= 4
+    b = B.BatchedSmoke(scs, tol=1e-6)
+    b.configure(tile, sweeps, cycle)
+    b.step(ORACLE_STEPS)
+    torch.cuda.synchronize()
+    cyc, rel, _ = b.stats()
+    assert np.all(rel <= 1e-6) and np.all(cyc < 50)
+    ref = _oracle_batch(sweeps, cycle, scs)
+    for k, (d0, u0, v0, p0) in enumerate(ref):
+        d, u, v, p = (t.double().cpu().numpy() for t in b.fields(k))
+        assert np.max(d0) > 0.5, k
+        assert _rel(d, d0) <= 1e-5, (k, "density", _rel(d, d0))
+        assert _rel(u, u0) <= 1e-5, (k, "u", _rel(u, u0))
+        assert _rel(v, v0) <= 1e-5, (k, "v", _rel(v, v0))
+        pc, p0c = p - p.mean(), p0 - p0.mean()
+        assert _rel(pc, p0c) <= 1e-5, (k, "pressure", _rel(pc, p0c))

@@ -202,3 +202,23 @@ def test_gmg_oracle_default_over_relaxation():
         assert hist[-1] <= 1e-10
     assert O.GMGOracle(fmu, fmv, fl).omega == 1.3
     assert cycles[1.3] <= 6 and cycles[1.3] < cycles[1.2] and cycles[1.3] < cycles[1.4]
+
+
+@pytest.mark.parametrize("name", ["jacobi", "mg"])
+def test_oracle_substeps_with_obstacles_match_reference(name):
+    """set_solid_mask with interior obstacles before the third substep (simulation.py:133-143,
+    masks rebuilt at the next substep, :198-204; the reference multigrid with rebuild_masks)."""
+    d = golden("sim_obstacles")
+    solver, kw = SIM_CASES[name]
+    if name == "mg":
+        kw = dict(kw, rebuild_masks=True)
+    sim = O.OracleSim(32, 32, 1 / 32, solver or O.MultigridReference(), kw)
+    sim.emitters.append(O.EmitterSpec((16, 6), 4.0, 3.0, 2.0, (0.3, 2.0), "linear"))
+    for step in range(8):
+        if step == 2:
+            sim.set_solid_mask(d["solid"])
+        sim.substep(sim.dt)
+        if step in (1, 2, 7):
+            for k, attr in (("density", "density"), ("u", "velocity_u"), ("v", "velocity_v"), ("p", "pressure"),
+                            ("t", "temperature"), ("div", "divergence"), ("res", "pressure_residual")):
+                assert np.array_equal(getattr(sim, attr), d[f"{name}_s{step}_{k}"]), (step, k)

@@ -36,12 +36,12 @@ if not torch.cuda.is_available():
     pytest.skip("CUDA device required", allow_module_level=True)
 
 import oracle as O  # noqa: E402
+from sim_checks import check_divergence_bound, recording  # noqa: E402
 
 sg = package()
 scenes = sg.scenes
 TOL = 1e-6
 SOR_CHECK = 200
-_RECORDED = {}
 
 
 def _rel(a, b):
@@ -53,34 +53,6 @@ def _rel(a, b):
 def _prel(a, b):
     a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
     return _rel(a - a.mean(), b - b.mean())
-
-
-def recording(method):
-    """The CUDA solver `method` registered once more under a test name that first records the
-    norm of the divergence it is handed (the pre-projection divergence)."""
-    name = f"test_recorded_{method}"
-    if name not in _RECORDED:
-        inner = sg.get_solver(method, "cuda")
-        norms = []
-
-        def fn(pressure, divergence, *args, **kw):
-            norms.append(float(divergence.double().norm()))
-            inner(pressure, divergence, *args, **kw)
-
-        sg.register_solver(name, "cuda", fn)
-        _RECORDED[name] = norms
-    return name, _RECORDED[name]
-
-
-def check_divergence_bound(sim, div_before, tol):
-    """||div after projection|| on cells >= 2 from the ring <= tol ||div before|| + rounding."""
-    d = sim.divergence.double()[2:-2, 2:-2]
-    eps = 6e-8 if sim.divergence.dtype == torch.float32 else 1.2e-16
-    vmax = max(float(sim.velocity_u.abs().max()), float(sim.velocity_v.abs().max()))
-    rounding = 8 * eps * vmax / sim.cell_size * np.sqrt(d.numel())
-    got = float(d.norm())
-    assert got <= tol * div_before * 1.001 + rounding, (got, tol * div_before, rounding)
-    return got
 
 
 def _oracle(sc, solver, dtype):
