@@ -184,6 +184,16 @@ int sg_plume_sources(int dtype, int64_t H, int64_t W, void* density, int64_t ld_
 int sg_build_masks(int64_t H, int64_t W, const uint8_t* solid, int64_t ld_s, uint8_t* fmu, int64_t ld_fmu,
                    uint8_t* fmv, int64_t ld_fmv, uint8_t* is_fluid, int64_t ld_fluid, void* stream);
 
+/* Bounds-check build (lib/libsmoke_b200_bc.so, compiled with -DSG_BOUNDS_CHECK=1): the
+ * tiled kernels check their index arithmetic before each access, skip an access that fails
+ * and record the source line of the first failure per compilation unit; nothing traps.
+ * sg_bounds_check reports the first recorded line (0: none) and its unit (0 operators,
+ * 1 gmg, 2 batch, 3 rbsor_split, 4 advect_fast, 5 adjoint, 6 metrics; -1: none) and, with
+ * clear != 0, resets the records. sg_bounds_check_enabled: 1 in that build, 0 otherwise (where
+ * sg_bounds_check always reports none). No counterpart in the reference. */
+int sg_bounds_check_enabled(void);
+int sg_bounds_check(unsigned int* first_line, int* unit, int clear);
+
 /* ---------------------------------------------------------------- reference solvers */
 
 /* backends/numba/solvers/jacobi.py:8-52: `iterations` ping-pong sweeps. scratch: device

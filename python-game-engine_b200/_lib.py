@@ -11,7 +11,9 @@ import os
 import torch
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libsmoke_b200.so")
+# SG_LIBRARY_VARIANT=bounds selects the bounds-check build (index checks in the tiled kernels)
+LIB_PATH = os.path.join(_HERE, "lib", "libsmoke_b200_bc.so" if os.environ.get("SG_LIBRARY_VARIANT") == "bounds"
+                        else "libsmoke_b200.so")
 
 SG_F32, SG_F64 = 0, 1
 SG_MASK_PLANES, SG_MASK_OPEN, SG_MASK_RING, SG_MASK_NONE = 0, 1, 2, 3
@@ -111,6 +113,8 @@ SIGNATURES = {
     "sg_gmg_set_inner_cycles": [P, I],
     "sg_field_stats_workspace_bytes": [],
     "sg_field_stats": [I, I64, I64, P, I64, P, P, P],
+    "sg_bounds_check_enabled": [],
+    "sg_bounds_check": [ctypes.POINTER(ctypes.c_uint), PI, I],
     "sg_version": [],
     "sg_last_error": [],
     "sg_launch_count": [],
@@ -162,6 +166,14 @@ def load():
             fn.restype = _RESTYPE.get(name, ctypes.c_int)
         _lib = lib
     return _lib
+
+
+def bounds_check(clear=True):
+    """(first failed source line, unit) recorded by the bounds-check build since the last
+    clear, (0, -1) when none (and always in the normal build)."""
+    line, unit = ctypes.c_uint(0), ctypes.c_int(-1)
+    check(load().sg_bounds_check(ctypes.byref(line), ctypes.byref(unit), 1 if clear else 0), "sg_bounds_check")
+    return line.value, unit.value
 
 
 def exported_symbols():

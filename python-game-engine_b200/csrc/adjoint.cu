@@ -467,3 +467,5 @@ int sg_adjoint_divergence(int dtype, int64_t H, int64_t W, const void* lam_div, 
 }
 
 }  // extern "C"
+
+SG_BOUNDS_ACCESSOR(adjoint)

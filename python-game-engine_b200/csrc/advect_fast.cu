@@ -139,3 +139,5 @@ int sg_advect_scalar_f32(int64_t H, int64_t W, const void* src, int64_t ld_src, 
 }
 
 }  // extern "C"
+
+SG_BOUNDS_ACCESSOR(advect_fast)

@@ -525,6 +525,7 @@ __global__ void __launch_bounds__(32 * BReg::NWARP, BReg::MINB) k_b_reg_pre(BPoo
     const float* bsrc = ((P.cycles[t.scene] & 1) ? P.b1 : P.b0) + sc.oc;
     const BLevel C = level_of(P, sc, 1);
     const int i0 = t.tx * S::TXO - S::HALO, j0 = t.ty * S::TYO - S::HALO;
+    if (!SG_IN_BOUNDS(t.scene >= 0 && i0 + S::HALO >= 0 && i0 + S::HALO < sc.W && j0 + S::HALO < sc.H)) continue;
     const bool inside = i0 >= 0 && i0 + kRW <= sc.W && j0 >= 0 && j0 + BReg::NWARP * BReg::RPT <= sc.H;
     if (inside)
       reg_pre_body<float, SW, BReg::RPT, BReg::NWARP, false>(x, nullptr, P.e2c + sc.oc, bsrc, sc.W, sc.H, sc.W, C.b,
@@ -550,6 +551,7 @@ __global__ void __launch_bounds__(32 * BReg::NWARP, BReg::MINB_FINAL)
     float* bdst = (odd ? P.b0 : P.b1) + sc.oc;
     const BLevel C = level_of(P, sc, 1);
     const int i0 = t.tx * S::TXO - S::HALO, j0 = t.ty * S::TYO - S::HALO;
+    if (!SG_IN_BOUNDS(t.scene >= 0 && i0 + S::HALO >= 0 && i0 + S::HALO < sc.W && j0 + S::HALO < sc.H)) continue;
     const bool inside = i0 >= 0 && i0 + kRW <= sc.W && j0 >= 0 && j0 + BReg::NWARP * BReg::RPT <= sc.H;
     double sq = 0.0;
     if (inside)
@@ -581,6 +583,7 @@ __global__ void __launch_bounds__(32 * BReg::NWARP, BReg::MINB) k_b_reg_pre_lev(
     const BScene& sc = P.scenes[t.scene];
     const BLevel L = level_of(P, sc, k), C = level_of(P, sc, k + 1);
     const int i0 = t.tx * S::TXO - S::HALO, j0 = t.ty * S::TYO - S::HALO;
+    if (!SG_IN_BOUNDS(t.scene >= 0 && i0 + S::HALO >= 0 && i0 + S::HALO < L.W && j0 + S::HALO < L.H)) continue;
     const bool inside = i0 >= 0 && i0 + kRW <= L.W && j0 >= 0 && j0 + BReg::NWARP * BReg::RPT <= L.H;
     if (inside)
       reg_pre_body<float, SW, BReg::RPT, BReg::NWARP, false>(x, zero ? nullptr : L.e, e2_of(P, sc, k), L.b, L.W, L.H,
@@ -603,6 +606,7 @@ __global__ void __launch_bounds__(32 * BReg::NWARP, BReg::MINB) k_b_reg_post_lev
     const BScene& sc = P.scenes[t.scene];
     const BLevel L = level_of(P, sc, k), C = level_of(P, sc, k + 1);
     const int i0 = t.tx * S::TXO - S::HALO, j0 = t.ty * S::TYO - S::HALO;
+    if (!SG_IN_BOUNDS(t.scene >= 0 && i0 + S::HALO >= 0 && i0 + S::HALO < L.W && j0 + S::HALO < L.H)) continue;
     const bool inside = i0 >= 0 && i0 + kRW <= L.W && j0 >= 0 && j0 + BReg::NWARP * BReg::RPT <= L.H;
     if (inside)
       reg_post_body<float, SW, BReg::RPT, BReg::NWARP, false>(x, e2_of(P, sc, k), L.e, L.b, L.W, L.H, L.W, C.e, C.W,
@@ -1548,3 +1552,5 @@ int sg_batch_autotune(sg_batch* b, int steps, void* scratch, int64_t scratch_byt
 }
 
 }  // extern "C"
+
+SG_BOUNDS_ACCESSOR(batch)

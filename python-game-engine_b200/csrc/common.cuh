@@ -21,6 +21,41 @@ int check_launch(const char* what);
 void note_launch();
 unsigned long long launch_count();
 
+// ------------------------------------------------------------------ bounds-check build
+// Built with -DSG_BOUNDS_CHECK=1 (lib/libsmoke_b200_bc.so), the index arithmetic of the
+// tiled kernels is checked before each access: SG_IN_BOUNDS(cond) records the source line of
+// the first failed check in a per-unit device word (sg_bounds_check reads them) and returns
+// false, and the caller skips the access. In the normal build the check is `true` and
+// compiles away. Nothing traps: a bad index is reported to the host, the context stays usable.
+#ifndef SG_BOUNDS_CHECK
+#define SG_BOUNDS_CHECK 0
+#endif
+#if SG_BOUNDS_CHECK
+static __device__ unsigned int g_bounds_line;  // one word per translation unit
+__device__ __forceinline__ bool in_bounds(bool ok, unsigned line) {
+  if (!ok) atomicCAS(&g_bounds_line, 0u, line);
+  return ok;
+}
+#define SG_IN_BOUNDS(cond) (::sg::in_bounds((cond), __LINE__))
+// first failed line of this unit (0: none); clear != 0 resets it
+#define SG_BOUNDS_ACCESSOR(unit)                                                          \
+  extern "C" int sg_bounds_line_##unit(unsigned* line, int clear) {                       \
+    if (cudaMemcpyFromSymbol(line, ::sg::g_bounds_line, sizeof(unsigned)) != cudaSuccess) \
+      return SG_ERR_CUDA;                                                                 \
+    const unsigned zero = 0;                                                              \
+    if (clear && cudaMemcpyToSymbol(::sg::g_bounds_line, &zero, sizeof(unsigned)) != cudaSuccess) \
+      return SG_ERR_CUDA;                                                                 \
+    return SG_OK;                                                                         \
+  }
+#else
+#define SG_IN_BOUNDS(cond) true
+#define SG_BOUNDS_ACCESSOR(unit)                                  \
+  extern "C" int sg_bounds_line_##unit(unsigned* line, int) {     \
+    *line = 0;                                                    \
+    return SG_OK;                                                 \
+  }
+#endif
+
 // Launch a kernel and count it: SG_LAUNCH(k<T><<<grid, block, smem, stream>>>(args));
 #define SG_LAUNCH(...)   \
   do {                   \

@@ -1842,3 +1842,5 @@ int sg_gmg_fine_kernel_async(sg_gmg_plan* plan, int which, void* p, int64_t ld_p
 }
 
 }  // extern "C"
+
+SG_BOUNDS_ACCESSOR(gmg)

@@ -164,9 +164,13 @@ __device__ __forceinline__ void reg_load(T (&v)[RPT][2], const T* __restrict__ a
   for (int r = 0; r < RPT; ++r) {
     const int jj = j + r;
     if (!BOUNDED) {
-      const V t = *reinterpret_cast<const V*>(a + (int64_t)jj * ld + i);
-      v[r][0] = t.x;
-      v[r][1] = t.y;
+      if (SG_IN_BOUNDS(jj >= 0 && jj < H && i >= 0 && i + 1 < W)) {
+        const V t = *reinterpret_cast<const V*>(a + (int64_t)jj * ld + i);
+        v[r][0] = t.x;
+        v[r][1] = t.y;
+      } else {
+        v[r][0] = v[r][1] = (T)0;
+      }
     } else {
       const bool row = jj >= 0 && jj < H;
       v[r][0] = (row && i >= 0 && i < W) ? a[(int64_t)jj * ld + i] : (T)0;
@@ -186,12 +190,13 @@ __device__ __forceinline__ void reg_store(const T (&v)[RPT][2], T* __restrict__ 
     if (r < r_lo || r >= r_hi) continue;
     const int jj = j + r;
     if (!BOUNDED) {
+      if (!SG_IN_BOUNDS(jj >= 0 && jj < H && i >= 0 && i + 1 < W)) continue;
       V t;
       t.x = v[r][0];
       t.y = v[r][1];
       *reinterpret_cast<V*>(a + (int64_t)jj * ld + i) = t;
     } else {
-      if (jj >= H) continue;
+      if (jj >= H || !SG_IN_BOUNDS(jj >= 0 && i >= 0)) continue;
       if (i < W) a[(int64_t)jj * ld + i] = v[r][0];
       if (i + 1 < W) a[(int64_t)jj * ld + i + 1] = v[r][1];
     }
@@ -372,8 +377,9 @@ __device__ __forceinline__ void reg_prolong_smooth(RegXchg<T, NWARP>& x, T (&e)[
   auto fetch = [&](int J, T& cl, T& cm, T& cr) {
     const int Jc = J < 0 ? 0 : (J > Hc - 1 ? Hc - 1 : J);
     const T* row = ec + (int64_t)Jc * ldc;
-    const T v = row[Ic];
-    const T ve = edge ? row[Iedge] : (T)0;
+    const bool ok = SG_IN_BOUNDS(Jc >= 0 && Jc < Hc && Ic >= 0 && Ic < Wc && Iedge >= 0 && Iedge < Wc);
+    const T v = ok ? row[Ic] : (T)0;
+    const T ve = (edge && ok) ? row[Iedge] : (T)0;
     const T lv = shfl_up1(v), rv = shfl_down1(v);
     cl = lane == 0 ? ve : lv;
     cm = v;
@@ -491,6 +497,7 @@ __device__ __forceinline__ void reg_post_final_body(RegXchg<TC, NWARP>& x, const
     if (r < r_lo || r >= r_hi || !cols_owned) continue;
     const int jj = j + r;
     if (BOUNDED && jj >= H) continue;
+    if (!SG_IN_BOUNDS(jj >= 0 && jj < H && i >= 0 && (BOUNDED || i + 1 < W))) continue;
     const int64_t o = (int64_t)jj * ld + i;
     TP acc[2];
     if (r64 && !BOUNDED) {

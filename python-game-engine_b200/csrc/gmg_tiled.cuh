@@ -123,7 +123,8 @@ __device__ __forceinline__ void tile_load(const SplitTile<T>& t, const T* __rest
   for (int f = tile_tid(); f < EX * EY; f += tile_nt()) {
     const int r = f / EX, c = f - r * EX;
     const int j = t.j0 + r, i = t.i0 + c;
-    const bool in = INTERIOR || (j >= 0 && j < t.H && i >= 0 && i < t.W);
+    const bool in = (INTERIOR && SG_IN_BOUNDS(j >= 0 && j < t.H && i >= 0 && i < t.W)) ||
+                    (!INTERIOR && j >= 0 && j < t.H && i >= 0 && i < t.W);
     const int64_t g = (int64_t)j * ld + i;
     t.E(r, c) = (in && e) ? e[g] : (T)0;
     t.B(r, c) = in ? b[g] : (T)0;
@@ -135,7 +136,8 @@ __device__ __forceinline__ void tile_store(const SplitTile<T>& t, T* __restrict_
   for (int f = tile_tid(); f < TX * TY; f += tile_nt()) {
     const int rr = f / TX, cc = f - rr * TX;
     const int j = t.j0 + HALO + rr, i = t.i0 + HALO + cc;
-    if (INTERIOR || (j < t.H && i < t.W)) e[(int64_t)j * ld + i] = t.E(HALO + rr, HALO + cc);
+    if (INTERIOR ? SG_IN_BOUNDS(j >= 0 && j < t.H && i >= 0 && i < t.W) : (j < t.H && i < t.W))
+      e[(int64_t)j * ld + i] = t.E(HALO + rr, HALO + cc);
   }
 }
 
@@ -273,7 +275,8 @@ __device__ __forceinline__ void post_body(const SplitTile<T>& t, const T* __rest
     const int r = f / S::EX, c = f - r * S::EX;
     const int j = t.j0 + r, i = t.i0 + c;
     T ev = (T)0, bv = (T)0;
-    if (INTERIOR || (j >= 0 && j < t.H && i >= 0 && i < t.W)) {
+    if (INTERIOR ? SG_IN_BOUNDS(j >= 0 && j < t.H && i >= 0 && i < t.W && (j >> 1) < Hc && (i >> 1) < Wc)
+                 : (j >= 0 && j < t.H && i >= 0 && i < t.W)) {
       const int J = j >> 1, I = i >> 1;
       int Y = J + ((j & 1) ? 1 : -1), X = I + ((i & 1) ? 1 : -1);
       Y = Y < 0 ? 0 : (Y > Hc - 1 ? Hc - 1 : Y);

@@ -184,3 +184,5 @@ int sg_field_stats(int dtype, int64_t H, int64_t W, const void* field, int64_t l
 }
 
 }  // extern "C"
+
+SG_BOUNDS_ACCESSOR(metrics)

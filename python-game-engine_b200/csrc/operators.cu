@@ -338,6 +338,7 @@ __global__ void __launch_bounds__(kJT) k_jacobi_tiles(int H, int W, const T* __r
   const int nc = C1 - C0;
   for (int e = threadIdx.x; e < (R1 - R0) * nc; e += kJT) {
     const int rr = e / nc, cc = e - rr * nc;
+    if (!SG_IN_BOUNDS(rr < RR && cc < CC && R0 + rr < H && C0 + cc < W)) continue;
     sa[rr * CC + cc] = src[(int64_t)(R0 + rr) * lds + C0 + cc];
     sdv[rr * CC + cc] = div[(int64_t)(R0 + rr) * lddv + C0 + cc];
   }
@@ -351,6 +352,9 @@ __global__ void __launch_bounds__(kJT) k_jacobi_tiles(int H, int W, const T* __r
     for (int e = threadIdx.x; e < (rhi - rlo) * w; e += kJT) {
       const int j = rlo + e / w, i = clo + e % w;
       const int rr = j - R0, cc = i - C0;
+      if (!SG_IN_BOUNDS(rr >= 0 && rr < RR && cc >= 0 && cc < CC && (i == 0 || i - 1 >= C0) &&
+                        (i == W - 1 || i + 1 < C1) && (j == 0 || j - 1 >= R0) && (j == H - 1 || j + 1 < R1)))
+        continue;
       const T c = a[rr * CC + cc];
       T out = c;
       if (m.fluid(j, i)) {
@@ -375,6 +379,7 @@ __global__ void __launch_bounds__(kJT) k_jacobi_tiles(int H, int W, const T* __r
   const int ow = ih - i0;
   for (int e = threadIdx.x; e < (jh - j0) * ow; e += kJT) {
     const int j = j0 + e / ow, i = i0 + e % ow;
+    if (!SG_IN_BOUNDS(j - R0 < RR && i - C0 < CC && j < H && i < W)) continue;
     dst[(int64_t)j * ldd + i] = a[(j - R0) * CC + (i - C0)];
   }
 }
@@ -957,4 +962,36 @@ int sg_mg_coarsen_solid(int64_t H, int64_t W, const uint8_t* solid, int64_t ld_s
   return check_launch("sg_mg_coarsen_solid");
 }
 
+}  // extern "C"
+
+SG_BOUNDS_ACCESSOR(operators)
+
+extern "C" {
+int sg_bounds_line_gmg(unsigned* line, int clear);
+int sg_bounds_line_batch(unsigned* line, int clear);
+int sg_bounds_line_rbsor_split(unsigned* line, int clear);
+int sg_bounds_line_advect_fast(unsigned* line, int clear);
+int sg_bounds_line_adjoint(unsigned* line, int clear);
+int sg_bounds_line_metrics(unsigned* line, int clear);
+
+int sg_bounds_check_enabled(void) { return SG_BOUNDS_CHECK; }
+
+int sg_bounds_check(unsigned* first_line, int* unit, int clear) {
+  SG_REQUIRE(first_line && unit, "null output");
+  int (*const fns[])(unsigned*, int) = {sg_bounds_line_operators,   sg_bounds_line_gmg,     sg_bounds_line_batch,
+                                        sg_bounds_line_rbsor_split, sg_bounds_line_advect_fast,
+                                        sg_bounds_line_adjoint,     sg_bounds_line_metrics};
+  *first_line = 0;
+  *unit = -1;
+  for (int k = 0; k < (int)(sizeof(fns) / sizeof(fns[0])); ++k) {
+    unsigned line = 0;
+    const int rc = fns[k](&line, clear);
+    if (rc != SG_OK) return fail(rc, "bounds-check word of unit %d unreadable", k);
+    if (line && !*first_line) {
+      *first_line = line;
+      *unit = k;
+    }
+  }
+  return SG_OK;
+}
 }  // extern "C"

@@ -115,6 +115,7 @@ __global__ void __launch_bounds__(256) k_rbsor_split_half(int H, int W, T* __res
   if (j >= H || kv >= nk) return;
   const int s = (j + color) & 1;
   const int64_t row = (int64_t)j * ldh;
+  if (!SG_IN_BOUNDS(kv + N <= ldh && j >= 0)) return;
   T cc[N], dd[N], oo[N], dn[N], up[N];
   vec_to_array<T>(*reinterpret_cast<const V*>(own + row + kv), cc);
   vec_to_array<T>(*reinterpret_cast<const V*>(dvc + row + kv), dd);
@@ -187,6 +188,7 @@ __global__ void __launch_bounds__(kTileThreads) k_rbsor_split_tiles(int H, int W
     const int rr = e / nkk, kk = e - rr * nkk;
     const int64_t g = (int64_t)(R0 + rr) * ldh + kb + kk;
     const int sidx = rr * S::KP + kk;
+    if (!SG_IN_BOUNDS(R0 + rr < H && kb + kk < ldh && rr < S::RR && kk < S::KK)) continue;
     sp[sidx] = a0[g];
     sp[S::RR * S::KP + sidx] = a1[g];
     sd[sidx] = d0[g];
@@ -209,6 +211,9 @@ __global__ void __launch_bounds__(kTileThreads) k_rbsor_split_tiles(int H, int W
         const int i = C0 + 2 * kk + s;
         if (i < clo || i >= chi || !m.fluid(j, i)) continue;
         const int sidx = rr * S::KP + kk;
+        if (!SG_IN_BOUNDS(rr >= 1 - (j == 0) && rr + 1 < S::RR + (j == H - 1) && kk + s <= S::KK &&
+                          (i == 0 || kk - 1 + s >= 0)))
+          continue;
         const T cv = own[sidx];
         const T l = m.u(j, i) ? (i > 0 ? oth[max(sidx - 1 + s, 0)] : cv) : cv;
         const T r = m.u(j, i + 1) ? (i < W - 1 ? oth[sidx + s] : cv) : cv;
@@ -232,6 +237,7 @@ __global__ void __launch_bounds__(kTileThreads) k_rbsor_split_tiles(int H, int W
     const int i = 2 * k + ((j + c) & 1);
     if (i >= ochi) continue;
     const int sidx = (j - R0) * S::KP + (k - kb);
+    if (!SG_IN_BOUNDS(j < H && k < ldh && k - kb >= 0 && k - kb < S::KK && j - R0 < S::RR)) continue;
     (c ? b1 : b0)[(int64_t)j * ldh + k] = sp[c * S::RR * S::KP + sidx];
   }
 }
@@ -718,3 +724,5 @@ int sg_rbsor_mixed_solve(int64_t H, int64_t W, void* p, int64_t ld_p, const void
 }
 
 }  // extern "C"
+
+SG_BOUNDS_ACCESSOR(rbsor_split)
