@@ -550,6 +550,13 @@ def run_ours(args):
         return ms, info, launches, clocks
 
     # ---- mixed precision (headline)
+    if args.only == "sor":  # profiler runs: the split-layout SOR sweep kernel alone
+        if rank == 0:
+            print(json.dumps({"only": "sor", "sor_split_kernel": sor_split_kernel(sg, dev, lib, _peaks()[0],
+                                                                                 sweeps_per_launch=2, reps=1)}))
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
     only_fp64 = args.only == "fp64"
     sim = make(torch.float64, "fp64") if only_fp64 else make(torch.float32, "mixed")
     ms, info, launches, clocks = timed(sim, args.steps, args.warmup, sample_clocks=True)
@@ -728,6 +735,34 @@ def _time_steps(torch, fn, steps, warmup):
     return a.elapsed_time(b) / steps
 
 
+def sor_split_kernel(sg, dev, lib, peak_gbs, n=4096, sweeps_per_launch=10, reps=3):
+    """The split-layout red-black SOR sweep kernel alone (streaming half sweeps) at n^2, float32
+    and float64, on a grid well above L2: 4 S bytes per cell and sweep moved (each half sweep
+    reads the other colour's plane, its own plane and divergence, writes its own)."""
+    import torch
+
+    kern = {}
+    for dtype in (torch.float32, torch.float64):
+        code = sg._lib.dtype_code(torch.empty((), dtype=dtype))
+        nb = int(lib.sg_rbsor_split_workspace_bytes(code, n, n))
+        ws = torch.zeros(nb, dtype=torch.uint8, device=dev)
+        s = sg._lib.stream_ptr()
+
+        def sweeps(k, code=code, nb=nb, ws=ws, s=s):
+            rc = lib.sg_rbsor_split_sweeps(code, n, n, ws.data_ptr(), nb, sg._lib.SG_MASK_OPEN, None, 0, None, 0,
+                                           -1e-3, 0.25, 1.9, k, 0, s)
+            assert rc == 0, lib.sg_last_error()
+        ms = _time_steps(torch, lambda: sweeps(sweeps_per_launch), reps, 1) / sweeps_per_launch
+        S = dtype.itemsize
+        gbs = 4 * S * n * n / (ms / 1e3) / 1e9
+        kern[str(dtype).replace("torch.", "")] = {"grid": [n, n], "us_per_sweep": ms * 1e3,
+                                                  "bytes_per_cell_sweep": 4 * S, "achieved_gbs": gbs,
+                                                  "frac": gbs / peak_gbs}
+        del ws
+    torch.cuda.empty_cache()
+    return kern
+
+
 def other_workloads(sg, dev, lib, peak_gbs):
     """Bounded runs of the other configurations, as sub-objects of the line:
     plume_512  512^2 plume: red-black SOR omega 1.9 (float64; float32 state with float64
@@ -772,27 +807,7 @@ def other_workloads(sg, dev, lib, peak_gbs):
             entry["last_cycles"], entry["last_relres"], entry["converged"] = cyc, rel, bool(ok)
         p512[name] = entry
         del sim
-    # the split-layout sweep kernel alone, at a size well above L2
-    kern = {}
-    for dtype in (torch.float32, torch.float64):
-        n = 4096
-        code = sg._lib.dtype_code(torch.empty((), dtype=dtype))
-        nb = int(lib.sg_rbsor_split_workspace_bytes(code, n, n))
-        ws = torch.zeros(nb, dtype=torch.uint8, device=dev)
-        s = sg._lib.stream_ptr()
-
-        def sweeps(k, code=code, nb=nb, ws=ws, s=s):
-            rc = lib.sg_rbsor_split_sweeps(code, n, n, ws.data_ptr(), nb, sg._lib.SG_MASK_OPEN, None, 0, None, 0,
-                                           -1e-3, 0.25, 1.9, k, 0, s)
-            assert rc == 0, lib.sg_last_error()
-        ms = _time_steps(torch, lambda: sweeps(10), 3, 1) / 10
-        S = dtype.itemsize
-        gbs = 4 * S * n * n / (ms / 1e3) / 1e9
-        kern[str(dtype).replace("torch.", "")] = {"grid": [n, n], "us_per_sweep": ms * 1e3,
-                                                  "bytes_per_cell_sweep": 4 * S, "achieved_gbs": gbs,
-                                                  "frac": gbs / peak_gbs}
-        del ws
-    p512["sor_split_kernel"] = kern
+    p512["sor_split_kernel"] = sor_split_kernel(sg, dev, lib, peak_gbs)
     out["plume_512"] = p512
     torch.cuda.empty_cache()
     # ---- 128^2, Jacobi x 100, float64
@@ -933,7 +948,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the other workloads' sub-objects")
     ap.add_argument("--no-reference-numba", action="store_true",
                     help="reference arm: skip timing the reference's own Numba code beside the oracle port")
-    ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
+    ap.add_argument("--only", choices=["mixed", "fp64", "sor"], default=None,
                     help="time one path only, without e2e / roofline / CPU parts (for profiler runs)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

@@ -51,14 +51,16 @@ struct RegXchg {
   T xbot[NWARP][32];
 };
 
-// Synchronisation of the row exchange. With SG_REG_PAIR_SYNC (the default) each pair of
-// adjacent warps shares one named barrier (id w for warps w - 1 and w, 64 threads), so a
-// warp waits for its two neighbours only, not for the slowest warp of the block. A warp
-// takes its upper barrier before its lower one: warp 0 has no upper one, so the chain always
-// completes. Double buffering stays safe: a warp rewrites buffer buf only after the next
-// exchange's barriers with both neighbours, which they reach after reading buf.
+// Synchronisation of the row exchange: the block-wide barrier by default. With
+// SG_REG_PAIR_SYNC=1 each pair of adjacent warps shares one named barrier instead (id w for
+// warps w - 1 and w, 64 threads), so a warp waits for its two neighbours only. A warp takes
+// its upper barrier before its lower one: warp 0 has no upper one, so the chain always
+// completes; double buffering stays safe, since a warp rewrites buffer buf only after the
+// next exchange's barriers with both neighbours, which they reach after reading buf.
+// Measured at 2048^2 (mixed, ncu launch list): the pair barriers made the register-tile
+// kernels slower (fine post 42.9 -> 44.1 us, pre 12.8 -> 13.4 us, 1024^2 post 9.2 -> 10.3 us).
 #ifndef SG_REG_PAIR_SYNC
-#define SG_REG_PAIR_SYNC 1
+#define SG_REG_PAIR_SYNC 0
 #endif
 template <int NWARP>
 __device__ __forceinline__ void sync_neighbour_warps(int w) {
