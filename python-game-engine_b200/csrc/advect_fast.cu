@@ -17,15 +17,29 @@
 
 namespace sg {
 
+// floor(x) as an integer k and as a float f, for |x| < 2^22, without a conversion
+// instruction (the conversion unit was the busiest pipe of this kernel): adding 1.5 * 2^23
+// rounded toward -infinity puts floor(x) + 1.5 * 2^23 in a float whose unit in the last place
+// is 1, so its bit pattern minus that of 1.5 * 2^23 is floor(x), and subtracting the constant
+// back is exact.
+__device__ __forceinline__ void floor_split(float x, int& k, float& f) {
+  const float t = __fadd_rd(x, 12582912.0f);
+  k = __float_as_int(t) - 0x4B400000;
+  f = t - 12582912.0f;
+}
+
 // Clamped bilinear sample of f (rows x cols, row stride ld) at (bi + ox, bj + oy).
 __device__ __forceinline__ float sample_rel(const float* __restrict__ f, int64_t ld, int rows, int cols, int bi, int bj,
                                             float ox, float oy) {
-  // keep the offsets finite and far from integer overflow (NaN ends at an edge, as in the
-  // reference kernels' saturating conversions)
+  // keep the offsets finite and well inside floor_split's range (NaN ends at an edge, as in
+  // the reference kernels' saturating conversions)
   ox = fminf(fmaxf(ox, -1048576.f), 1048576.f);
   oy = fminf(fmaxf(oy, -1048576.f), 1048576.f);
-  const float fx = floorf(ox), fy = floorf(oy);
-  const int x0 = bi + (int)fx, y0 = bj + (int)fy;
+  int kx, ky;
+  float fx, fy;
+  floor_split(ox, kx, fx);
+  floor_split(oy, ky, fy);
+  const int x0 = bi + kx, y0 = bj + ky;
   const bool inx = x0 >= 0 && x0 < cols - 1;
   const bool iny = y0 >= 0 && y0 < rows - 1;
   const int xa = min(max(x0, 0), cols - 1), xb = inx ? x0 + 1 : xa;
