@@ -13,50 +13,47 @@
 //
 // Clamping follows advection.py:31-38: indices are clamped to the grid before the weight is
 // taken, so a sample whose bracket leaves the grid takes the edge value.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace sg {
 
-// floor(x) as an integer k and as a float f, for |x| < 2^22, without a conversion
-// instruction (the conversion unit was the busiest pipe of this kernel): adding 1.5 * 2^23
-// rounded toward -infinity puts floor(x) + 1.5 * 2^23 in a float whose unit in the last place
-// is 1, so its bit pattern minus that of 1.5 * 2^23 is floor(x), and subtracting the constant
-// back is exact.
-__device__ __forceinline__ void floor_split(float x, int& k, float& f) {
-  const float t = __fadd_rd(x, 12582912.0f);
-  k = __float_as_int(t) - 0x4B400000;
-  f = t - 12582912.0f;
-}
-
-// Clamped bilinear sample of f (rows x cols, row stride ld) at (bi + ox, bj + oy).
-__device__ __forceinline__ float sample_rel(const float* __restrict__ f, int64_t ld, int rows, int cols, int bi, int bj,
+// Clamped bilinear sample of f (rows x cols, row stride ld; rows * ld < 2^31) at
+// (bi + ox, bj + oy).
+__device__ __forceinline__ float sample_rel(const float* __restrict__ f, int ld, int rows, int cols, int bi, int bj,
                                             float ox, float oy) {
-  // keep the offsets finite and well inside floor_split's range (NaN ends at an edge, as in
-  // the reference kernels' saturating conversions)
+  // keep the offsets finite and far from integer overflow (NaN ends at an edge, as in the
+  // reference kernels' saturating conversions)
   ox = fminf(fmaxf(ox, -1048576.f), 1048576.f);
   oy = fminf(fmaxf(oy, -1048576.f), 1048576.f);
-  int kx, ky;
-  float fx, fy;
-  floor_split(ox, kx, fx);
-  floor_split(oy, ky, fy);
-  const int x0 = bi + kx, y0 = bj + ky;
+  const float fx = floorf(ox), fy = floorf(oy);
+  const int x0 = bi + (int)fx, y0 = bj + (int)fy;
   const bool inx = x0 >= 0 && x0 < cols - 1;
   const bool iny = y0 >= 0 && y0 < rows - 1;
   const int xa = min(max(x0, 0), cols - 1), xb = inx ? x0 + 1 : xa;
   const int ya = min(max(y0, 0), rows - 1), yb = iny ? y0 + 1 : ya;
   const float tx = inx ? ox - fx : 0.f, ty = iny ? oy - fy : 0.f;
-  const float* r0 = f + (int64_t)ya * ld;
-  const float* r1 = f + (int64_t)yb * ld;
+  const float* r0 = f + ya * ld;
+  const float* r1 = f + yb * ld;
   const float c0 = fmaf(r0[xb] - r0[xa], tx, r0[xa]);
   const float c1 = fmaf(r1[xb] - r1[xa], tx, r1[xa]);
   return fmaf(c1 - c0, ty, c0);
 }
 
+// The mean of a 2 x 2 block (a b / c d) as two lerps at 1/2 and one between them, the
+// bilinear sample at the block's centre without index arithmetic.
+__device__ __forceinline__ float centre4(float a, float b, float c, float d) {
+  const float c0 = fmaf(b - a, 0.5f, a);
+  const float c1 = fmaf(d - c, 0.5f, c);
+  return fmaf(c1 - c0, 0.5f, c0);
+}
+
 // u faces (H x (W+1)) and v faces ((H+1) x W) in one launch; c = dt / h.
 template <int MM>
-__global__ void k_advect_uv_f32(int H, int W, const float* __restrict__ us, int64_t ldus, float* __restrict__ ud,
-                                int64_t ldud, const float* __restrict__ vs, int64_t ldvs, float* __restrict__ vd,
-                                int64_t ldvd, MasksT<MM> m, float c) {
+__global__ void k_advect_uv_f32(int H, int W, const float* __restrict__ us, int ldus, float* __restrict__ ud, int ldud,
+                                const float* __restrict__ vs, int ldvs, float* __restrict__ vd, int ldvd, MasksT<MM> m,
+                                float c) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
 #pragma unroll
   for (int q = 0; q < kRows; ++q) {
@@ -64,31 +61,39 @@ __global__ void k_advect_uv_f32(int H, int W, const float* __restrict__ us, int6
     if (j < H && i <= W) {
       float out = 0.f;
       if (m.u(j, i)) {
-        // advection.py:130-154: v at the u face (i, j + 0.5) is the v grid at (i - 0.5, j + 0.5)
-        const float uu = us[(int64_t)j * ldus + i];
-        const float vv = sample_rel(vs, ldvs, H + 1, W, i, j, -0.5f, 0.5f);
+        // advection.py:130-154: v at the u face (i, j + 0.5) is the v grid at (i - 0.5, j + 0.5):
+        // the 2 x 2 block of columns i - 1, i and rows j, j + 1 away from the side walls
+        const float uu = us[j * ldus + i];
+        const float vv = (i >= 1 && i <= W - 1)
+                             ? centre4(vs[j * ldvs + i - 1], vs[j * ldvs + i], vs[(j + 1) * ldvs + i - 1],
+                                       vs[(j + 1) * ldvs + i])
+                             : sample_rel(vs, ldvs, H + 1, W, i, j, -0.5f, 0.5f);
         out = sample_rel(us, ldus, H, W + 1, i, j, -uu * c, -vv * c);
       }
-      ud[(int64_t)j * ldud + i] = out;
+      ud[j * ldud + i] = out;
     }
     if (j <= H && i < W) {
       float out = 0.f;
       if (m.v(j, i)) {
-        // advection.py:156-180: u at the v face (i + 0.5, j) is the u grid at (i + 0.5, j - 0.5)
-        const float uu = sample_rel(us, ldus, H, W + 1, i, j, 0.5f, -0.5f);
-        const float vv = vs[(int64_t)j * ldvs + i];
+        // advection.py:156-180: u at the v face (i + 0.5, j) is the u grid at (i + 0.5, j - 0.5):
+        // the 2 x 2 block of columns i, i + 1 and rows j - 1, j away from the floor and ceiling
+        const float uu = (j >= 1 && j <= H - 1)
+                             ? centre4(us[(j - 1) * ldus + i], us[(j - 1) * ldus + i + 1], us[j * ldus + i],
+                                       us[j * ldus + i + 1])
+                             : sample_rel(us, ldus, H, W + 1, i, j, 0.5f, -0.5f);
+        const float vv = vs[j * ldvs + i];
         out = sample_rel(vs, ldvs, H + 1, W, i, j, -uu * c, -vv * c);
       }
-      vd[(int64_t)j * ldvd + i] = out;
+      vd[j * ldvd + i] = out;
     }
   }
 }
 
 // advection.py:112-128 (+ dissipation, simulation.py:232)
 template <int MM>
-__global__ void k_advect_scalar_f32(int H, int W, const float* __restrict__ src, int64_t lds, float* __restrict__ dst,
-                                    int64_t ldd, const float* __restrict__ u, int64_t ldu, const float* __restrict__ v,
-                                    int64_t ldv, MasksT<MM> m, float c, float diss) {
+__global__ void k_advect_scalar_f32(int H, int W, const float* __restrict__ src, int lds, float* __restrict__ dst,
+                                    int ldd, const float* __restrict__ u, int ldu, const float* __restrict__ v, int ldv,
+                                    MasksT<MM> m, float c, float diss) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= W) return;
 #pragma unroll
@@ -98,11 +103,13 @@ __global__ void k_advect_scalar_f32(int H, int W, const float* __restrict__ src,
     float out = 0.f;
     if (m.fluid(j, i)) {
       // face velocities at the cell centre: u grid at (i + 0.5, j), v grid at (i, j + 0.5)
-      const float uu = sample_rel(u, ldu, H, W + 1, i, j, 0.5f, 0.f);
-      const float vv = sample_rel(v, ldv, H + 1, W, i, j, 0.f, 0.5f);
+      const float ua = u[j * ldu + i], ub = u[j * ldu + i + 1];
+      const float va = v[j * ldv + i], vb = v[(j + 1) * ldv + i];
+      const float uu = fmaf(ub - ua, 0.5f, ua);
+      const float vv = fmaf(vb - va, 0.5f, va);
       out = sample_rel(src, lds, H, W, i, j, -uu * c, -vv * c) * diss;
     }
-    dst[(int64_t)j * ldd + i] = out;
+    dst[j * ldd + i] = out;
   }
 }
 
@@ -122,12 +129,14 @@ int sg_advect_velocity_f32(int64_t H, int64_t W, const void* u_src, int64_t ld_u
   SG_REQUIRE(cell_size > 0.0, "cell_size must be positive");
   SG_REQUIRE(mask_mode == SG_MASK_OPEN || mask_mode == SG_MASK_RING || (mask_mode == SG_MASK_PLANES && fmu && fmv),
              "bad mask mode or missing mask planes");
+  SG_REQUIRE((H + 1) * std::max(std::max(ld_us, ld_ud), std::max(ld_vs, ld_vd)) < ((int64_t)1 << 31),
+             "fields of 2^31 elements or more: use sg_advect_velocity");
   Masks m = make_masks(mask_mode, H, W, fmu, ld_fmu, fmv, ld_fmv, nullptr, 0);
   const float c = (float)(dt / cell_size);
   SG_MASK_DISPATCH(mask_mode, {
     SG_LAUNCH(k_advect_uv_f32<MM><<<grid2d_rows(W + 1, H + 1), block2d(), 0, as_stream(stream)>>>(
-        (int)H, (int)W, (const float*)u_src, ld_us, (float*)u_dst, ld_ud, (const float*)v_src, ld_vs, (float*)v_dst,
-        ld_vd, m.as<MM>(), c));
+        (int)H, (int)W, (const float*)u_src, (int)ld_us, (float*)u_dst, (int)ld_ud, (const float*)v_src, (int)ld_vs,
+        (float*)v_dst, (int)ld_vd, m.as<MM>(), c));
   });
   return check_launch("sg_advect_velocity_f32");
 }
@@ -142,12 +151,14 @@ int sg_advect_scalar_f32(int64_t H, int64_t W, const void* src, int64_t ld_src, 
   SG_REQUIRE(cell_size > 0.0, "cell_size must be positive");
   SG_REQUIRE(mask_mode == SG_MASK_OPEN || mask_mode == SG_MASK_RING || (mask_mode == SG_MASK_PLANES && is_fluid),
              "bad mask mode or missing is_fluid plane");
+  SG_REQUIRE((H + 1) * std::max(std::max(ld_src, ld_dst), std::max(ld_u, ld_v)) < ((int64_t)1 << 31),
+             "fields of 2^31 elements or more: use sg_advect_scalar");
   Masks m = make_masks(mask_mode, H, W, nullptr, 0, nullptr, 0, is_fluid, ld_fluid);
   const float c = (float)(dt / cell_size);
   SG_MASK_DISPATCH(mask_mode, {
     SG_LAUNCH(k_advect_scalar_f32<MM><<<grid2d_rows(W, H), block2d(), 0, as_stream(stream)>>>(
-        (int)H, (int)W, (const float*)src, ld_src, (float*)dst, ld_dst, (const float*)u, ld_u, (const float*)v, ld_v,
-        m.as<MM>(), c, (float)dissipation));
+        (int)H, (int)W, (const float*)src, (int)ld_src, (float*)dst, (int)ld_dst, (const float*)u, (int)ld_u,
+        (const float*)v, (int)ld_v, m.as<MM>(), c, (float)dissipation));
   });
   return check_launch("sg_advect_scalar_f32");
 }
