@@ -29,6 +29,15 @@ __device__ __forceinline__ float sample_rel(const float* __restrict__ f, int ld,
   oy = fminf(fmaxf(oy, -1048576.f), 1048576.f);
   const float fx = floorf(ox), fy = floorf(oy);
   const int x0 = bi + (int)fx, y0 = bj + (int)fy;
+  if ((unsigned)x0 < (unsigned)(cols - 1) && (unsigned)y0 < (unsigned)(rows - 1)) {
+    // the whole 2 x 2 stencil inside the grid (almost every sample): no clamping
+    const float* r0 = f + y0 * ld + x0;
+    const float tx = ox - fx, ty = oy - fy;
+    const float a = r0[0], b = r0[1], cc = r0[ld], d = r0[ld + 1];
+    const float c0 = fmaf(b - a, tx, a);
+    const float c1 = fmaf(d - cc, tx, cc);
+    return fmaf(c1 - c0, ty, c0);
+  }
   const bool inx = x0 >= 0 && x0 < cols - 1;
   const bool iny = y0 >= 0 && y0 < rows - 1;
   const int xa = min(max(x0, 0), cols - 1), xb = inx ? x0 + 1 : xa;
