@@ -231,8 +231,10 @@ class TimingProfiler:
     """Per-call durations of named scopes, in nanoseconds, measured on the device.
 
     ``with profiler.scope("simulation.pressure.solve"): ...`` records a CUDA event on the
-    current stream on entry and on exit; the duration is the device time between them.
-    Scopes whose name is not enabled cost nothing.
+    current stream on entry and on exit; the duration is the device time between them. An
+    enabled scope is also an NVTX range of the same name (the TIMINGS names of
+    profiling/config.py:228-242), so a timeline profiler shows the phases under the names
+    the reference reports them. Scopes whose name is not enabled cost nothing.
     """
 
     def __init__(self, enabled_timings: list[str] | None = None):
@@ -251,11 +253,13 @@ class TimingProfiler:
             yield
             return
         start, end = self._event(), self._event()
+        torch.cuda.nvtx.range_push(name)
         start.record()
         try:
             yield
         finally:
             end.record()
+            torch.cuda.nvtx.range_pop()
             self._pending.append((name, start, end))
 
     def _resolve(self) -> None:
