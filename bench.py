@@ -470,7 +470,7 @@ def run_ours(args):
 
     def make(dtype, precision, tol=TOL, remove_mean=False, inner=1):
         params = sg.GeometricMultigridParams(tol=tol, max_cycles=40, precision=precision, omega=OMEGA,
-                                             coarsest=COARSEST, fixed_cycles=args.fixed_cycles,
+                                             coarsest=args.coarsest, fixed_cycles=args.fixed_cycles,
                                              remove_mean=remove_mean, inner_cycles=inner)
         sim = sg.scenes.make_sim(sc, "geometric_multigrid", params, dtype=dtype, device=dev)
         # float32 states advect in the arithmetic chosen for the run; float64 states in the
@@ -946,6 +946,8 @@ def main():
                     help="arithmetic of the float32 state's advection: float32 (relative to the cell) or the "
                          "reference's float64 positions and weights (bit for bit)")
     ap.add_argument("--no-extras", action="store_true", help="skip the other workloads' sub-objects")
+    ap.add_argument("--coarsest", type=int, default=COARSEST,
+                    help="exact coarsest level side of the 2048^2 multigrid (cosine transform; 17..256)")
     ap.add_argument("--no-reference-numba", action="store_true",
                     help="reference arm: skip timing the reference's own Numba code beside the oracle port")
     ap.add_argument("--only", choices=["mixed", "fp64", "sor"], default=None,

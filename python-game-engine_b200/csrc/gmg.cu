@@ -386,7 +386,8 @@ __global__ void k_gmg_finalize_rel(const double* __restrict__ partial, int n, Gm
 // ---------------------------------------------------------------- single-block tail
 constexpr int kMaxLevels = 16;
 constexpr int kPinvMaxSide = 16;  // coarsest levels up to this side: dense pseudo-inverse
-constexpr int kDctMaxSide = 64;   // open-box coarsest levels up to this side: cosine transform
+constexpr int kDctMaxSide = 64;   // open-box coarsest levels up to this side: one-block cosine transform
+constexpr int kDctMultiMaxSide = 256;  // and up to this side: the transform as four tiled products
 
 // Exact solve of an open-box coarsest level by the discrete cosine transform. Its operator
 // (sum over open faces of e - e_nb, walls closed) is L_y (x) I + I (x) L_x, L the Laplacian
@@ -450,6 +451,61 @@ __global__ void __launch_bounds__(1024) k_gmg_coarse_dct(const T* __restrict__ b
     const int j = q / W, i = q - j * W;
     e[(int64_t)j * lde + i] = dot(X + j * W, 1, cx + i, W, W);
   }
+}
+
+// The same solve for coarsest levels above kDctMaxSide, as four products over many blocks:
+// X = B C_x^T, Y = (C_y X) / (lambda_y + lambda_x) with Y(0, 0) = 0, Z = C_y^T Y, e = Z C_x.
+// k_dct_gemm computes C (M x N) = op(A) (M x K) op(B) (K x N) on 32 x 32 output tiles
+// (256 threads, 2 x 2 outputs each, K in chunks of 32 through shared memory); op(A)(m, k) is
+// A[m * lda + k], or A[k * lda + m] with TA; op(B)(k, n) is B[k * ldb + n], or B[n * ldb + k]
+// with TB. EPI = 1 divides output (m, n) by ly[m] + lx[n] and zeroes (0, 0).
+constexpr int kDG = 32;
+template <typename T, bool TA, bool TB, int EPI>
+__global__ void __launch_bounds__(256) k_dct_gemm(int M, int N, int K, const T* __restrict__ A, int64_t lda,
+                                                  const T* __restrict__ B, int64_t ldb, T* __restrict__ C, int64_t ldc,
+                                                  const T* __restrict__ ly, const T* __restrict__ lx) {
+  __shared__ T As[kDG][kDG + 1];  // [k][m]
+  __shared__ T Bs[kDG][kDG + 1];  // [k][n]
+  const int m0 = blockIdx.y * kDG, n0 = blockIdx.x * kDG;
+  const int tid = threadIdx.x, tr = tid >> 4, tc = tid & 15;
+  T acc00 = (T)0, acc01 = (T)0, acc10 = (T)0, acc11 = (T)0;
+  for (int k0 = 0; k0 < K; k0 += kDG) {
+    for (int e = tid; e < kDG * kDG; e += 256) {
+      const int hi = e / kDG, lo = e - hi * kDG;  // lo runs along the contiguous index
+      {
+        const int m = TA ? lo : hi, k = TA ? hi : lo;
+        const int gm = m0 + m, gk = k0 + k;
+        As[k][m] = (gm < M && gk < K) ? (TA ? A[(int64_t)gk * lda + gm] : A[(int64_t)gm * lda + gk]) : (T)0;
+      }
+      {
+        const int n = TB ? hi : lo, k = TB ? lo : hi;
+        const int gn = n0 + n, gk = k0 + k;
+        Bs[k][n] = (gn < N && gk < K) ? (TB ? B[(int64_t)gn * ldb + gk] : B[(int64_t)gk * ldb + gn]) : (T)0;
+      }
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int k = 0; k < kDG; ++k) {
+      const T a0 = As[k][2 * tr], a1 = As[k][2 * tr + 1];
+      const T b0 = Bs[k][2 * tc], b1 = Bs[k][2 * tc + 1];
+      acc00 += a0 * b0;
+      acc01 += a0 * b1;
+      acc10 += a1 * b0;
+      acc11 += a1 * b1;
+    }
+    __syncthreads();
+  }
+  const T accs[2][2] = {{acc00, acc01}, {acc10, acc11}};
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const int gm = m0 + 2 * tr + u, gn = n0 + 2 * tc + v;
+      if (gm >= M || gn >= N) continue;
+      T val = accs[u][v];
+      if (EPI == 1) val = (gm == 0 && gn == 0) ? (T)0 : val / (ly[gm] + lx[gn]);
+      C[(int64_t)gm * ldc + gn] = val;
+    }
 }
 
 template <typename T>
@@ -750,6 +806,8 @@ struct sg_gmg_plan {
   // coarsest open-box level above kPinvMaxSide cells a side: exact solve by the cosine
   // transform (k_gmg_coarse_dct) from the tables in dct (C_x, C_y, eigenvalues)
   int coarse_dct = 0;
+  int coarse_dct_multi = 0;  // above kDctMaxSide: the four-product form (k_dct_gemm), scratch at off_dct_x
+  int64_t off_dct_x = 0;
   std::vector<double> dct;
   std::vector<float> dct_f;  // the same in float, for FP32 cycles
   int64_t off_dct = 0, dct_smem = 0;
@@ -1164,6 +1222,24 @@ template <typename T>
 static void cycle(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
   if (p->coarse_dct && k == (int)p->levels.size() - 1) {
     const Level& C = p->levels[k];
+    if (p->coarse_dct_multi) {
+      const int H = C.H, W = C.W;
+      const T* tab = ws_ptr<T>(p, p->off_dct);
+      const T* cx = tab;                          // cx[k W + i]
+      const T* cy = tab + 2 * (int64_t)W * W;      // cy[m H + j]
+      const T* lx = cy + (int64_t)H * H;
+      const T* ly = lx + W;
+      T* X = ws_ptr<T>(p, p->off_dct_x);
+      T* Y = X + (int64_t)H * W;
+      const dim3 g((W + kDG - 1) / kDG, (H + kDG - 1) / kDG);
+      SG_LAUNCH((k_dct_gemm<T, false, true, 0><<<g, 256, 0, s>>>(H, W, W, ws_ptr<T>(p, C.off_b), C.ld, cx, W, X, W,
+                                                                   nullptr, nullptr)));
+      SG_LAUNCH((k_dct_gemm<T, false, false, 1><<<g, 256, 0, s>>>(H, W, H, cy, H, X, W, Y, W, ly, lx)));
+      SG_LAUNCH((k_dct_gemm<T, true, false, 0><<<g, 256, 0, s>>>(H, W, H, cy, H, Y, W, X, W, nullptr, nullptr)));
+      SG_LAUNCH((k_dct_gemm<T, false, false, 0><<<g, 256, 0, s>>>(H, W, W, X, W, cx, W, ws_ptr<T>(p, C.off_e), C.ld,
+                                                                    nullptr, nullptr)));
+      return;
+    }
     SG_LAUNCH(k_gmg_coarse_dct<T><<<1, 1024, p->dct_smem, s>>>(ws_ptr<T>(p, C.off_b), C.ld, ws_ptr<T>(p, C.off_e), C.ld,
                                                                 C.H, C.W, ws_ptr<T>(p, p->off_dct)));
     return;
@@ -1400,7 +1476,7 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
   SG_REQUIRE(out, "null plan pointer");
   *out = nullptr;
   SG_REQUIRE(H >= 1 && W >= 1 && H <= (1 << 16) && W <= (1 << 16), "bad grid %lld x %lld", (long long)H, (long long)W);
-  SG_REQUIRE(coarsest >= 1 && coarsest <= kDctMaxSide, "coarsest must be in 1..%d", kDctMaxSide);
+  SG_REQUIRE(coarsest >= 1 && coarsest <= kDctMultiMaxSide, "coarsest must be in 1..%d", kDctMultiMaxSide);
   SG_REQUIRE(omega > 0.0 && omega < 2.0, "omega must be in (0, 2)");
   SG_REQUIRE(pre_sweeps >= 0 && post_sweeps >= 0 && pre_sweeps + post_sweeps >= 1, "need at least one smoothing sweep");
   SG_REQUIRE(pre_sweeps <= 16 && post_sweeps <= 16, "at most 16 sweeps per side");
@@ -1485,6 +1561,7 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
                   "lower coarsest", kPinvMaxSide);
     }
     p->coarse_dct = 1;
+    p->coarse_dct_multi = std::max(last.H, last.W) > kDctMaxSide ? 1 : 0;
     coarse_dct_tables(last.H, last.W, p->dct);
   } else {
     std::vector<uint8_t> lastcode = last.analytic ? pack_codes(fl, fu, fv, last.H, last.W) : last.code;
@@ -1520,8 +1597,9 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
   if (p->coarse_dct) {
     const Level& C = p->levels.back();
     p->tail_smem = 0;
-    p->dct_smem = (int64_t)(precision == SG_GMG_FP64 ? coarse_dct_smem<double>(C.H, C.W)
-                                                     : coarse_dct_smem<float>(C.H, C.W));
+    p->dct_smem = p->coarse_dct_multi ? 0
+                                      : (int64_t)(precision == SG_GMG_FP64 ? coarse_dct_smem<double>(C.H, C.W)
+                                                                           : coarse_dct_smem<float>(C.H, C.W));
   } else {
     p->tail_smem = (p->tail_open ? (int64_t)open_tail_layout(p->levels, p->tail_start).total
                                  : generic_elems(p->tail_start)) *
@@ -1566,6 +1644,10 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
   off = align256(off + (int64_t)p->pinv.size() * 8);
   p->off_dct = off;
   off = align256(off + (int64_t)p->dct.size() * 8);
+  if (p->coarse_dct_multi) {  // the products' two H x W intermediates
+    p->off_dct_x = off;
+    off = align256(off + 2 * (int64_t)p->levels.back().H * p->levels.back().W * (int64_t)cyc);
+  }
   dim3 g = grid_wide(p->W, p->H);
   p->n_partial = (int64_t)g.x * g.y;
   if (p->fused_ir) {
@@ -1620,10 +1702,11 @@ int sg_gmg_bind(sg_gmg_plan* plan, void* workspace, void* stream) {
                   "sg_gmg_bind cosine tables");
     }
     const int ds = (int)plan->dct_smem;
-    SG_CUDA_TRY(plan->precision == SG_GMG_FP64
-                    ? cudaFuncSetAttribute(k_gmg_coarse_dct<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ds)
-                    : cudaFuncSetAttribute(k_gmg_coarse_dct<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, ds),
-                "smem attr");
+    if (!plan->coarse_dct_multi)
+      SG_CUDA_TRY(plan->precision == SG_GMG_FP64
+                      ? cudaFuncSetAttribute(k_gmg_coarse_dct<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ds)
+                      : cudaFuncSetAttribute(k_gmg_coarse_dct<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, ds),
+                  "smem attr");
   }
   SG_CUDA_TRY(cudaMemsetAsync(plan->ws + plan->off_state, 0, sizeof(GmgState), s), "sg_gmg_bind state");
   // host vectors must outlive the asynchronous copies

@@ -123,6 +123,49 @@ def test_gmg_one_cycle_cosine_coarsest_vs_oracle(shape, cycle, precision):
     assert np.max(np.abs(got - pe)) <= tol * np.max(np.abs(pe))
 
 
+@pytest.mark.parametrize("shape,coarsest,cycle,precision", [
+    ((512, 512), 128, "V", "fp64"), ((1024, 768), 256, "V", "fp64"), ((300, 260), 80, "V", "fp64"),
+    ((300, 260), 80, "W", "fp64"), ((2048, 2048), 256, "V", "mixed"), ((1024, 768), 256, "V", "fp32"),
+    ((200, 176), 256, "V", "fp64")])
+def test_gmg_one_cycle_large_cosine_coarsest_vs_oracle(shape, coarsest, cycle, precision):
+    """coarsest above 64 (up to 256): the last level is solved exactly by the cosine transform
+    written as four tiled products over many blocks (k_dct_gemm); one cycle must equal the
+    oracle's cycle, whose coarsest solve is the same transform in float64 (scipy's orthonormal
+    DCT-II, checked against the dense pseudo-inverse in the oracle tests). Odd and rectangular
+    coarsest levels (75 x 65, 256 x 192) and a grid that is its own coarsest level (200 x 176)
+    included."""
+    H, W = shape
+    fmu, fmv, fl, div = _problem(H, W, False, 5)
+    alpha = -0.7
+    g = O.GMGOracle(fmu, fmv, fl, coarsest=coarsest, omega=OMEGA, cycle=cycle)
+    assert g.coarse_dct
+    pe = np.zeros((H, W))
+    g.vcycle(0, pe, alpha * div)
+    solver = sg.GeometricMultigridSolver()
+    p = torch.zeros((H, W), dtype=torch.float32 if precision == "fp32" else torch.float64, device="cuda")
+    solver(p, dev(div.astype(np.float64 if precision == "fp64" else np.float32)), sg.OPEN_BOX, sg.OPEN_BOX, 0.7,
+           1.0, 1.0, precision=precision, fixed_cycles=1, cycle=cycle, coarsest=coarsest, omega=OMEGA)
+    got = p.double().cpu().numpy()
+    tol = 1e-10 if precision == "fp64" else 2e-5
+    assert np.max(np.abs(got - pe)) <= tol * np.max(np.abs(pe))
+
+
+def test_gmg_large_cosine_coarsest_reaches_1e8_in_no_more_cycles():
+    """The 2048^2 scene's first solve to 1e-8 (mixed): an exact 256^2 coarsest level needs no
+    more V(2,2) cycles than the exact 32^2 one."""
+    sc = scenes.mixed_2048(steps=1)
+    cycles = {}
+    for coarsest in (32, 256):
+        params = sg.GeometricMultigridParams(tol=1e-8, precision="mixed", max_cycles=30, coarsest=coarsest,
+                                             omega=OMEGA)
+        sim = scenes.make_sim(sc, "geometric_multigrid", params, dtype=torch.float32)
+        sim.substep(sc.dt)
+        solver = sg.get_solver("geometric_multigrid", "cuda")
+        assert solver.converged and solver.last_relres <= 1e-8
+        cycles[coarsest] = solver.last_cycles
+    assert cycles[256] <= cycles[32], cycles
+
+
 @pytest.mark.parametrize("precision,obstacles", [("fp64", False), ("mixed", False), ("mixed", True)])
 def test_gmg_remove_mean_reaches_1e10(precision, obstacles):
     """An rhs whose sum is not zero (as float rounding leaves a divergence) has a constant part

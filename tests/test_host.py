@@ -124,13 +124,15 @@ def test_gmg_plan_with_obstacle_planes():
     L.load().sg_gmg_plan_destroy(h)
 
 
-@pytest.mark.parametrize("H,W,levels,last", [(2048, 2048, 7, (32, 32)), (1100, 1300, 7, (18, 21)),
-                                             (20, 30, 1, (20, 30)), (64, 64, 2, (32, 32))])
-def test_gmg_plan_cosine_coarsest(H, W, levels, last):
-    """coarsest=32 on an open box: the hierarchy stops at the first level <= 32 a side
-    (solved by the cosine transform)."""
+@pytest.mark.parametrize("H,W,levels,last,coarsest", [(2048, 2048, 7, (32, 32), 32), (1100, 1300, 7, (18, 21), 32),
+                                                      (20, 30, 1, (20, 30), 32), (64, 64, 2, (32, 32), 32),
+                                                      (2048, 2048, 4, (256, 256), 256),
+                                                      (1024, 768, 3, (256, 192), 256), (300, 260, 3, (75, 65), 80)])
+def test_gmg_plan_cosine_coarsest(H, W, levels, last, coarsest):
+    """coarsest 17..256 on an open box: the hierarchy stops at the first level <= coarsest a
+    side (solved by the cosine transform: one block up to 64 a side, tiled products above)."""
     lib = L.load()
-    rc, h = _plan(H, W, coarsest=32)
+    rc, h = _plan(H, W, coarsest=coarsest)
     assert rc == L.SG_OK
     try:
         assert lib.sg_gmg_num_levels(h) == levels
@@ -156,7 +158,7 @@ def test_gmg_cosine_coarsest_needs_open_box():
     assert "open box" in L.load().sg_last_error().decode()
 
 
-@pytest.mark.parametrize("kw", [dict(omega=2.5), dict(coarsest=0), dict(coarsest=65), dict(pre=0, post=0),
+@pytest.mark.parametrize("kw", [dict(omega=2.5), dict(coarsest=0), dict(coarsest=257), dict(pre=0, post=0),
                                 dict(cycle=3), dict(precision=9)])
 def test_gmg_plan_rejects_bad_parameters(kw):
     rc, h = _plan(64, 64, **kw)

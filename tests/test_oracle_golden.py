@@ -222,3 +222,18 @@ def test_oracle_substeps_with_obstacles_match_reference(name):
             for k, attr in (("density", "density"), ("u", "velocity_u"), ("v", "velocity_v"), ("p", "pressure"),
                             ("t", "temperature"), ("div", "divergence"), ("res", "pressure_residual")):
                 assert np.array_equal(getattr(sim, attr), d[f"{name}_s{step}_{k}"]), (step, k)
+
+
+def test_gmg_oracle_cosine_coarsest_equals_pseudo_inverse():
+    """The oracle's cosine-transform solve of a large open-box coarsest level (used above
+    64 x 64 cells, where a dense pseudo-inverse is too large) is the pseudo-inverse solution:
+    it solves A e = b - mean(b) to rounding and has zero mean."""
+    H, W = 72, 80
+    fmu, fmv = O.face_masks_from_solid(np.zeros((H, W), bool))
+    fl = O.is_fluid_from_faces(fmu, fmv)
+    g = O.GMGOracle(fmu, fmv, fl, coarsest=100)
+    assert g.coarse_dct and len(g.levels) == 1
+    b = np.random.default_rng(0).standard_normal((H, W))
+    e = g.coarse_solve(b)
+    assert np.max(np.abs((b - b.mean()) - O.gmg_apply(e, fl, fmu, fmv))) <= 1e-12 * np.max(np.abs(b))
+    assert abs(e.mean()) <= 1e-14 * np.max(np.abs(e))
