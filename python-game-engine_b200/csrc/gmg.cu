@@ -455,57 +455,70 @@ __global__ void __launch_bounds__(1024) k_gmg_coarse_dct(const T* __restrict__ b
 
 // The same solve for coarsest levels above kDctMaxSide, as four products over many blocks:
 // X = B C_x^T, Y = (C_y X) / (lambda_y + lambda_x) with Y(0, 0) = 0, Z = C_y^T Y, e = Z C_x.
-// k_dct_gemm computes C (M x N) = op(A) (M x K) op(B) (K x N) on 32 x 32 output tiles
-// (256 threads, 2 x 2 outputs each, K in chunks of 32 through shared memory); op(A)(m, k) is
-// A[m * lda + k], or A[k * lda + m] with TA; op(B)(k, n) is B[k * ldb + n], or B[n * ldb + k]
-// with TB. EPI = 1 divides output (m, n) by ly[m] + lx[n] and zeroes (0, 0).
-constexpr int kDG = 32;
+// k_dct_gemm computes C (M x N) = op(A) (M x K) op(B) (K x N) for K <= kDctMultiMaxSide: a
+// block of 256 threads owns a 16 x 16 output tile, stages the whole 16 x K panel of op(A) and
+// K x 16 panel of op(B) in shared memory with one round of coalesced loads (the latency of
+// these small products is the loads', not the arithmetic's), and each thread forms one output
+// with four partial sums. op(A)(m, k) is A[m * lda + k], or A[k * lda + m] with TA; op(B)(k, n)
+// is B[k * ldb + n], or B[n * ldb + k] with TB. EPI = 1 divides output (m, n) by
+// ly[m] + lx[n] and zeroes (0, 0).
+constexpr int kDT = 16;      // output tile side
+constexpr int kDP = kDT + 1;  // shared-memory pitch of the panels (conflict-free stores)
+template <typename T>
+static size_t dct_gemm_smem(int K) {
+  return (size_t)2 * K * kDP * sizeof(T);
+}
 template <typename T, bool TA, bool TB, int EPI>
-__global__ void __launch_bounds__(256) k_dct_gemm(int M, int N, int K, const T* __restrict__ A, int64_t lda,
-                                                  const T* __restrict__ B, int64_t ldb, T* __restrict__ C, int64_t ldc,
-                                                  const T* __restrict__ ly, const T* __restrict__ lx) {
-  __shared__ T As[kDG][kDG + 1];  // [k][m]
-  __shared__ T Bs[kDG][kDG + 1];  // [k][n]
-  const int m0 = blockIdx.y * kDG, n0 = blockIdx.x * kDG;
-  const int tid = threadIdx.x, tr = tid >> 4, tc = tid & 15;
-  T acc00 = (T)0, acc01 = (T)0, acc10 = (T)0, acc11 = (T)0;
-  for (int k0 = 0; k0 < K; k0 += kDG) {
-    for (int e = tid; e < kDG * kDG; e += 256) {
-      const int hi = e / kDG, lo = e - hi * kDG;  // lo runs along the contiguous index
-      {
-        const int m = TA ? lo : hi, k = TA ? hi : lo;
-        const int gm = m0 + m, gk = k0 + k;
-        As[k][m] = (gm < M && gk < K) ? (TA ? A[(int64_t)gk * lda + gm] : A[(int64_t)gm * lda + gk]) : (T)0;
-      }
-      {
-        const int n = TB ? hi : lo, k = TB ? lo : hi;
-        const int gn = n0 + n, gk = k0 + k;
-        Bs[k][n] = (gn < N && gk < K) ? (TB ? B[(int64_t)gn * ldb + gk] : B[(int64_t)gk * ldb + gn]) : (T)0;
-      }
+__global__ void __launch_bounds__(kDT* kDT) k_dct_gemm(int M, int N, int K, const T* __restrict__ A, int64_t lda,
+                                                       const T* __restrict__ B, int64_t ldb, T* __restrict__ C,
+                                                       int64_t ldc, const T* __restrict__ ly, const T* __restrict__ lx) {
+  extern __shared__ __align__(16) unsigned char dct_gemm_smem_raw[];
+  T* As = reinterpret_cast<T*>(dct_gemm_smem_raw);  // [k][m], pitch kDP
+  T* Bs = As + (size_t)K * kDP;                      // [k][n], pitch kDP
+  const int m0 = blockIdx.y * kDT, n0 = blockIdx.x * kDT;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < kDT * K; e += kDT * kDT) {
+    {
+      // TA: A[k * lda + m], contiguous in m; otherwise A[m * lda + k], contiguous in k
+      const int m = TA ? e % kDT : e / K, k = TA ? e / kDT : e % K;
+      const int gm = m0 + m;
+      As[k * kDP + m] = gm < M ? (TA ? A[(int64_t)k * lda + gm] : A[(int64_t)gm * lda + k]) : (T)0;
     }
-    __syncthreads();
-#pragma unroll 8
-    for (int k = 0; k < kDG; ++k) {
-      const T a0 = As[k][2 * tr], a1 = As[k][2 * tr + 1];
-      const T b0 = Bs[k][2 * tc], b1 = Bs[k][2 * tc + 1];
-      acc00 += a0 * b0;
-      acc01 += a0 * b1;
-      acc10 += a1 * b0;
-      acc11 += a1 * b1;
+    {
+      const int n = TB ? e / K : e % kDT, k = TB ? e % K : e / kDT;
+      const int gn = n0 + n;
+      Bs[k * kDP + n] = gn < N ? (TB ? B[(int64_t)gn * ldb + k] : B[(int64_t)k * ldb + gn]) : (T)0;
     }
-    __syncthreads();
   }
-  const T accs[2][2] = {{acc00, acc01}, {acc10, acc11}};
-#pragma unroll
-  for (int u = 0; u < 2; ++u)
-#pragma unroll
-    for (int v = 0; v < 2; ++v) {
-      const int gm = m0 + 2 * tr + u, gn = n0 + 2 * tc + v;
-      if (gm >= M || gn >= N) continue;
-      T val = accs[u][v];
-      if (EPI == 1) val = (gm == 0 && gn == 0) ? (T)0 : val / (ly[gm] + lx[gn]);
-      C[(int64_t)gm * ldc + gn] = val;
-    }
+  __syncthreads();
+  const int r = tid / kDT, c = tid % kDT;
+  T s0 = (T)0, s1 = (T)0, s2 = (T)0, s3 = (T)0;
+  int k = 0;
+  for (; k + 4 <= K; k += 4) {
+    s0 += As[k * kDP + r] * Bs[k * kDP + c];
+    s1 += As[(k + 1) * kDP + r] * Bs[(k + 1) * kDP + c];
+    s2 += As[(k + 2) * kDP + r] * Bs[(k + 2) * kDP + c];
+    s3 += As[(k + 3) * kDP + r] * Bs[(k + 3) * kDP + c];
+  }
+  for (; k < K; ++k) s0 += As[k * kDP + r] * Bs[k * kDP + c];
+  const int gm = m0 + r, gn = n0 + c;
+  if (gm >= M || gn >= N) return;
+  T val = (s0 + s1) + (s2 + s3);
+  if (EPI == 1) val = (gm == 0 && gn == 0) ? (T)0 : val / (ly[gm] + lx[gn]);
+  C[(int64_t)gm * ldc + gn] = val;
+}
+
+template <typename T>
+static int set_dct_gemm_smem() {
+  const int bytes = (int)dct_gemm_smem<T>(kDctMultiMaxSide);
+  cudaError_t e = cudaFuncSetAttribute(k_dct_gemm<T, false, true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_dct_gemm<T, false, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_dct_gemm<T, true, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_dct_gemm<T, false, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return e == cudaSuccess ? SG_OK : fail(SG_ERR_CUDA, "cosine-transform products: %s", cudaGetErrorString(e));
 }
 
 template <typename T>
@@ -1231,13 +1244,16 @@ static void cycle(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
       const T* ly = lx + W;
       T* X = ws_ptr<T>(p, p->off_dct_x);
       T* Y = X + (int64_t)H * W;
-      const dim3 g((W + kDG - 1) / kDG, (H + kDG - 1) / kDG);
-      SG_LAUNCH((k_dct_gemm<T, false, true, 0><<<g, 256, 0, s>>>(H, W, W, ws_ptr<T>(p, C.off_b), C.ld, cx, W, X, W,
-                                                                   nullptr, nullptr)));
-      SG_LAUNCH((k_dct_gemm<T, false, false, 1><<<g, 256, 0, s>>>(H, W, H, cy, H, X, W, Y, W, ly, lx)));
-      SG_LAUNCH((k_dct_gemm<T, true, false, 0><<<g, 256, 0, s>>>(H, W, H, cy, H, Y, W, X, W, nullptr, nullptr)));
-      SG_LAUNCH((k_dct_gemm<T, false, false, 0><<<g, 256, 0, s>>>(H, W, W, X, W, cx, W, ws_ptr<T>(p, C.off_e), C.ld,
-                                                                    nullptr, nullptr)));
+      const dim3 g((W + kDT - 1) / kDT, (H + kDT - 1) / kDT);
+      const size_t sw = dct_gemm_smem<T>(W), sh = dct_gemm_smem<T>(H);
+      SG_LAUNCH((k_dct_gemm<T, false, true, 0><<<g, kDT * kDT, sw, s>>>(H, W, W, ws_ptr<T>(p, C.off_b), C.ld, cx, W,
+                                                                         X, W, nullptr, nullptr)));
+      SG_LAUNCH((k_dct_gemm<T, false, false, 1><<<g, kDT * kDT, sh, s>>>(H, W, H, cy, H, X, W, Y, W, ly, lx)));
+      SG_LAUNCH((k_dct_gemm<T, true, false, 0><<<g, kDT * kDT, sh, s>>>(H, W, H, cy, H, Y, W, X, W, nullptr,
+                                                                         nullptr)));
+      SG_LAUNCH((k_dct_gemm<T, false, false, 0><<<g, kDT * kDT, sw, s>>>(H, W, W, X, W, cx, W,
+                                                                          ws_ptr<T>(p, C.off_e), C.ld, nullptr,
+                                                                          nullptr)));
       return;
     }
     SG_LAUNCH(k_gmg_coarse_dct<T><<<1, 1024, p->dct_smem, s>>>(ws_ptr<T>(p, C.off_b), C.ld, ws_ptr<T>(p, C.off_e), C.ld,
@@ -1702,6 +1718,10 @@ int sg_gmg_bind(sg_gmg_plan* plan, void* workspace, void* stream) {
                   "sg_gmg_bind cosine tables");
     }
     const int ds = (int)plan->dct_smem;
+    if (plan->coarse_dct_multi) {
+      const int rc = plan->precision == SG_GMG_FP64 ? set_dct_gemm_smem<double>() : set_dct_gemm_smem<float>();
+      if (rc != SG_OK) return rc;
+    }
     if (!plan->coarse_dct_multi)
       SG_CUDA_TRY(plan->precision == SG_GMG_FP64
                       ? cudaFuncSetAttribute(k_gmg_coarse_dct<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ds)
