@@ -477,17 +477,32 @@ __global__ void __launch_bounds__(kDT* kDT) k_dct_gemm(int M, int N, int K, cons
   T* Bs = As + (size_t)K * kDP;                      // [k][n], pitch kDP
   const int m0 = blockIdx.y * kDT, n0 = blockIdx.x * kDT;
   const int tid = threadIdx.x;
-  for (int e = tid; e < kDT * K; e += kDT * kDT) {
-    {
+  // every load of both panels is issued before the first store (K <= 256: at most 16 per
+  // panel and thread), so the block waits for one round trip, not sixteen
+  constexpr int kQ = kDctMultiMaxSide / kDT;
+  T va[kQ], vb[kQ];
+#pragma unroll
+  for (int q = 0; q < kQ; ++q) {
+    const int e = tid + q * kDT * kDT;
+    va[q] = vb[q] = (T)0;
+    if (e < kDT * K) {
       // TA: A[k * lda + m], contiguous in m; otherwise A[m * lda + k], contiguous in k
       const int m = TA ? e % kDT : e / K, k = TA ? e / kDT : e % K;
       const int gm = m0 + m;
-      As[k * kDP + m] = gm < M ? (TA ? A[(int64_t)k * lda + gm] : A[(int64_t)gm * lda + k]) : (T)0;
-    }
-    {
-      const int n = TB ? e / K : e % kDT, k = TB ? e % K : e / kDT;
+      if (gm < M) va[q] = TA ? A[(int64_t)k * lda + gm] : A[(int64_t)gm * lda + k];
+      const int n = TB ? e / K : e % kDT, k2 = TB ? e % K : e / kDT;
       const int gn = n0 + n;
-      Bs[k * kDP + n] = gn < N ? (TB ? B[(int64_t)gn * ldb + k] : B[(int64_t)k * ldb + gn]) : (T)0;
+      if (gn < N) vb[q] = TB ? B[(int64_t)gn * ldb + k2] : B[(int64_t)k2 * ldb + gn];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kQ; ++q) {
+    const int e = tid + q * kDT * kDT;
+    if (e < kDT * K) {
+      const int m = TA ? e % kDT : e / K, k = TA ? e / kDT : e % K;
+      As[k * kDP + m] = va[q];
+      const int n = TB ? e / K : e % kDT, k2 = TB ? e % K : e / kDT;
+      Bs[k2 * kDP + n] = vb[q];
     }
   }
   __syncthreads();
