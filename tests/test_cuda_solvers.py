@@ -125,7 +125,8 @@ def test_gmg_one_cycle_cosine_coarsest_vs_oracle(shape, cycle, precision):
 
 @pytest.mark.parametrize("shape,coarsest,cycle,precision", [
     ((512, 512), 128, "V", "fp64"), ((1024, 768), 256, "V", "fp64"), ((300, 260), 80, "V", "fp64"),
-    ((300, 260), 80, "W", "fp64"), ((2048, 2048), 256, "V", "mixed"), ((1024, 768), 256, "V", "fp32"),
+    ((300, 260), 80, "W", "fp64"), ((2048, 2048), 256, "V", "mixed"), ((2048, 2048), 128, "V", "mixed"),
+    ((2048, 2048), 128, "V", "fp64"), ((1024, 768), 256, "V", "fp32"),
     ((200, 176), 256, "V", "fp64")])
 def test_gmg_one_cycle_large_cosine_coarsest_vs_oracle(shape, coarsest, cycle, precision):
     """coarsest above 64 (up to 256): the last level is solved exactly by the cosine transform

@@ -1,5 +1,5 @@
 """The 2048^2 four-source scene over 20 substeps: the mixed-precision path (float32 state,
-FP32 V(2,2) cycles in FP64 iterative refinement to 1e-8, 32^2 exact coarsest) against the
+FP32 V(2,2) cycles in FP64 iterative refinement to 1e-8, 128^2 exact coarsest) against the
 all-FP64 GPU path and against the CPU oracle (the reference's kernels restated in C with the
 same multigrid, mixed precision, to 1e-8).
 
@@ -49,7 +49,7 @@ def oracle_fields():
     sc = sg.scenes.mixed_2048(steps=STEPS)
     fmu, fmv = O.face_masks_from_solid(np.zeros((sc.H, sc.W), bool))
     fl = O.is_fluid_from_faces(fmu, fmv)
-    gmg = O.GMGOracle(fmu, fmv, fl, coarsest=32, omega=1.3)
+    gmg = O.GMGOracle(fmu, fmv, fl, coarsest=128, omega=1.3)
     rec = []
 
     def solver(p, div, fmu_, fmv_, rho, h, dt, **_):
@@ -70,7 +70,7 @@ def oracle_fields():
 
 def _run(dtype, precision, arithmetic="reference"):
     sc = sg.scenes.mixed_2048(steps=STEPS)
-    params = sg.GeometricMultigridParams(tol=TOL, max_cycles=40, precision=precision, omega=1.3, coarsest=32)
+    params = sg.GeometricMultigridParams(tol=TOL, max_cycles=40, precision=precision, omega=1.3, coarsest=128)
     sim = sg.scenes.make_sim(sc, "geometric_multigrid", params, dtype=dtype)
     sim.advection_arithmetic = arithmetic
     name, norms = recording("geometric_multigrid")
