@@ -613,8 +613,8 @@ def run_ours(args):
             for _ in range(2):
                 sim.substep(sc.dt)
             torch.cuda.synchronize()
-        d = [e.device_time_total for e in prof.key_averages() if "k_gmg_post_final_reg" in e.key]
-        n = [e.count for e in prof.key_averages() if "k_gmg_post_final_reg" in e.key]
+        d = [e.device_time_total for e in prof.key_averages() if "k_gmg_post_final" in e.key]
+        n = [e.count for e in prof.key_averages() if "k_gmg_post_final" in e.key]
         if d and sum(n):
             in_graph_ms = sum(d) / sum(n) / 1e3
     except Exception:  # the trace is a cross-check; the events above are the figure
@@ -626,7 +626,7 @@ def run_ours(args):
     post_bytes = 45 * H0 * W0
     pre_bytes = 9 * H0 * W0
     achieved = post_bytes / (post_ms / 1e3) / 1e9
-    traffic = _measured_traffic("k_gmg_post_final_reg")
+    traffic = _measured_traffic("k_gmg_post_final_stage")
     # ---- error of the mixed path against the all-FP64 GPU path, same scene and steps
     errors = compare_fp64(sg, sc, make, 5)
     # ---- all-FP64 GPU path at the same residual
@@ -698,7 +698,7 @@ def run_ours(args):
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h + 8},
         "gpu_launches": int(launches),
-        "roofline": {"kernel": "k_gmg_post_final_reg<float,double> (fine level: post-smoothing + correction + "
+        "roofline": {"kernel": "k_gmg_post_final_stage<float,double> (fine level: post-smoothing + correction + "
                                "residual)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                      "alg_bytes_per_launch": post_bytes, "avg_launch_ms": post_ms,

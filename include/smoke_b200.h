@@ -405,6 +405,12 @@ int sg_gmg_smooth_async(sg_gmg_plan* plan, int level, int sweeps, void* stream);
  * enough to fill the GPU): pre-smoothing + restriction in one launch, post-smoothing +
  * correction of p + next residual in another. */
 int sg_gmg_fine_fused(const sg_gmg_plan* plan);
+/* How the plan solves its coarsest level exactly: 0 dense pseudo-inverse, 1 cosine transform
+ * in one block, 2 cosine transform as four tiled products, 3 cosine transform as two launches
+ * streaming their operands into shared memory with bulk asynchronous copies (chosen at
+ * sg_gmg_bind when the level's rows are whole 16-byte units); -1 for a NULL plan. No
+ * counterpart in the reference. */
+int sg_gmg_coarse_solve_kind(const sg_gmg_plan* plan);
 /* One launch of a fused fine-level kernel on the bound workspace, whatever it holds
  * (which = 0: pre kernel; 1: post kernel, which adds its correction to p, ld_p >= W, in the
  * plan's fine precision). Exposed for timing the solver's dominant kernels in isolation;

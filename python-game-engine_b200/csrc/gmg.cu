@@ -24,6 +24,7 @@
 #include <cstring>
 #include <vector>
 
+#include "bulk_copy.cuh"
 #include "common.cuh"
 
 namespace sg {
@@ -59,8 +60,8 @@ struct GmgState {
   double alpha;
   int cycles;
   int max_cycles;
-  int status;  // 0 running, 1 converged, 2 cycle cap reached, 3 non-finite residual
-  int pad;
+  int status;  // 0 running, 1 converged, 2 cycle cap reached, 3 non-finite residual, 4 device error
+  int dev_error;  // non-zero: a kernel's bounded wait gave up (kDevErr* code); the solve stops
   long long total_cycles;  // cycles run since the plan was bound (all solves)
   long long solves;
   long long failures;      // solves that ended at the cycle cap or on a non-finite residual
@@ -371,7 +372,7 @@ __device__ void finalize_rel_state(double s, GmgState* st, cudaGraphConditionalH
   st->relres = rel;
   if (c < kHist) st->history[c] = rel;
   bool finite = (rel == rel) && !isinf(rel);
-  int status = !finite ? 3 : (rel <= st->tol ? 1 : (c >= st->max_cycles ? 2 : 0));
+  int status = st->dev_error ? 4 : (!finite ? 3 : (rel <= st->tol ? 1 : (c >= st->max_cycles ? 2 : 0)));
   st->status = status;
   if (status >= 2) st->failures += 1;
   if (use_handle) cudaGraphSetConditional(h, status == 0 ? 1u : 0u);
@@ -534,6 +535,203 @@ static int set_dct_gemm_smem() {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_dct_gemm<T, false, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   return e == cudaSuccess ? SG_OK : fail(SG_ERR_CUDA, "cosine-transform products: %s", cudaGetErrorString(e));
+}
+
+// The same solve in two launches that stream the operands through shared memory, for
+// coarsest levels whose rows are whole 16-byte units (W * sizeof(T) % 16 == 0):
+//   forward (one block per kDsRB spectral rows m): T1 = C_y[m, :] B, T2 = T1 C_x^T,
+//     Y = T2 / (lambda_y[m] + lambda_x) with Y(0, 0) = 0, X[m, :] = Y C_x;
+//   inverse (one block per kDsRB output rows j): e[j, :] = sum_m C_y[m, j] X[m, :].
+// Every product here has one streamed operand whose rows are W long (B, C_x^T, C_x, X) and a
+// small left factor held in shared memory ([k][r], the block's kDsRB rows side by side), so a
+// launch is one stream of rows: warp 0 issues bulk copies of kDsKC rows per chunk into a ring
+// of `ns` slots sized to keep most of the stream in flight. A thread owns one column c and
+// all kDsRB rows (one vector load of the left factor feeds kDsRB FMAs); the NKG thread groups
+// of a block take every NKG-th streamed row and their partial sums meet in shared memory at
+// the end of each product. The four products of k_dct_gemm become two launches, and the
+// intermediates T1 / T2 never leave shared memory. A wait that gives up sets st->dev_error.
+constexpr int kDsRB = 4;                   // rows per block
+constexpr int kDsKC = 32;                  // streamed rows per chunk
+constexpr int kDsMaxSlots = 32;            // mbarriers reserved at the start of shared memory
+constexpr int kDsSmemBudget = 220 * 1024;  // bytes of shared memory per block
+constexpr int kDevErrBulkWait = 1;
+
+struct DctStreamLayout {
+  int ns;           // ring slots
+  size_t off_left;  // left factors: L0 (max(H, W) x kDsRB), L1 and L2 (W x kDsRB)
+  size_t off_red;   // partial sums of the thread groups: 3 x kDsRB x W
+  size_t off_ring;  // ns x kDsKC x W
+  size_t bytes;
+};
+
+// The ring takes what the budget leaves: when the whole stream fits (float32 up to ~128^2),
+// every chunk has its own slot and the launch needs no slot reuse and no per-chunk barrier.
+template <typename T>
+__host__ __device__ inline DctStreamLayout dct_stream_layout(int H, int W) {
+  DctStreamLayout L;
+  const size_t slot = (size_t)kDsKC * W * sizeof(T);
+  const int chunks = (H + kDsKC - 1) / kDsKC + 2 * ((W + kDsKC - 1) / kDsKC);
+  L.off_left = 8 * kDsMaxSlots;
+  L.off_red = L.off_left + ((size_t)(H > W ? H : W) + 2 * (size_t)W) * kDsRB * sizeof(T);
+  L.off_ring = (L.off_red + (size_t)3 * kDsRB * W * sizeof(T) + 127) & ~(size_t)127;
+  const size_t room = kDsSmemBudget > L.off_ring ? kDsSmemBudget - L.off_ring : 0;
+  int ns = (int)(room / slot);
+  ns = ns < 2 ? 2 : ns;
+  ns = ns > chunks ? chunks : ns;
+  ns = ns > kDsMaxSlots ? kDsMaxSlots : ns;
+  L.ns = ns;
+  L.bytes = L.off_ring + (size_t)ns * slot;
+  return L;
+}
+
+template <typename T>
+__device__ __forceinline__ void load_rows4(const T* __restrict__ p, T (&v)[kDsRB]) {
+  static_assert(kDsRB == 4, "four rows per block");
+  if constexpr (sizeof(T) == 4) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+  } else {
+    const double2 q0 = *reinterpret_cast<const double2*>(p);
+    const double2 q1 = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = q0.x, v[1] = q0.y, v[2] = q1.x, v[3] = q1.y;
+  }
+}
+
+// NKG thread groups of roundup32(W) threads (blockDim = NKG * roundup32(W) <= 256). INVERSE:
+// the second launch. b: the level's rhs (row stride ldb); X: H x W scratch (row stride W);
+// tab: the tables of k_gmg_coarse_dct.
+template <typename T, int NKG, bool INVERSE>
+__global__ void __launch_bounds__(256) k_dct_stream(int H, int W, const T* __restrict__ b, int64_t ldb,
+                                                    const T* __restrict__ tab, T* __restrict__ X, T* __restrict__ e,
+                                                    int64_t lde, GmgState* __restrict__ st) {
+  extern __shared__ __align__(128) unsigned char ds_smem[];
+  const DctStreamLayout lay = dct_stream_layout<T>(H, W);
+  uint64_t* full = reinterpret_cast<uint64_t*>(ds_smem);
+  T* L0 = reinterpret_cast<T*>(ds_smem + lay.off_left);  // [k][r], k < max(H, W)
+  T* L1 = L0 + (size_t)(H > W ? H : W) * kDsRB;          // [i][r], i < W
+  T* L2 = L1 + (size_t)W * kDsRB;                        // [k][r], k < W
+  T* red = reinterpret_cast<T*>(ds_smem + lay.off_red);  // [group - 1][r][c]
+  T* ring = reinterpret_cast<T*>(ds_smem + lay.off_ring);
+  const T* cx = tab;                   // cx[k W + i]
+  const T* cxt = cx + (int64_t)W * W;  // cxt[i W + k]
+  const T* cy = cxt + (int64_t)W * W;  // cy[m H + j]
+  const T* lx = cy + (int64_t)H * H;
+  const T* ly = lx + W;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int cw = (W + 31) & ~31;
+  const int c = tid % cw, kg = tid / cw;  // column and thread group
+  const int r0 = blockIdx.x * kDsRB;      // the block's first row (m forward, j inverse)
+  const int ns = lay.ns;
+  // phases: forward streams B (H rows), C_x^T (W rows), C_x (W rows); inverse streams X (H)
+  auto nrows = [&](int q) { return q == 0 ? H : W; };
+  auto nch = [&](int q) { return (nrows(q) + kDsKC - 1) / kDsKC; };
+  const int total = INVERSE ? nch(0) : nch(0) + 2 * nch(1);
+  const uint32_t row_bytes = (uint32_t)W * sizeof(T);
+  // warp 0: chunk ch into slot ch % ns. Lane 0 arrives with the chunk's byte count; the
+  // copies (one for a contiguous chunk, else one per row from lanes 0 .. nr - 1) may land
+  // before that arrival: the phase cannot complete while the arrival is pending.
+  auto issue = [&](int ch) {
+    const int lane = tid & 31;
+    int q = 0, k = ch;
+    while (k >= nch(q)) k -= nch(q++);
+    const int row0 = k * kDsKC;
+    const int nr = min(kDsKC, nrows(q) - row0);
+    const T* src = INVERSE ? X : (q == 0 ? b : (q == 1 ? cxt : cx));
+    const int64_t ld = (!INVERSE && q == 0) ? ldb : (int64_t)W;
+    uint64_t* bar = full + ch % ns;
+    T* dst = ring + (size_t)(ch % ns) * kDsKC * W;
+    if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)nr * row_bytes);
+    if (ld == W) {
+      if (lane == 0) bulk_g2s(dst, src + (int64_t)row0 * W, (uint32_t)nr * row_bytes, bar);
+    } else if (lane < nr) {
+      bulk_g2s(dst + (size_t)lane * W, src + (int64_t)(row0 + lane) * ld, row_bytes, bar);
+    }
+  };
+  if (tid == 0) {
+    for (int s = 0; s < ns; ++s) mbar_init(full + s, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (tid < 32)
+    for (int ch = 0; ch < ns && ch < total; ++ch) issue(ch);
+  // the first left factor: forward C_y[r0 + r, j] at L0[j][r]; inverse C_y[m, r0 + r] at L0[m][r]
+  for (int q = tid; q < H * kDsRB; q += nt) {
+    const int k = q / kDsRB, r = q - k * kDsRB;
+    const int row = r0 + r;
+    L0[q] = row < H ? (INVERSE ? cy[(int64_t)k * H + row] : cy[(int64_t)row * H + k]) : (T)0;
+  }
+  __syncthreads();
+  bool ok = true;
+  T acc[kDsRB];
+#pragma unroll
+  for (int r = 0; r < kDsRB; ++r) acc[r] = (T)0;
+  int q = 0, kq = 0;  // phase of the current chunk and its index within the phase
+  for (int ch = 0; ch < total; ++ch) {
+    if (!mbar_wait(full + ch % ns, (uint32_t)((ch / ns) & 1))) ok = false;
+    const int row0 = kq * kDsKC;
+    const int nr = min(kDsKC, nrows(q) - row0);
+    const T* left = (q == 0 ? L0 : (q == 1 ? L1 : L2)) + (size_t)row0 * kDsRB;
+    const T* slot = ring + (size_t)(ch % ns) * kDsKC * W;
+    if (c < W) {
+      if (nr == kDsKC) {
+#pragma unroll
+        for (int tt = 0; tt < kDsKC / NKG; ++tt) {
+          const int t = tt * NKG + kg;
+          const T v = slot[(size_t)t * W + c];
+          T l[kDsRB];
+          load_rows4(left + t * kDsRB, l);
+#pragma unroll
+          for (int r = 0; r < kDsRB; ++r) acc[r] += l[r] * v;
+        }
+      } else {
+        for (int t = kg; t < nr; t += NKG) {
+          const T v = slot[(size_t)t * W + c];
+          T l[kDsRB];
+          load_rows4(left + t * kDsRB, l);
+#pragma unroll
+          for (int r = 0; r < kDsRB; ++r) acc[r] += l[r] * v;
+        }
+      }
+    }
+    if (++kq == nch(q)) {  // the phase's products are complete: sum the groups, epilogue
+      if (NKG > 1) {
+        if (kg > 0 && c < W) {
+#pragma unroll
+          for (int r = 0; r < kDsRB; ++r) red[((size_t)(kg - 1) * kDsRB + r) * W + c] = acc[r];
+        }
+        __syncthreads();
+      }
+      if (kg == 0 && c < W) {
+#pragma unroll
+        for (int r = 0; r < kDsRB; ++r) {
+          T v = acc[r];
+#pragma unroll
+          for (int g = 1; g < NKG; ++g) v += red[((size_t)(g - 1) * kDsRB + r) * W + c];
+          const int row = r0 + r;
+          if (INVERSE) {
+            if (row < H) e[(int64_t)row * lde + c] = v;
+          } else if (q == 0) {
+            L1[c * kDsRB + r] = v;
+          } else if (q == 1) {
+            L2[c * kDsRB + r] = (row == 0 && c == 0) || row >= H ? (T)0 : v / (ly[row < H ? row : 0] + lx[c]);
+          } else if (row < H) {
+            X[(int64_t)row * W + c] = v;
+          }
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < kDsRB; ++r) acc[r] = (T)0;
+      ++q;
+      kq = 0;
+    }
+    if (kq == 0 || ns < total) __syncthreads();  // a left factor written / the slot consumed
+    if (tid < 32 && ch + ns < total) issue(ch + ns);
+  }
+  if (!ok) {
+    atomicExch(&st->dev_error, kDevErrBulkWait);
+    // let copies still in flight land before the block's shared memory is released
+    for (int ch = total - ns < 0 ? 0 : total - ns; ch < total; ++ch) mbar_wait(full + ch % ns, (uint32_t)((ch / ns) & 1));
+  }
 }
 
 template <typename T>
@@ -813,6 +1011,7 @@ __global__ void __launch_bounds__(kRX * kRY) k_gmg_residual_restrict_tiled(const
 #include "gmg_tiled.cuh"
 #include "gmg_tail_open.cuh"
 #include "gmg_regtile.cuh"
+#include "gmg_regtile_stage.cuh"
 
 // ---------------------------------------------------------------- plan
 struct Level {
@@ -835,6 +1034,8 @@ struct sg_gmg_plan {
   // transform (k_gmg_coarse_dct) from the tables in dct (C_x, C_y, eigenvalues)
   int coarse_dct = 0;
   int coarse_dct_multi = 0;  // above kDctMaxSide: the four-product form (k_dct_gemm), scratch at off_dct_x
+  int coarse_dct_stream = 0;  // ... run as the two streaming launches (k_dct_stream), decided at bind
+  int64_t dct_stream_smem = 0;
   int64_t off_dct_x = 0;
   std::vector<double> dct;
   std::vector<float> dct_f;  // the same in float, for FP32 cycles
@@ -1203,6 +1404,16 @@ static void launch_post_final(const sg_gmg_plan* p, TP* pp, int64_t ldp, cudaStr
   const Level& L = p->levels[0];
   const Level& C = p->levels[1];
   TP* r64 = p->off_r64 ? (TP*)(p->ws + p->off_r64) : nullptr;
+  // p and r64 staged in shared memory by bulk copies when every owned row of theirs starts on
+  // a 16-byte boundary (the workspace rows always do; the caller's p must)
+  const bool staged = ((uintptr_t)pp % 16) == 0 && ((size_t)ldp * sizeof(TP)) % 16 == 0 &&
+                      ((uintptr_t)p->ws % 16) == 0 && ((size_t)L.ld * sizeof(TP)) % 16 == 0;
+  if (staged) {
+    SG_LAUNCH(k_gmg_post_final_stage<TC, TP, SW, RPT, NW, MB><<<post_final_grid<TC>(p), 32 * NW, 0, s>>>(
+        ws_ptr<TC>(p, L.off_e2), ws_ptr<TC>(p, L.off_b), ws_ptr<TC>(p, p->off_b2), state_ptr(p), L.ld, L.H, L.W,
+        ws_ptr<TC>(p, C.off_e), C.ld, C.H, C.W, (TC)p->omega, pp, ldp, r64, (double*)(p->ws + p->off_partial)));
+    return;
+  }
   SG_LAUNCH(k_gmg_post_final_reg<TC, TP, SW, RPT, NW, MB><<<post_final_grid<TC>(p), 32 * NW, 0, s>>>(
       ws_ptr<TC>(p, L.off_e2), ws_ptr<TC>(p, L.off_b), ws_ptr<TC>(p, p->off_b2), state_ptr(p), L.ld, L.H, L.W,
       ws_ptr<TC>(p, C.off_e), C.ld, C.H, C.W, (TC)p->omega, pp, ldp, r64, (double*)(p->ws + p->off_partial)));
@@ -1245,11 +1456,74 @@ static int set_tiled_smem_limits() {
   return SG_OK;
 }
 
+// Thread groups of k_dct_stream for a level W cells wide (at most 256 threads a block).
+static int dct_stream_groups(int W) {
+  const int cw = (W + 31) / 32 * 32;
+  return cw <= 64 ? 4 : (cw <= 128 ? 2 : 1);
+}
+
+// The streaming form of the coarsest cosine transform applies when every streamed row (of B,
+// the tables and the scratch) starts and ends on 16-byte boundaries and its shared memory
+// fits one block; otherwise the four-product form stays. Called at bind (the workspace
+// address is known then).
+template <typename T>
+static int choose_dct_stream(sg_gmg_plan* p) {
+  const Level& C = p->levels.back();
+  const DctStreamLayout lay = dct_stream_layout<T>(C.H, C.W);
+  const bool aligned = ((size_t)C.W * sizeof(T)) % 16 == 0 && ((size_t)C.ld * sizeof(T)) % 16 == 0 &&
+                       ((uintptr_t)p->ws % 16) == 0;
+  p->coarse_dct_stream = 0;
+  if (!aligned || lay.bytes > 220 * 1024) return SG_OK;
+  const int bytes = (int)lay.bytes;
+  cudaError_t e = cudaSuccess;
+#define SG_DS_ATTR(NKG)                                                                                         \
+  if (e == cudaSuccess)                                                                                         \
+    e = cudaFuncSetAttribute(k_dct_stream<T, NKG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);  \
+  if (e == cudaSuccess)                                                                                         \
+    e = cudaFuncSetAttribute(k_dct_stream<T, NKG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  switch (dct_stream_groups(C.W)) {
+    case 4: SG_DS_ATTR(4) break;
+    case 2: SG_DS_ATTR(2) break;
+    default: SG_DS_ATTR(1) break;
+  }
+#undef SG_DS_ATTR
+  if (e != cudaSuccess) return fail(SG_ERR_CUDA, "cosine-transform stream smem: %s", cudaGetErrorString(e));
+  p->coarse_dct_stream = 1;
+  p->dct_stream_smem = bytes;
+  return SG_OK;
+}
+
+template <typename T, int NKG>
+static void dct_stream_launch_g(const sg_gmg_plan* p, const Level& C, cudaStream_t s) {
+  const T* tab = ws_ptr<T>(p, p->off_dct);
+  T* X = ws_ptr<T>(p, p->off_dct_x);
+  const int cw = (C.W + 31) / 32 * 32;
+  const dim3 g((C.H + kDsRB - 1) / kDsRB), b(cw * NKG);
+  const size_t sm = (size_t)p->dct_stream_smem;
+  SG_LAUNCH((k_dct_stream<T, NKG, false><<<g, b, sm, s>>>(C.H, C.W, ws_ptr<T>(p, C.off_b), C.ld, tab, X, nullptr, 0,
+                                                          state_ptr(p))));
+  SG_LAUNCH((k_dct_stream<T, NKG, true><<<g, b, sm, s>>>(C.H, C.W, nullptr, 0, tab, X, ws_ptr<T>(p, C.off_e), C.ld,
+                                                         state_ptr(p))));
+}
+
+template <typename T>
+static void dct_stream_launch(const sg_gmg_plan* p, const Level& C, cudaStream_t s) {
+  switch (dct_stream_groups(C.W)) {
+    case 4: dct_stream_launch_g<T, 4>(p, C, s); break;
+    case 2: dct_stream_launch_g<T, 2>(p, C, s); break;
+    default: dct_stream_launch_g<T, 1>(p, C, s); break;
+  }
+}
+
 // One cycle on level k for A_k e_k = b_k; zero_init: start from e_k = 0.
 template <typename T>
 static void cycle(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
   if (p->coarse_dct && k == (int)p->levels.size() - 1) {
     const Level& C = p->levels[k];
+    if (p->coarse_dct_stream) {
+      dct_stream_launch<T>(p, C, s);
+      return;
+    }
     if (p->coarse_dct_multi) {
       const int H = C.H, W = C.W;
       const T* tab = ws_ptr<T>(p, p->off_dct);
@@ -1736,6 +2010,8 @@ int sg_gmg_bind(sg_gmg_plan* plan, void* workspace, void* stream) {
     if (plan->coarse_dct_multi) {
       const int rc = plan->precision == SG_GMG_FP64 ? set_dct_gemm_smem<double>() : set_dct_gemm_smem<float>();
       if (rc != SG_OK) return rc;
+      const int rc2 = plan->precision == SG_GMG_FP64 ? choose_dct_stream<double>(plan) : choose_dct_stream<float>(plan);
+      if (rc2 != SG_OK) return rc2;
     }
     if (!plan->coarse_dct_multi)
       SG_CUDA_TRY(plan->precision == SG_GMG_FP64
@@ -1845,6 +2121,7 @@ int sg_gmg_solve(sg_gmg_plan* plan, void* p, int64_t ld_p, const void* div, int6
   if (cycles_out) *cycles_out = cycles;
   if (relres_out) *relres_out = rel;
   if (status == 3) return fail(SG_ERR_NONFINITE, "non-finite residual after %d cycles", cycles);
+  if (status == 4) return fail(SG_ERR_CUDA, "a bounded device wait of the solve gave up (bulk copy never landed)");
   if (status != 1)
     return fail(SG_ERR_NOT_CONVERGED, "relative residual %.3e > tol %.3e after %d cycles", rel, tol, cycles);
   return SG_OK;
@@ -1924,6 +2201,12 @@ int sg_gmg_smooth_async(sg_gmg_plan* plan, int level, int sweeps, void* stream) 
 }
 
 int sg_gmg_fine_fused(const sg_gmg_plan* plan) { return plan ? plan->fused_ir : 0; }
+
+int sg_gmg_coarse_solve_kind(const sg_gmg_plan* plan) {
+  if (!plan) return -1;
+  if (!plan->coarse_dct) return 0;
+  return plan->coarse_dct_stream ? 3 : (plan->coarse_dct_multi ? 2 : 1);
+}
 
 int sg_gmg_fine_kernel_async(sg_gmg_plan* plan, int which, void* p, int64_t ld_p, void* stream) {
   SG_REQUIRE(plan && plan->ws, "plan not bound to a workspace");

@@ -321,6 +321,12 @@ class GMGPlan:
     def tail_start(self):
         return L.load().sg_gmg_tail_start(self.handle)
 
+    def level_shape(self, level):
+        """(H, W) of one level of the hierarchy (0 is the fine grid)."""
+        h, w = ctypes.c_int(0), ctypes.c_int(0)
+        L.call("sg_gmg_level_shape", self.handle, int(level), ctypes.byref(h), ctypes.byref(w))
+        return h.value, w.value
+
     def relres_async(self, dst, stream=None):
         """Enqueue a copy of the last solve's relative residual into `dst` (one float64,
         pinned host or CUDA tensor) on `stream`; no synchronisation."""
@@ -329,6 +335,13 @@ class GMGPlan:
     def fine_fused(self):
         """True when the fine level runs the fused register-tiled pre/post kernels."""
         return bool(L.load().sg_gmg_fine_fused(self.handle))
+
+    COARSE_SOLVE_KINDS = ("pseudo-inverse", "cosine transform (one block)", "cosine transform (four products)",
+                          "cosine transform (two streaming launches)")
+
+    def coarse_solve_kind(self):
+        """How the coarsest level is solved (one of COARSE_SOLVE_KINDS)."""
+        return self.COARSE_SOLVE_KINDS[L.load().sg_gmg_coarse_solve_kind(self.handle)]
 
     def fine_kernel_async(self, which, pressure=None):
         """Launch the fused fine-level pre (0) or post (1) kernel once on the workspace as it
@@ -374,6 +387,9 @@ class GeometricMultigridSolver:
             if status == 3:
                 self._last = (cycles, rel, False)
                 raise L.SmokeCudaError(f"multigrid: non-finite residual after {cycles} cycles")
+            if status == 4:
+                self._last = (cycles, rel, False)
+                raise L.SmokeCudaError("multigrid: a bounded device wait gave up (a bulk copy never landed)")
             self._last = (cycles, rel, status == 1)
         return self._last
 

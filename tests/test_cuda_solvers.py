@@ -149,6 +149,11 @@ def test_gmg_one_cycle_large_cosine_coarsest_vs_oracle(shape, coarsest, cycle, p
     got = p.double().cpu().numpy()
     tol = 1e-10 if precision == "fp64" else 2e-5
     assert np.max(np.abs(got - pe)) <= tol * np.max(np.abs(pe))
+    # rows of whole 16-byte units run the two streaming launches, the rest the four products
+    plan = solver.current_plan()
+    Wc = plan.level_shape(plan.num_levels - 1)[1]
+    streams = (Wc * (8 if precision == "fp64" else 4)) % 16 == 0
+    assert plan.coarse_solve_kind() == plan.COARSE_SOLVE_KINDS[3 if streams else 2]
 
 
 def test_gmg_large_cosine_coarsest_reaches_1e8_in_no_more_cycles():
@@ -339,3 +344,32 @@ def test_jacobi_multi_sweep_tiles_vs_oracle(dtype, shape, iters):
     got = dev(p0)
     sg.solvers.jacobi_pressure_solver(got, dev(div), dev(fmu), dev(fmv), 1.0, 1.0 / W, 0.5 / W, iterations=iters)
     assert np.array_equal(got.cpu().numpy(), exp)
+
+
+@pytest.mark.parametrize("precision,pdtype", [("fp64", torch.float64), ("fp32", torch.float32),
+                                              ("mixed", torch.float64)])
+def test_gmg_fused_post_kernel_staged_and_unstaged_agree(precision, pdtype):
+    """The fused fine-level post kernel stages the caller's pressure rows (and, in mixed
+    precision, the carried float64 residual) in shared memory with bulk asynchronous copies
+    when they start on 16-byte boundaries, and reads them from global memory otherwise. Both
+    forms run the same arithmetic: a pressure array whose rows sit one element off a 16-byte
+    boundary (row stride W + 2) must come out of a 3-cycle solve with the same bits, and with
+    the same relative residual, as a contiguous one."""
+    H, W = 1024, 1280
+    _, _, _, div = _problem(H, W, False, 7)
+    d = dev(div.astype(np.float32 if precision == "fp32" else np.float64))
+    out = []
+    for off in (False, True):
+        if off:
+            base = torch.zeros((H, W + 2), dtype=pdtype, device="cuda")
+            p = base[:, 1:W + 1]
+            assert (p.data_ptr() % 16) != 0
+        else:
+            p = torch.zeros((H, W), dtype=pdtype, device="cuda")
+        solver = sg.GeometricMultigridSolver()
+        solver(p, d, sg.OPEN_BOX, sg.OPEN_BOX, 0.7, 1.0, 1.0, precision=precision, fixed_cycles=3, coarsest=32,
+               omega=OMEGA)
+        assert solver.current_plan().fine_fused()
+        out.append((p.clone(), solver.last_relres))
+    assert torch.equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1]
