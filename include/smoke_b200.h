@@ -411,6 +411,13 @@ int sg_gmg_fine_fused(const sg_gmg_plan* plan);
  * sg_gmg_bind when the level's rows are whole 16-byte units); -1 for a NULL plan. No
  * counterpart in the reference. */
 int sg_gmg_coarse_solve_kind(const sg_gmg_plan* plan);
+/* Timing hook for kernel-by-kernel solves (the fixed-cycle entry points; never inside stream
+ * capture): events[2k] and events[2k + 1] (cudaEvent_t, created by the caller with timing
+ * enabled) are recorded on the solve's stream right before and after the k-th fused
+ * fine-level post launch that follows this call, for k < n_pairs; n_pairs = 0 clears it. The
+ * plan keeps the handles, not the events. For timing the solver's dominant kernel in the
+ * context of a real step. No counterpart in the reference. */
+int sg_gmg_set_post_events(sg_gmg_plan* plan, void* const* events, int n_pairs);
 /* One launch of a fused fine-level kernel on the bound workspace, whatever it holds
  * (which = 0: pre kernel; 1: post kernel, which adds its correction to p, ld_p >= W, in the
  * plan's fine precision). Exposed for timing the solver's dominant kernels in isolation;

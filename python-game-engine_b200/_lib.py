@@ -82,6 +82,7 @@ SIGNATURES = {
     "sg_gmg_smooth_async": [P, I, I, P],
     "sg_gmg_fine_fused": [P],
     "sg_gmg_coarse_solve_kind": [P],
+    "sg_gmg_set_post_events": [P, P, I],
     "sg_gmg_relres_async": [P, P, P],
     "sg_project_metrics": [I, I64, I64, P, I64, P, I64, P, I64, P, I64, P, I64, I, P, I64, P, I64, P, I64, I, P, I64,
                            D, D, D, D, D, P, I64, P, I64, P],

@@ -21,6 +21,7 @@
 // a solve needs no host synchronisation.
 
 #include <algorithm>
+#include <type_traits>
 #include <cstring>
 #include <vector>
 
@@ -396,32 +397,33 @@ constexpr int kDctMultiMaxSide = 256;  // and up to this side: the transform as 
 // c_k(i) = s_k cos(pi k (i + 1/2) / n) (s_0 = sqrt(1/n), s_k = sqrt(2/n)) with eigenvalues
 // 4 sin^2(pi k / (2 n)). So e = C_y^T [(C_y b C_x^T) / (lambda_y + lambda_x)] C_x with the
 // constant mode (0, 0) set to 0, which is the pseudo-inverse solution the dense
-// pseudo-inverse gives on smaller coarsest levels. One block of 1024 threads; tab (in the
-// cycle precision, copied whole into shared memory) = C_x (c_k(i) at k W + i), C_x^T,
+// pseudo-inverse gives on smaller coarsest levels. One block of 1024 threads; b and e in the
+// level type T, the arithmetic and tab in TA (float64 in mixed precision, as for the dense
+// pseudo-inverse; copied whole into shared memory) = C_x (c_k(i) at k W + i), C_x^T,
 // C_y (H x H), lambda_x (W), lambda_y (H). Every product keeps four partial sums.
-template <typename T>
+template <typename T, typename TA = T>
 __global__ void __launch_bounds__(1024) k_gmg_coarse_dct(const T* __restrict__ b, int64_t ldb, T* __restrict__ e,
-                                                         int64_t lde, int H, int W, const T* __restrict__ tab) {
+                                                         int64_t lde, int H, int W, const TA* __restrict__ tab) {
   extern __shared__ __align__(16) unsigned char dct_smem[];
-  T* sm = reinterpret_cast<T*>(dct_smem);
+  TA* sm = reinterpret_cast<TA*>(dct_smem);
   const int ntab = 2 * W * W + H * H + W + H;
-  const T* cx = sm;             // cx[k W + i]
-  const T* cxt = cx + W * W;    // cxt[i W + k]
-  const T* cy = cxt + W * W;    // cy[m H + j]
-  const T* lx = cy + H * H;
-  const T* ly = lx + W;
-  T* X = sm + ntab;
-  T* Y = X + H * W;
+  const TA* cx = sm;             // cx[k W + i]
+  const TA* cxt = cx + W * W;    // cxt[i W + k]
+  const TA* cy = cxt + W * W;    // cy[m H + j]
+  const TA* lx = cy + H * H;
+  const TA* ly = lx + W;
+  TA* X = sm + ntab;
+  TA* Y = X + H * W;
   const int tid = threadIdx.x, nt = blockDim.x, n = H * W;
   for (int q = tid; q < ntab; q += nt) sm[q] = tab[q];
   for (int q = tid; q < n; q += nt) {
     const int j = q / W, i = q - j * W;
-    Y[q] = b[(int64_t)j * ldb + i];
+    Y[q] = (TA)b[(int64_t)j * ldb + i];
   }
   __syncthreads();
   // sum_t a[t * sa] * c[t * sc] over t < len with four partial sums
-  auto dot = [](const T* a, int sa, const T* c, int sc, int len) {
-    T s0 = (T)0, s1 = (T)0, s2 = (T)0, s3 = (T)0;
+  auto dot = [](const TA* a, int sa, const TA* c, int sc, int len) {
+    TA s0 = (TA)0, s1 = (TA)0, s2 = (TA)0, s3 = (TA)0;
     int t = 0;
     for (; t + 4 <= len; t += 4) {
       s0 += a[t * sa] * c[t * sc];
@@ -439,8 +441,8 @@ __global__ void __launch_bounds__(1024) k_gmg_coarse_dct(const T* __restrict__ b
   __syncthreads();
   for (int q = tid; q < n; q += nt) {  // Y = (C_y X) / (lambda_y + lambda_x)
     const int m = q / W, k = q - m * W;
-    const T acc = dot(cy + m * H, 1, X + k, W, H);
-    Y[q] = (m == 0 && k == 0) ? (T)0 : acc / (ly[m] + lx[k]);
+    const TA acc = dot(cy + m * H, 1, X + k, W, H);
+    Y[q] = (m == 0 && k == 0) ? (TA)0 : acc / (ly[m] + lx[k]);
   }
   __syncthreads();
   for (int q = tid; q < n; q += nt) {  // X = C_y^T Y
@@ -450,7 +452,7 @@ __global__ void __launch_bounds__(1024) k_gmg_coarse_dct(const T* __restrict__ b
   __syncthreads();
   for (int q = tid; q < n; q += nt) {  // e = X C_x
     const int j = q / W, i = q - j * W;
-    e[(int64_t)j * lde + i] = dot(X + j * W, 1, cx + i, W, W);
+    e[(int64_t)j * lde + i] = (T)dot(X + j * W, 1, cx + i, W, W);
   }
 }
 
@@ -597,26 +599,53 @@ __device__ __forceinline__ void load_rows4(const T* __restrict__ p, T (&v)[kDsRB
   }
 }
 
+// One chunk's products for the thread's column c: acc[r] += left[t][r] * slot[t][c] over the
+// chunk's rows t taken by thread group kg (every NKG-th), slot rows W long in type TS.
+template <int NKG, typename TS, typename TA>
+__device__ __forceinline__ void dct_stream_consume(const TS* __restrict__ slot, int W, int c, int kg, int nr,
+                                                   const TA* __restrict__ left, TA (&acc)[kDsRB]) {
+  if (nr == kDsKC) {
+#pragma unroll
+    for (int tt = 0; tt < kDsKC / NKG; ++tt) {
+      const int t = tt * NKG + kg;
+      const TA v = (TA)slot[(size_t)t * W + c];
+      TA l[kDsRB];
+      load_rows4(left + t * kDsRB, l);
+#pragma unroll
+      for (int r = 0; r < kDsRB; ++r) acc[r] += l[r] * v;
+    }
+  } else {
+    for (int t = kg; t < nr; t += NKG) {
+      const TA v = (TA)slot[(size_t)t * W + c];
+      TA l[kDsRB];
+      load_rows4(left + t * kDsRB, l);
+#pragma unroll
+      for (int r = 0; r < kDsRB; ++r) acc[r] += l[r] * v;
+    }
+  }
+}
+
 // NKG thread groups of roundup32(W) threads (blockDim = NKG * roundup32(W) <= 256). INVERSE:
-// the second launch. b: the level's rhs (row stride ldb); X: H x W scratch (row stride W);
-// tab: the tables of k_gmg_coarse_dct.
-template <typename T, int NKG, bool INVERSE>
+// the second launch. b: the level's rhs (row stride ldb) and e its solution, in the level type
+// T; the arithmetic, the tables of k_gmg_coarse_dct (tab) and the H x W scratch X (row stride
+// W) in TA (float64 in mixed precision).
+template <typename T, typename TA, int NKG, bool INVERSE>
 __global__ void __launch_bounds__(256) k_dct_stream(int H, int W, const T* __restrict__ b, int64_t ldb,
-                                                    const T* __restrict__ tab, T* __restrict__ X, T* __restrict__ e,
+                                                    const TA* __restrict__ tab, TA* __restrict__ X, T* __restrict__ e,
                                                     int64_t lde, GmgState* __restrict__ st) {
   extern __shared__ __align__(128) unsigned char ds_smem[];
-  const DctStreamLayout lay = dct_stream_layout<T>(H, W);
+  const DctStreamLayout lay = dct_stream_layout<TA>(H, W);
   uint64_t* full = reinterpret_cast<uint64_t*>(ds_smem);
-  T* L0 = reinterpret_cast<T*>(ds_smem + lay.off_left);  // [k][r], k < max(H, W)
-  T* L1 = L0 + (size_t)(H > W ? H : W) * kDsRB;          // [i][r], i < W
-  T* L2 = L1 + (size_t)W * kDsRB;                        // [k][r], k < W
-  T* red = reinterpret_cast<T*>(ds_smem + lay.off_red);  // [group - 1][r][c]
-  T* ring = reinterpret_cast<T*>(ds_smem + lay.off_ring);
-  const T* cx = tab;                   // cx[k W + i]
-  const T* cxt = cx + (int64_t)W * W;  // cxt[i W + k]
-  const T* cy = cxt + (int64_t)W * W;  // cy[m H + j]
-  const T* lx = cy + (int64_t)H * H;
-  const T* ly = lx + W;
+  TA* L0 = reinterpret_cast<TA*>(ds_smem + lay.off_left);  // [k][r], k < max(H, W)
+  TA* L1 = L0 + (size_t)(H > W ? H : W) * kDsRB;           // [i][r], i < W
+  TA* L2 = L1 + (size_t)W * kDsRB;                         // [k][r], k < W
+  TA* red = reinterpret_cast<TA*>(ds_smem + lay.off_red);  // [group - 1][r][c]
+  TA* ring = reinterpret_cast<TA*>(ds_smem + lay.off_ring);  // slots of kDsKC x W elements of TA
+  const TA* cx = tab;                   // cx[k W + i]
+  const TA* cxt = cx + (int64_t)W * W;  // cxt[i W + k]
+  const TA* cy = cxt + (int64_t)W * W;  // cy[m H + j]
+  const TA* lx = cy + (int64_t)H * H;
+  const TA* ly = lx + W;
   const int tid = threadIdx.x, nt = blockDim.x;
   const int cw = (W + 31) & ~31;
   const int c = tid % cw, kg = tid / cw;  // column and thread group
@@ -626,7 +655,6 @@ __global__ void __launch_bounds__(256) k_dct_stream(int H, int W, const T* __res
   auto nrows = [&](int q) { return q == 0 ? H : W; };
   auto nch = [&](int q) { return (nrows(q) + kDsKC - 1) / kDsKC; };
   const int total = INVERSE ? nch(0) : nch(0) + 2 * nch(1);
-  const uint32_t row_bytes = (uint32_t)W * sizeof(T);
   // warp 0: chunk ch into slot ch % ns. Lane 0 arrives with the chunk's byte count; the
   // copies (one for a contiguous chunk, else one per row from lanes 0 .. nr - 1) may land
   // before that arrival: the phase cannot complete while the arrival is pending.
@@ -636,15 +664,19 @@ __global__ void __launch_bounds__(256) k_dct_stream(int H, int W, const T* __res
     while (k >= nch(q)) k -= nch(q++);
     const int row0 = k * kDsKC;
     const int nr = min(kDsKC, nrows(q) - row0);
-    const T* src = INVERSE ? X : (q == 0 ? b : (q == 1 ? cxt : cx));
-    const int64_t ld = (!INVERSE && q == 0) ? ldb : (int64_t)W;
+    const bool lvl = !INVERSE && q == 0;  // rows of the level (type T), else of TA
+    const unsigned char* src =
+        lvl ? reinterpret_cast<const unsigned char*>(b)
+            : reinterpret_cast<const unsigned char*>(INVERSE ? (const TA*)X : (q == 1 ? cxt : cx));
+    const uint32_t rb = (uint32_t)W * (uint32_t)(lvl ? sizeof(T) : sizeof(TA));
+    const int64_t ldbytes = lvl ? ldb * (int64_t)sizeof(T) : (int64_t)rb;
     uint64_t* bar = full + ch % ns;
-    T* dst = ring + (size_t)(ch % ns) * kDsKC * W;
-    if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)nr * row_bytes);
-    if (ld == W) {
-      if (lane == 0) bulk_g2s(dst, src + (int64_t)row0 * W, (uint32_t)nr * row_bytes, bar);
+    unsigned char* dst = reinterpret_cast<unsigned char*>(ring + (size_t)(ch % ns) * kDsKC * W);
+    if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)nr * rb);
+    if (ldbytes == (int64_t)rb) {
+      if (lane == 0) bulk_g2s(dst, src + (int64_t)row0 * rb, (uint32_t)nr * rb, bar);
     } else if (lane < nr) {
-      bulk_g2s(dst + (size_t)lane * W, src + (int64_t)(row0 + lane) * ld, row_bytes, bar);
+      bulk_g2s(dst + (size_t)lane * rb, src + (int64_t)(row0 + lane) * ldbytes, rb, bar);
     }
   };
   if (tid == 0) {
@@ -658,40 +690,25 @@ __global__ void __launch_bounds__(256) k_dct_stream(int H, int W, const T* __res
   for (int q = tid; q < H * kDsRB; q += nt) {
     const int k = q / kDsRB, r = q - k * kDsRB;
     const int row = r0 + r;
-    L0[q] = row < H ? (INVERSE ? cy[(int64_t)k * H + row] : cy[(int64_t)row * H + k]) : (T)0;
+    L0[q] = row < H ? (INVERSE ? cy[(int64_t)k * H + row] : cy[(int64_t)row * H + k]) : (TA)0;
   }
   __syncthreads();
   bool ok = true;
-  T acc[kDsRB];
+  TA acc[kDsRB];
 #pragma unroll
-  for (int r = 0; r < kDsRB; ++r) acc[r] = (T)0;
+  for (int r = 0; r < kDsRB; ++r) acc[r] = (TA)0;
   int q = 0, kq = 0;  // phase of the current chunk and its index within the phase
   for (int ch = 0; ch < total; ++ch) {
     if (!mbar_wait(full + ch % ns, (uint32_t)((ch / ns) & 1))) ok = false;
     const int row0 = kq * kDsKC;
     const int nr = min(kDsKC, nrows(q) - row0);
-    const T* left = (q == 0 ? L0 : (q == 1 ? L1 : L2)) + (size_t)row0 * kDsRB;
-    const T* slot = ring + (size_t)(ch % ns) * kDsKC * W;
+    const TA* left = (q == 0 ? L0 : (q == 1 ? L1 : L2)) + (size_t)row0 * kDsRB;
+    const TA* slot = ring + (size_t)(ch % ns) * kDsKC * W;
     if (c < W) {
-      if (nr == kDsKC) {
-#pragma unroll
-        for (int tt = 0; tt < kDsKC / NKG; ++tt) {
-          const int t = tt * NKG + kg;
-          const T v = slot[(size_t)t * W + c];
-          T l[kDsRB];
-          load_rows4(left + t * kDsRB, l);
-#pragma unroll
-          for (int r = 0; r < kDsRB; ++r) acc[r] += l[r] * v;
-        }
-      } else {
-        for (int t = kg; t < nr; t += NKG) {
-          const T v = slot[(size_t)t * W + c];
-          T l[kDsRB];
-          load_rows4(left + t * kDsRB, l);
-#pragma unroll
-          for (int r = 0; r < kDsRB; ++r) acc[r] += l[r] * v;
-        }
-      }
+      if (!INVERSE && q == 0 && !std::is_same<T, TA>::value)
+        dct_stream_consume<NKG>(reinterpret_cast<const T*>(slot), W, c, kg, nr, left, acc);
+      else
+        dct_stream_consume<NKG>(slot, W, c, kg, nr, left, acc);
     }
     if (++kq == nch(q)) {  // the phase's products are complete: sum the groups, epilogue
       if (NKG > 1) {
@@ -704,23 +721,23 @@ __global__ void __launch_bounds__(256) k_dct_stream(int H, int W, const T* __res
       if (kg == 0 && c < W) {
 #pragma unroll
         for (int r = 0; r < kDsRB; ++r) {
-          T v = acc[r];
+          TA v = acc[r];
 #pragma unroll
           for (int g = 1; g < NKG; ++g) v += red[((size_t)(g - 1) * kDsRB + r) * W + c];
           const int row = r0 + r;
           if (INVERSE) {
-            if (row < H) e[(int64_t)row * lde + c] = v;
+            if (row < H) e[(int64_t)row * lde + c] = (T)v;
           } else if (q == 0) {
             L1[c * kDsRB + r] = v;
           } else if (q == 1) {
-            L2[c * kDsRB + r] = (row == 0 && c == 0) || row >= H ? (T)0 : v / (ly[row < H ? row : 0] + lx[c]);
+            L2[c * kDsRB + r] = (row == 0 && c == 0) || row >= H ? (TA)0 : v / (ly[row < H ? row : 0] + lx[c]);
           } else if (row < H) {
             X[(int64_t)row * W + c] = v;
           }
         }
       }
 #pragma unroll
-      for (int r = 0; r < kDsRB; ++r) acc[r] = (T)0;
+      for (int r = 0; r < kDsRB; ++r) acc[r] = (TA)0;
       ++q;
       kq = 0;
     }
@@ -1034,7 +1051,12 @@ struct sg_gmg_plan {
   // transform (k_gmg_coarse_dct) from the tables in dct (C_x, C_y, eigenvalues)
   int coarse_dct = 0;
   int coarse_dct_multi = 0;  // above kDctMaxSide: the four-product form (k_dct_gemm), scratch at off_dct_x
-  int coarse_dct_stream = 0;  // ... run as the two streaming launches (k_dct_stream), decided at bind
+  int coarse_dct_stream = 0;  // ... run as the two streaming launches (k_dct_stream)
+  int dct_fp64 = 0;           // the transform's arithmetic and tables in float64 (FP64 and mixed precision)
+  // events recorded around the fused fine-level post launches of kernel-by-kernel solves
+  // (pairs, consumed in order; sg_gmg_set_post_events)
+  mutable std::vector<cudaEvent_t> post_ev;
+  mutable size_t post_ev_next = 0;
   int64_t dct_stream_smem = 0;
   int64_t off_dct_x = 0;
   std::vector<double> dct;
@@ -1408,15 +1430,26 @@ static void launch_post_final(const sg_gmg_plan* p, TP* pp, int64_t ldp, cudaStr
   // a 16-byte boundary (the workspace rows always do; the caller's p must)
   const bool staged = ((uintptr_t)pp % 16) == 0 && ((size_t)ldp * sizeof(TP)) % 16 == 0 &&
                       ((uintptr_t)p->ws % 16) == 0 && ((size_t)L.ld * sizeof(TP)) % 16 == 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (p->post_ev_next + 1 < p->post_ev.size()) {  // timing events, outside stream capture only
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusActive;
+    if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
+      ev0 = p->post_ev[p->post_ev_next];
+      ev1 = p->post_ev[p->post_ev_next + 1];
+      p->post_ev_next += 2;
+    }
+  }
+  if (ev0) cudaEventRecord(ev0, s);
   if (staged) {
     SG_LAUNCH(k_gmg_post_final_stage<TC, TP, SW, RPT, NW, MB><<<post_final_grid<TC>(p), 32 * NW, 0, s>>>(
         ws_ptr<TC>(p, L.off_e2), ws_ptr<TC>(p, L.off_b), ws_ptr<TC>(p, p->off_b2), state_ptr(p), L.ld, L.H, L.W,
         ws_ptr<TC>(p, C.off_e), C.ld, C.H, C.W, (TC)p->omega, pp, ldp, r64, (double*)(p->ws + p->off_partial)));
-    return;
+  } else {
+    SG_LAUNCH(k_gmg_post_final_reg<TC, TP, SW, RPT, NW, MB><<<post_final_grid<TC>(p), 32 * NW, 0, s>>>(
+        ws_ptr<TC>(p, L.off_e2), ws_ptr<TC>(p, L.off_b), ws_ptr<TC>(p, p->off_b2), state_ptr(p), L.ld, L.H, L.W,
+        ws_ptr<TC>(p, C.off_e), C.ld, C.H, C.W, (TC)p->omega, pp, ldp, r64, (double*)(p->ws + p->off_partial)));
   }
-  SG_LAUNCH(k_gmg_post_final_reg<TC, TP, SW, RPT, NW, MB><<<post_final_grid<TC>(p), 32 * NW, 0, s>>>(
-      ws_ptr<TC>(p, L.off_e2), ws_ptr<TC>(p, L.off_b), ws_ptr<TC>(p, p->off_b2), state_ptr(p), L.ld, L.H, L.W,
-      ws_ptr<TC>(p, C.off_e), C.ld, C.H, C.W, (TC)p->omega, pp, ldp, r64, (double*)(p->ws + p->off_partial)));
+  if (ev1) cudaEventRecord(ev1, s);
 }
 
 // Large levels: register tiles; small levels: 16 x 16 shared-memory tiles.
@@ -1464,54 +1497,51 @@ static int dct_stream_groups(int W) {
 
 // The streaming form of the coarsest cosine transform applies when every streamed row (of B,
 // the tables and the scratch) starts and ends on 16-byte boundaries and its shared memory
-// fits one block; otherwise the four-product form stays. Called at bind (the workspace
-// address is known then).
-template <typename T>
-static int choose_dct_stream(sg_gmg_plan* p) {
-  const Level& C = p->levels.back();
-  const DctStreamLayout lay = dct_stream_layout<T>(C.H, C.W);
-  const bool aligned = ((size_t)C.W * sizeof(T)) % 16 == 0 && ((size_t)C.ld * sizeof(T)) % 16 == 0 &&
-                       ((uintptr_t)p->ws % 16) == 0;
-  p->coarse_dct_stream = 0;
-  if (!aligned || lay.bytes > 220 * 1024) return SG_OK;
-  const int bytes = (int)lay.bytes;
+// fits one block; otherwise the four-product form stays. T: level type, TA: arithmetic type.
+// The workspace itself is 256-byte aligned (sg_gmg_bind checks it).
+template <typename T, typename TA>
+static bool dct_stream_fits(const Level& C) {
+  return ((size_t)C.W * sizeof(T)) % 16 == 0 && ((size_t)C.W * sizeof(TA)) % 16 == 0 &&
+         ((size_t)C.ld * sizeof(T)) % 16 == 0 && dct_stream_layout<TA>(C.H, C.W).bytes <= (size_t)kDsSmemBudget;
+}
+
+template <typename T, typename TA>
+static int set_dct_stream_smem(const sg_gmg_plan* p) {
+  const int bytes = (int)p->dct_stream_smem;
   cudaError_t e = cudaSuccess;
-#define SG_DS_ATTR(NKG)                                                                                         \
-  if (e == cudaSuccess)                                                                                         \
-    e = cudaFuncSetAttribute(k_dct_stream<T, NKG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);  \
-  if (e == cudaSuccess)                                                                                         \
-    e = cudaFuncSetAttribute(k_dct_stream<T, NKG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  switch (dct_stream_groups(C.W)) {
+#define SG_DS_ATTR(NKG)                                                                                            \
+  if (e == cudaSuccess)                                                                                            \
+    e = cudaFuncSetAttribute(k_dct_stream<T, TA, NKG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes); \
+  if (e == cudaSuccess)                                                                                            \
+    e = cudaFuncSetAttribute(k_dct_stream<T, TA, NKG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  switch (dct_stream_groups(p->levels.back().W)) {
     case 4: SG_DS_ATTR(4) break;
     case 2: SG_DS_ATTR(2) break;
     default: SG_DS_ATTR(1) break;
   }
 #undef SG_DS_ATTR
-  if (e != cudaSuccess) return fail(SG_ERR_CUDA, "cosine-transform stream smem: %s", cudaGetErrorString(e));
-  p->coarse_dct_stream = 1;
-  p->dct_stream_smem = bytes;
-  return SG_OK;
+  return e == cudaSuccess ? SG_OK : fail(SG_ERR_CUDA, "cosine-transform stream smem: %s", cudaGetErrorString(e));
 }
 
-template <typename T, int NKG>
+template <typename T, typename TA, int NKG>
 static void dct_stream_launch_g(const sg_gmg_plan* p, const Level& C, cudaStream_t s) {
-  const T* tab = ws_ptr<T>(p, p->off_dct);
-  T* X = ws_ptr<T>(p, p->off_dct_x);
+  const TA* tab = (const TA*)(p->ws + p->off_dct);
+  TA* X = (TA*)(p->ws + p->off_dct_x);
   const int cw = (C.W + 31) / 32 * 32;
   const dim3 g((C.H + kDsRB - 1) / kDsRB), b(cw * NKG);
   const size_t sm = (size_t)p->dct_stream_smem;
-  SG_LAUNCH((k_dct_stream<T, NKG, false><<<g, b, sm, s>>>(C.H, C.W, ws_ptr<T>(p, C.off_b), C.ld, tab, X, nullptr, 0,
-                                                          state_ptr(p))));
-  SG_LAUNCH((k_dct_stream<T, NKG, true><<<g, b, sm, s>>>(C.H, C.W, nullptr, 0, tab, X, ws_ptr<T>(p, C.off_e), C.ld,
-                                                         state_ptr(p))));
+  SG_LAUNCH((k_dct_stream<T, TA, NKG, false><<<g, b, sm, s>>>(C.H, C.W, ws_ptr<T>(p, C.off_b), C.ld, tab, X, nullptr,
+                                                              0, state_ptr(p))));
+  SG_LAUNCH((k_dct_stream<T, TA, NKG, true><<<g, b, sm, s>>>(C.H, C.W, nullptr, 0, tab, X, ws_ptr<T>(p, C.off_e),
+                                                             C.ld, state_ptr(p))));
 }
 
-template <typename T>
+template <typename T, typename TA>
 static void dct_stream_launch(const sg_gmg_plan* p, const Level& C, cudaStream_t s) {
   switch (dct_stream_groups(C.W)) {
-    case 4: dct_stream_launch_g<T, 4>(p, C, s); break;
-    case 2: dct_stream_launch_g<T, 2>(p, C, s); break;
-    default: dct_stream_launch_g<T, 1>(p, C, s); break;
+    case 4: dct_stream_launch_g<T, TA, 4>(p, C, s); break;
+    case 2: dct_stream_launch_g<T, TA, 2>(p, C, s); break;
+    default: dct_stream_launch_g<T, TA, 1>(p, C, s); break;
   }
 }
 
@@ -1521,7 +1551,10 @@ static void cycle(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
   if (p->coarse_dct && k == (int)p->levels.size() - 1) {
     const Level& C = p->levels[k];
     if (p->coarse_dct_stream) {
-      dct_stream_launch<T>(p, C, s);
+      if (p->dct_fp64)
+        dct_stream_launch<T, double>(p, C, s);
+      else
+        dct_stream_launch<T, T>(p, C, s);
       return;
     }
     if (p->coarse_dct_multi) {
@@ -1545,8 +1578,12 @@ static void cycle(const sg_gmg_plan* p, int k, bool zero_init, cudaStream_t s) {
                                                                           nullptr)));
       return;
     }
-    SG_LAUNCH(k_gmg_coarse_dct<T><<<1, 1024, p->dct_smem, s>>>(ws_ptr<T>(p, C.off_b), C.ld, ws_ptr<T>(p, C.off_e), C.ld,
-                                                                C.H, C.W, ws_ptr<T>(p, p->off_dct)));
+    if (p->dct_fp64)
+      SG_LAUNCH((k_gmg_coarse_dct<T, double><<<1, 1024, p->dct_smem, s>>>(
+          ws_ptr<T>(p, C.off_b), C.ld, ws_ptr<T>(p, C.off_e), C.ld, C.H, C.W, (const double*)(p->ws + p->off_dct))));
+    else
+      SG_LAUNCH((k_gmg_coarse_dct<T, T><<<1, 1024, p->dct_smem, s>>>(ws_ptr<T>(p, C.off_b), C.ld, ws_ptr<T>(p, C.off_e),
+                                                                      C.ld, C.H, C.W, ws_ptr<T>(p, p->off_dct))));
     return;
   }
   if (k == p->tail_start) {
@@ -1902,9 +1939,20 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
   if (p->coarse_dct) {
     const Level& C = p->levels.back();
     p->tail_smem = 0;
+    // float64 arithmetic in FP64 and mixed precision (the coarsest solve stays FP64 there, as
+    // the dense pseudo-inverse's does); mixed levels that need the four-product form (rows
+    // not in 16-byte units) keep it in float32
+    const bool fits = precision == SG_GMG_FP64 ? dct_stream_fits<double, double>(C)
+                                               : (precision == SG_GMG_MIXED ? dct_stream_fits<float, double>(C)
+                                                                           : dct_stream_fits<float, float>(C));
+    p->coarse_dct_stream = p->coarse_dct_multi && fits ? 1 : 0;
+    p->dct_fp64 = precision == SG_GMG_FP64 || (precision == SG_GMG_MIXED && (!p->coarse_dct_multi || fits)) ? 1 : 0;
+    p->dct_stream_smem = !p->coarse_dct_stream ? 0
+                         : (int64_t)(p->dct_fp64 ? dct_stream_layout<double>(C.H, C.W).bytes
+                                                 : dct_stream_layout<float>(C.H, C.W).bytes);
     p->dct_smem = p->coarse_dct_multi ? 0
-                                      : (int64_t)(precision == SG_GMG_FP64 ? coarse_dct_smem<double>(C.H, C.W)
-                                                                           : coarse_dct_smem<float>(C.H, C.W));
+                                      : (int64_t)(p->dct_fp64 ? coarse_dct_smem<double>(C.H, C.W)
+                                                              : coarse_dct_smem<float>(C.H, C.W));
   } else {
     p->tail_smem = (p->tail_open ? (int64_t)open_tail_layout(p->levels, p->tail_start).total
                                  : generic_elems(p->tail_start)) *
@@ -1996,7 +2044,7 @@ int sg_gmg_bind(sg_gmg_plan* plan, void* workspace, void* stream) {
                               cudaMemcpyHostToDevice, s),
               "sg_gmg_bind pinv");
   if (plan->coarse_dct) {
-    if (plan->precision == SG_GMG_FP64) {
+    if (plan->dct_fp64) {
       SG_CUDA_TRY(cudaMemcpyAsync(plan->ws + plan->off_dct, plan->dct.data(), plan->dct.size() * 8,
                                   cudaMemcpyHostToDevice, s),
                   "sg_gmg_bind cosine tables");
@@ -2010,13 +2058,21 @@ int sg_gmg_bind(sg_gmg_plan* plan, void* workspace, void* stream) {
     if (plan->coarse_dct_multi) {
       const int rc = plan->precision == SG_GMG_FP64 ? set_dct_gemm_smem<double>() : set_dct_gemm_smem<float>();
       if (rc != SG_OK) return rc;
-      const int rc2 = plan->precision == SG_GMG_FP64 ? choose_dct_stream<double>(plan) : choose_dct_stream<float>(plan);
-      if (rc2 != SG_OK) return rc2;
+      if (plan->coarse_dct_stream) {
+        const int rc2 = plan->precision == SG_GMG_FP64 ? set_dct_stream_smem<double, double>(plan)
+                        : (plan->dct_fp64 ? set_dct_stream_smem<float, double>(plan)
+                                          : set_dct_stream_smem<float, float>(plan));
+        if (rc2 != SG_OK) return rc2;
+      }
     }
     if (!plan->coarse_dct_multi)
       SG_CUDA_TRY(plan->precision == SG_GMG_FP64
-                      ? cudaFuncSetAttribute(k_gmg_coarse_dct<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ds)
-                      : cudaFuncSetAttribute(k_gmg_coarse_dct<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, ds),
+                      ? cudaFuncSetAttribute(k_gmg_coarse_dct<double, double>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, ds)
+                      : (plan->dct_fp64 ? cudaFuncSetAttribute(k_gmg_coarse_dct<float, double>,
+                                                               cudaFuncAttributeMaxDynamicSharedMemorySize, ds)
+                                        : cudaFuncSetAttribute(k_gmg_coarse_dct<float, float>,
+                                                               cudaFuncAttributeMaxDynamicSharedMemorySize, ds)),
                   "smem attr");
   }
   SG_CUDA_TRY(cudaMemsetAsync(plan->ws + plan->off_state, 0, sizeof(GmgState), s), "sg_gmg_bind state");
@@ -2201,6 +2257,16 @@ int sg_gmg_smooth_async(sg_gmg_plan* plan, int level, int sweeps, void* stream) 
 }
 
 int sg_gmg_fine_fused(const sg_gmg_plan* plan) { return plan ? plan->fused_ir : 0; }
+
+int sg_gmg_set_post_events(sg_gmg_plan* plan, void* const* events, int n_pairs) {
+  SG_REQUIRE(plan, "null plan");
+  SG_REQUIRE(n_pairs >= 0 && (n_pairs == 0 || events), "n_pairs must be >= 0 with events for each pair");
+  for (int k = 0; k < 2 * n_pairs; ++k) SG_REQUIRE(events[k], "event %d is NULL", k);
+  plan->post_ev.assign(reinterpret_cast<const cudaEvent_t*>(events),
+                       reinterpret_cast<const cudaEvent_t*>(events) + 2 * (size_t)n_pairs);
+  plan->post_ev_next = 0;
+  return SG_OK;
+}
 
 int sg_gmg_coarse_solve_kind(const sg_gmg_plan* plan) {
   if (!plan) return -1;

@@ -74,6 +74,61 @@ def fd_check(n, steps, n_entries, eps=(1e-6, 1e-4), seed=11):
     return out
 
 
+def fd_floor_check(n=256, steps=64, n_entries=8, eps=1e-6, spread=(0.8, 0.9, 1.0, 1.1, 1.2), eps_wide=1e-4,
+                   seed=11, tol=1e-12):
+    """Where the central differences' error at eps comes from, on `n_entries` control entries
+    drawn from those with |grad| >= 1 % of the largest. Forward in FP64 with every pressure
+    solve to `tol` relative residual.
+
+    For each entry the differences are taken at eps times each factor in `spread`. Their
+    truncation error changes by < 1e-3 of itself across that range (it goes as eps^2), so
+    their scatter is the non-smooth part of the FP64 forward, i.e. its rounding. Reported: the
+    error at eps against the adjoint, that scatter (both relative to |grad|), the error of the
+    mean over the spread, the error at eps_wide, and the floor set by the final density's own
+    FP64 representation alone: sqrt(sum_c (ulp(d_c)^2 / 6) (2 (d_c - t_c))^2) / (2 eps |grad|),
+    the standard deviation of the differences if every cell of the two rollouts' densities
+    were rounded independently to nearest once and nothing else rounded."""
+    model, force, target = A.inverse_problem(n=n, steps=steps, dtype=torch.float64, precision="fp64", tol=tol,
+                                             max_cycles=60, exact_forces=True, adjoint_advection="gather")
+    loss0, g = A.loss_and_grad(model, force, target)
+    d0 = _final_density(model, force)
+    spacing = torch.nextafter(d0.abs(), torch.full_like(d0, float("inf"))) - d0.abs()
+    ulp_norm = float(torch.sqrt(((spacing * spacing / 6.0) * (2.0 * (d0 - target)) ** 2).sum()))
+    rng = np.random.default_rng(seed)
+    gmax = float(g.abs().max())
+    strong = torch.nonzero(g.abs() >= 0.01 * gmax).cpu().numpy()
+    idx = [tuple(int(x) for x in strong[rng.integers(0, len(strong))]) for _ in range(n_entries)]
+
+    def fd(k, e):
+        fp, fm = force.clone(), force.clone()
+        fp[k] += e
+        fm[k] -= e
+        dp, dm = _final_density(model, fp), _final_density(model, fm)
+        return float(((dp - dm) * (dp + dm - 2 * target)).sum()) / (2 * e)
+
+    rows = []
+    for k in idx:
+        an = float(g[k])
+        fs = [fd(k, eps * m) for m in spread]
+        fw = fd(k, eps_wide)
+        rel = lambda a: abs(a - an) / max(abs(a), abs(an), 1e-300)  # noqa: E731
+        rows.append({"adjoint": an, "err": rel(fs[list(spread).index(1.0)]), "scatter": float(np.std(fs)) / abs(an),
+                     "err_of_mean": rel(float(np.mean(fs))), "err_wide": rel(fw),
+                     "ulp_floor": ulp_norm / (2 * eps * abs(an))})
+    col = lambda key: [r[key] for r in rows]  # noqa: E731
+    return {"grid": [n, n], "steps": steps, "forward": f"FP64, every solve to {tol:g} relative residual",
+            "entries": n_entries, "selection": "|grad| >= 1 % of the largest", "loss": loss0, "grad_max": gmax,
+            "eps": eps, "spread": list(spread),
+            "max_rel_err": max(col("err")), "median_rel_err": float(np.median(col("err"))),
+            "median_scatter": float(np.median(col("scatter"))), "max_scatter": max(col("scatter")),
+            "median_err_over_scatter": float(np.median([r["err"] / r["scatter"] for r in rows])),
+            "median_rel_err_of_mean": float(np.median(col("err_of_mean"))),
+            "median_density_ulp_floor": float(np.median(col("ulp_floor"))),
+            f"eps={eps_wide:g}": {"max_rel_err": max(col("err_wide")),
+                                  "median_rel_err": float(np.median(col("err_wide")))},
+            "rows": rows}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=256)

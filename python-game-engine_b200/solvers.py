@@ -339,6 +339,14 @@ class GMGPlan:
     COARSE_SOLVE_KINDS = ("pseudo-inverse", "cosine transform (one block)", "cosine transform (four products)",
                           "cosine transform (two streaming launches)")
 
+    def set_post_events(self, events):
+        """Record the torch.cuda.Events (timing enabled, each already recorded once so that it
+        exists) in pairs around the next len(events) // 2 fused fine-level post launches of
+        kernel-by-kernel solves; an empty list clears it."""
+        n = len(events) // 2
+        arr = (ctypes.c_void_p * max(2 * n, 1))(*[ctypes.c_void_p(e.cuda_event) for e in events[:2 * n]])
+        L.call("sg_gmg_set_post_events", self.handle, arr, n)
+
     def coarse_solve_kind(self):
         """How the coarsest level is solved (one of COARSE_SOLVE_KINDS)."""
         return self.COARSE_SOLVE_KINDS[L.load().sg_gmg_coarse_solve_kind(self.handle)]
