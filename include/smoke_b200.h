@@ -424,6 +424,15 @@ int sg_gmg_set_post_events(sg_gmg_plan* plan, void* const* events, int n_pairs);
  * the solve itself runs them inside its graph. No counterpart in the reference. */
 int sg_gmg_fine_kernel_async(sg_gmg_plan* plan, int which, void* p, int64_t ld_p, void* stream);
 
+/* ---------------------------------------------------------------- host read-back
+ * Device copy of `rows` rows of `row_bytes` bytes (strides in bytes) into a staging buffer,
+ * with cache-streaming loads and stores so that the copy does not evict the solver's working
+ * set from L2; for reading a field back to the host while the simulation keeps stepping (the
+ * reference's get_density_field, common/simulation.py:322-324, returns the live array).
+ * Pointers, strides and row_bytes must be multiples of 16 bytes. */
+int sg_stage_copy(int64_t rows, int64_t row_bytes, const void* src, int64_t ld_src_bytes, void* dst,
+                  int64_t ld_dst_bytes, void* stream);
+
 /* ---------------------------------------------------------------- adjoint (gradients)
  * Reverse-mode kernels of the smoke step with a per-step control force, for gradients of a
  * loss on the final state; the reference has no differentiation, so none of these has a

@@ -15,7 +15,7 @@ from .operators import OPEN_BOX, RING_BOX, AnalyticMask, register_operators
 from .params import (DEFAULT_SOLVER_PARAMS, SOLVER_PARAM_TYPES, GaussSeidelParams, GeometricMultigridParams,
                      JacobiParams, MultigridParams, SORParams, SORToleranceParams)
 from .registry import OPERATOR_REGISTRY, SOLVER_REGISTRY, get_operator, get_solver, register_operator, register_solver
-from .simulation import Emitter2D, NullProfileSession, PlumeSource, SmokeSimulation2D
+from .simulation import Emitter2D, FieldReadback, NullProfileSession, PlumeSource, SmokeSimulation2D
 from .solvers import (GeometricMultigridSolver, MultigridSolver, SORToleranceSolver, calculate_alpha,
                       calculate_optimal_omega, calculate_reciprocal_beta, register_solvers, solve_pressure)
 from ._lib import NotConverged, SmokeCudaError
@@ -29,7 +29,7 @@ __all__ = [
     "OPEN_BOX", "RING_BOX", "AnalyticMask", "DEFAULT_SOLVER_PARAMS", "SOLVER_PARAM_TYPES", "GaussSeidelParams",
     "GeometricMultigridParams", "JacobiParams", "MultigridParams", "SORParams", "SORToleranceParams",
     "OPERATOR_REGISTRY", "SOLVER_REGISTRY", "get_operator", "get_solver", "register_operator", "register_solver",
-    "Emitter2D", "NullProfileSession", "PlumeSource", "SmokeSimulation2D", "GeometricMultigridSolver",
+    "Emitter2D", "FieldReadback", "NullProfileSession", "PlumeSource", "SmokeSimulation2D", "GeometricMultigridSolver",
     "MultigridSolver", "SORToleranceSolver", "calculate_alpha", "calculate_optimal_omega",
     "calculate_reciprocal_beta", "solve_pressure", "NotConverged", "SmokeCudaError", "ProfileConfig",
     "ProfileSession",

@@ -83,6 +83,7 @@ SIGNATURES = {
     "sg_gmg_fine_fused": [P],
     "sg_gmg_coarse_solve_kind": [P],
     "sg_gmg_set_post_events": [P, P, I],
+    "sg_stage_copy": [I64, I64, P, I64, P, I64, P],
     "sg_gmg_relres_async": [P, P, P],
     "sg_project_metrics": [I, I64, I64, P, I64, P, I64, P, I64, P, I64, P, I64, I, P, I64, P, I64, P, I64, I, P, I64,
                            D, D, D, D, D, P, I64, P, I64, P],

@@ -428,3 +428,66 @@ class SmokeSimulation2D:
         for t in (self.density, self.velocity_u, self.velocity_v, self._temperature, self.pressure, self.divergence):
             t.zero_()
         self.accumulator = 0.0
+
+
+class FieldReadback:
+    """Host read-back of a simulation field every step without stalling the steps.
+
+    ``SmokeSimulation2D.get_density_field`` (common/simulation.py:322-324) hands out the live
+    array; on the GPU the next substep rewrites it in place (the sources) while a host copy
+    would still be reading it. ``submit()``, called after a substep, copies the field on the
+    device into one of ``slots`` staging buffers (cache-streaming loads and stores,
+    sg_stage_copy) and queues its copy into pinned host memory on a copy stream; a slot is
+    reused only after its previous host copy has finished (the compute stream waits for it on
+    the device, not the host). ``result(slot)`` waits for that slot's copy and returns the
+    pinned host tensor."""
+
+    def __init__(self, sim, field="density", slots=2):
+        self.sim, self.field = sim, field
+        src = getattr(sim, field)
+        self.host = [torch.empty(src.shape, dtype=src.dtype).pin_memory() for _ in range(slots)]
+        self.staging = [torch.empty_like(src) for _ in range(slots)]
+        self.copy_stream = torch.cuda.Stream(device=src.device)
+        self.done = [None] * slots
+        self.next = 0
+
+    def _stage(self, dst, src):
+        es = src.element_size()
+        rb = src.shape[1] * es
+        if (src.data_ptr() | dst.data_ptr() | src.stride(0) * es | dst.stride(0) * es | rb) % 16 == 0 \
+                and src.stride(1) == 1 and dst.stride(1) == 1:
+            L.call("sg_stage_copy", src.shape[0], rb, src.data_ptr(), src.stride(0) * es, dst.data_ptr(),
+                   dst.stride(0) * es, L.stream_ptr())
+        else:
+            dst.copy_(src)
+
+    def submit(self):
+        """Queue the read-back of the field as it stands; returns the slot it lands in."""
+        k = self.next
+        self.next = (k + 1) % len(self.host)
+        stream = torch.cuda.current_stream()
+        if self.done[k] is not None:
+            stream.wait_event(self.done[k])
+        self._stage(self.staging[k], getattr(self.sim, self.field))
+        staged = torch.cuda.Event()
+        staged.record(stream)
+        self.copy_stream.wait_event(staged)
+        with torch.cuda.stream(self.copy_stream):
+            self.host[k].copy_(self.staging[k], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(self.copy_stream)
+        self.done[k] = ev
+        return k
+
+    def wait(self, stream=None):
+        """Make `stream` (default: the current one) wait for every queued read-back."""
+        stream = stream or torch.cuda.current_stream()
+        for ev in self.done:
+            if ev is not None:
+                stream.wait_event(ev)
+
+    def result(self, slot):
+        """The pinned host copy of slot `slot`, after waiting for it on the host."""
+        if self.done[slot] is not None:
+            self.done[slot].synchronize()
+        return self.host[slot]
