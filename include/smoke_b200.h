@@ -162,6 +162,24 @@ int sg_project_metrics(int dtype, int64_t H, int64_t W, const void* u_in, int64_
                        int64_t ld_s, double fluid_density, double cell_size, double dt, double alpha,
                        double reciprocal_beta, void* div, int64_t ld_div, void* res, int64_t ld_res, void* stream);
 
+/* Float32 fields in float32 arithmetic (no counterpart in the reference, whose kernels form
+ * these terms in float64; results equal the reference's up to rounding, 1e-5 of the fields'
+ * magnitude in the tests): the buoyancy force of sg_apply_forces (forces.py:19-105, the
+ * reference's face averaging) and the projection tail of sg_project_metrics
+ * (pressure_gradient.py:4-37, boundaries.py:7-39, divergence.py:4-25, residual.py:6-42).
+ * Same arguments as those entries without the dtype (and without f32_temporaries). Fields
+ * below 2^31 elements. */
+int sg_apply_forces_f32(int64_t H, int64_t W, void* v, int64_t ld_v, const void* density, int64_t ld_d,
+                        const void* temperature, int64_t ld_t, double dt, double gravity, double buoyancy_coefficient,
+                        double density_coefficient, double ambient_temperature, void* stream);
+int sg_project_metrics_f32(int64_t H, int64_t W, const void* u_in, int64_t ld_ui, const void* v_in, int64_t ld_vi,
+                           void* u_out, int64_t ld_uo, void* v_out, int64_t ld_vo, const void* p, int64_t ld_p,
+                           int mask_mode, const uint8_t* fmu, int64_t ld_fmu, const uint8_t* fmv, int64_t ld_fmv,
+                           const uint8_t* is_fluid, int64_t ld_fluid, int solid_mode, const uint8_t* solid,
+                           int64_t ld_s, double fluid_density, double cell_size, double dt, double alpha,
+                           double reciprocal_beta, void* div, int64_t ld_div, void* res, int64_t ld_res,
+                           void* stream);
+
 /* common/emitters.py:37-66 (_apply_scalar_field_numba); approach 0 hard_cutoff,
  * 1 linear, 2 quadratic, 3 gaussian (emitters.py:6-35). */
 int sg_emit_scalar(int dtype, int64_t H, int64_t W, void* field, int64_t ld, double value, double dt,

@@ -88,6 +88,9 @@ SIGNATURES = {
     "sg_project_metrics": [I, I64, I64, P, I64, P, I64, P, I64, P, I64, P, I64, I, P, I64, P, I64, P, I64, I, P, I64,
                            D, D, D, D, D, P, I64, P, I64, P],
     "sg_gmg_fine_kernel_async": [P, I, P, I64, P],
+    "sg_apply_forces_f32": [I64, I64, P, I64, P, I64, P, I64, D, D, D, D, D, P],
+    "sg_project_metrics_f32": [I64, I64, P, I64, P, I64, P, I64, P, I64, P, I64, I, P, I64, P, I64, P, I64, I, P,
+                               I64, D, D, D, D, D, P, I64, P, I64, P],
     "sg_add_control": [I, I64, I64, P, I64, P, I64, P, I64, P, I64, D, P],
     "sg_adjoint_advect_scalar_workspace": [I, I64, I64, I],
     "sg_adjoint_advect_scalar": [I, I64, I64, P, I64, P, I64, P, I64, P, I64, I, P, I64, D, D, D, P, I64, P, I64, P,

@@ -110,9 +110,12 @@ __global__ void k_apply_forces(int H, int W, T* __restrict__ v, int64_t ldv, con
                                double amb, int f32tmp) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= W) return;
+  // kRows consecutive faces per thread (the block's kBY * kRows rows as grid2d_rows lays them
+  // out), so each thread's density rows overlap and its loads run down one column
+  const int j0 = (blockIdx.y * blockDim.y + threadIdx.y) * kRows;
 #pragma unroll
   for (int q = 0; q < kRows; ++q) {
-    const int j = row_of(q);
+    const int j = j0 + q;
     if (j <= H) forces_face(j, i, H, W, v, ldv, d, ldd, t, ldt, dt, g, bc, dc, amb, f32tmp);
   }
 }

@@ -65,7 +65,7 @@ def _arithmetic(arithmetic, dt_code):
         return False
     if arithmetic == "float32":
         if dt_code != L.SG_F32:
-            raise TypeError("arithmetic='float32' advects float32 fields")
+            raise TypeError("arithmetic='float32' takes float32 fields")
         return True
     raise ValueError(f"arithmetic must be 'reference' or 'float32', got {arithmetic!r}")
 
@@ -142,8 +142,10 @@ def advect_velocity(u_src, u_dst, v_src, v_dst, face_mask_u, face_mask_v, dt, ce
 
 
 def apply_forces(velocity_v, density, temperature, dt, gravity, buoyancy_coefficient, density_coefficient,
-                 ambient_temperature, f32_temporaries: bool = True, **_ignored):
-    """forces.py:78-105. ``temperature`` may be None (ambient everywhere)."""
+                 ambient_temperature, f32_temporaries: bool = True, arithmetic="reference", **_ignored):
+    """forces.py:78-105. ``temperature`` may be None (ambient everywhere). ``arithmetic``:
+    "reference" (the reference's float64 terms, bit for bit) or, for float32 fields,
+    "float32" (``sg_apply_forces_f32``: equal up to rounding)."""
     dt_code = _same_dtype(velocity_v, density, *( [temperature] if temperature is not None else []))
     H, W = density.shape
     if tuple(velocity_v.shape) != (H + 1, W):
@@ -151,6 +153,10 @@ def apply_forces(velocity_v, density, temperature, dt, gravity, buoyancy_coeffic
     v, ldv = L.field(velocity_v, "velocity_v")
     d, ldd = L.field(density, "density")
     t, ldt = L.field(temperature, "temperature") if temperature is not None else _NULL
+    if _arithmetic(arithmetic, dt_code):
+        L.call("sg_apply_forces_f32", H, W, v, ldv, d, ldd, t, ldt, float(dt), float(gravity),
+               float(buoyancy_coefficient), float(density_coefficient), float(ambient_temperature), L.stream_ptr())
+        return
     L.call("sg_apply_forces", dt_code, H, W, v, ldv, d, ldd, t, ldt, float(dt), float(gravity),
            float(buoyancy_coefficient), float(density_coefficient), float(ambient_temperature),
            1 if f32_temporaries else 0, L.stream_ptr())
@@ -250,7 +256,7 @@ APPROACH_CODES = {"hard_cutoff": 0, "linear": 1, "quadratic": 2, "gaussian": 3}
 
 
 def project_metrics(u_in, v_in, u_out, v_out, pressure, face_mask_u, face_mask_v, is_fluid, solid_mask, fluid_density,
-                    cell_size, dt, alpha, reciprocal_beta, divergence_out, residual_out):
+                    cell_size, dt, alpha, reciprocal_beta, divergence_out, residual_out, arithmetic="reference"):
     """The substep's tail in one pass (simulation.py:244-265): project (u_in, v_in) into
     (u_out, v_out) (apply_pressure_gradient + enforce_boundary_conditions, out of place),
     then the divergence of the projected field into ``divergence_out`` and the reference
@@ -266,6 +272,12 @@ def project_metrics(u_in, v_in, u_out, v_out, pressure, face_mask_u, face_mask_v
     a = [L.field(x, n) for x, n in ((u_in, "u_in"), (v_in, "v_in"), (u_out, "u_out"), (v_out, "v_out"),
                                     (pressure, "pressure"), (divergence_out, "divergence_out"),
                                     (residual_out, "residual_out"))]
+    if _arithmetic(arithmetic, dt_code):  # float32 fields in float32 arithmetic
+        L.call("sg_project_metrics_f32", H, W, a[0][0], a[0][1], a[1][0], a[1][1], a[2][0], a[2][1], a[3][0],
+               a[3][1], a[4][0], a[4][1], mode, pu, lu, pv, lv, pf, ldf, smode, ps, lds, float(fluid_density),
+               float(cell_size), float(dt), float(alpha), float(reciprocal_beta), a[5][0], a[5][1], a[6][0],
+               a[6][1], L.stream_ptr())
+        return
     L.call("sg_project_metrics", dt_code, H, W, a[0][0], a[0][1], a[1][0], a[1][1], a[2][0], a[2][1], a[3][0],
            a[3][1], a[4][0], a[4][1], mode, pu, lu, pv, lv, pf, ldf, smode, ps, lds, float(fluid_density),
            float(cell_size), float(dt), float(alpha), float(reciprocal_beta), a[5][0], a[5][1], a[6][0], a[6][1],

@@ -229,6 +229,9 @@ class SmokeSimulation2D:
         # "reference": the reference's float64 sampling arithmetic, bit for bit; "float32":
         # float32 fields advected in float32 arithmetic (equal up to rounding, faster)
         self.advection_arithmetic = "reference"
+        # forces and the projection tail (projection, divergence and residual after it):
+        # "reference" (float64 terms, bit for bit) or, for float32 fields, "float32"
+        self.operator_arithmetic = "reference"
 
     def _init_boundaries(self):
         self._solid_mask[0, :] = True
@@ -357,7 +360,7 @@ class SmokeSimulation2D:
     def _apply_forces(self, dt):
         temp = self._temperature if self._temperature_active else None
         ops.apply_forces(self.velocity_v, self.density, temp, dt, self.gravity, self.buoyancy, 1.0,
-                         self.ambient_temperature)
+                         self.ambient_temperature, arithmetic=self.operator_arithmetic)
 
     def _advect_velocity(self, dt):
         fmu, fmv, _ = self._kmasks
@@ -411,7 +414,7 @@ class SmokeSimulation2D:
         ops.project_metrics(self.velocity_u, self.velocity_v, self.velocity_u_temp, self.velocity_v_temp,
                             self.pressure, fmu, fmv, fl, self._ksolid, self.fluid_density, self.cell_size, dt,
                             calculate_alpha(self.cell_size, self.fluid_density, dt), calculate_reciprocal_beta(),
-                            self.divergence, self.pressure_residual)
+                            self.divergence, self.pressure_residual, arithmetic=self.operator_arithmetic)
         self.velocity_u, self.velocity_u_temp = self.velocity_u_temp, self.velocity_u
         self.velocity_v, self.velocity_v_temp = self.velocity_v_temp, self.velocity_v
 

@@ -73,6 +73,7 @@ def _run(dtype, precision, arithmetic="reference"):
     params = sg.GeometricMultigridParams(tol=TOL, max_cycles=40, precision=precision, omega=1.3, coarsest=128)
     sim = sg.scenes.make_sim(sc, "geometric_multigrid", params, dtype=dtype)
     sim.advection_arithmetic = arithmetic
+    sim.operator_arithmetic = arithmetic
     name, norms = recording("geometric_multigrid")
     sim.pressure_solver_method = name
     solver = sg.get_solver("geometric_multigrid", "cuda")
