@@ -425,9 +425,10 @@ int sg_gmg_smooth_async(sg_gmg_plan* plan, int level, int sweeps, void* stream);
 int sg_gmg_fine_fused(const sg_gmg_plan* plan);
 /* How the plan solves its coarsest level exactly: 0 dense pseudo-inverse, 1 cosine transform
  * in one block, 2 cosine transform as four tiled products, 3 cosine transform as two launches
- * streaming their operands into shared memory with bulk asynchronous copies (chosen at
- * sg_gmg_bind when the level's rows are whole 16-byte units); -1 for a NULL plan. No
- * counterpart in the reference. */
+ * streaming their operands into shared memory with bulk asynchronous copies (when the
+ * level's rows are whole 16-byte units), 4 the same on clusters of two CTAs that split every
+ * product (when each CTA's share of the stream fits in its shared memory); -1 for a NULL
+ * plan. No counterpart in the reference. */
 int sg_gmg_coarse_solve_kind(const sg_gmg_plan* plan);
 /* Timing hook for kernel-by-kernel solves (the fixed-cycle entry points; never inside stream
  * capture): events[2k] and events[2k + 1] (cudaEvent_t, created by the caller with timing

@@ -22,6 +22,8 @@
 
 #include <algorithm>
 #include <type_traits>
+
+#include <cooperative_groups.h>
 #include <cstring>
 #include <vector>
 
@@ -630,7 +632,7 @@ __device__ __forceinline__ void dct_stream_consume(const TS* __restrict__ slot, 
 // T; the arithmetic, the tables of k_gmg_coarse_dct (tab) and the H x W scratch X (row stride
 // W) in TA (float64 in mixed precision).
 template <typename T, typename TA, int NKG, bool INVERSE>
-__global__ void __launch_bounds__(256) k_dct_stream(int H, int W, const T* __restrict__ b, int64_t ldb,
+__global__ void __launch_bounds__(256, 1) k_dct_stream(int H, int W, const T* __restrict__ b, int64_t ldb,
                                                     const TA* __restrict__ tab, TA* __restrict__ X, T* __restrict__ e,
                                                     int64_t lde, GmgState* __restrict__ st) {
   extern __shared__ __align__(128) unsigned char ds_smem[];
@@ -751,6 +753,244 @@ __global__ void __launch_bounds__(256) k_dct_stream(int H, int W, const T* __res
   }
 }
 
+// The streaming transform on thread-block clusters of kDcNC CTAs, for coarsest levels whose
+// whole per-CTA stream fits in shared memory (the 2048^2 workload's 128^2 level). One SM's
+// intake of its stream bounds k_dct_stream, so here the CTAs of a cluster split every product
+// and each streams a kDcNC-th of its operand, in contiguous rows:
+//   forward  T1 = C_y[m, :] B      CTA c streams B rows j in its share (partial sums over j),
+//            T2 = T1 C_x^T         CTA c forms the output columns k in its share from the split
+//                                  table (each of its rows W / kDcNC long),
+//            Y  = T2 / (ly + lx)   on those columns,
+//            X  = Y C_x            CTA c streams the C_x rows k it holds Y for (partial sums);
+//   inverse  e  = C_y^T X          CTA c streams X rows m in its share (partial sums).
+// Partial sums meet in distributed shared memory: each CTA publishes its partial, the cluster
+// synchronises, and every CTA adds the kDcNC partials in rank order (so all hold the same
+// bits of T1); X and e are written by column shares. Rows, chunks and waits as in
+// k_dct_stream, except that every chunk has its own place in shared memory.
+constexpr int kDcNC = 2;
+
+struct DctClusterLayout {
+  int nch;          // chunks in the stream
+  size_t off_left;  // L0 (H / kDcNC x kDsRB), L1 (W x kDsRB), L2 (W / kDcNC x kDsRB)
+  size_t off_red;   // thread-group partials: 3 x kDsRB x W
+  size_t off_xch;   // the CTA's published partial: kDsRB x W
+  size_t off_ring;  // the whole stream
+  size_t bytes;
+};
+
+// Phase q of a launch: rows streamed, bytes per row (level rows are T, the rest TA).
+__host__ __device__ inline void dct_cluster_phase(bool inverse, int q, int H, int W, size_t sT, size_t sTA, int& rows,
+                                                  size_t& rb) {
+  const int hc = H / kDcNC, wc = W / kDcNC;
+  if (inverse) {
+    rows = hc;
+    rb = (size_t)W * sTA;
+  } else if (q == 0) {
+    rows = hc;
+    rb = (size_t)W * sT;
+  } else if (q == 1) {
+    rows = W;
+    rb = (size_t)wc * sTA;
+  } else {
+    rows = wc;
+    rb = (size_t)W * sTA;
+  }
+}
+
+__host__ __device__ inline DctClusterLayout dct_cluster_layout(bool inverse, int H, int W, size_t sT, size_t sTA) {
+  DctClusterLayout L;
+  const int nph = inverse ? 1 : 3;
+  size_t ring = 0;
+  int nch = 0;
+  for (int q = 0; q < nph; ++q) {
+    int rows;
+    size_t rb;
+    dct_cluster_phase(inverse, q, H, W, sT, sTA, rows, rb);
+    ring += (size_t)rows * rb;
+    nch += (rows + kDsKC - 1) / kDsKC;
+  }
+  L.nch = nch;
+  L.off_left = 8 * kDsMaxSlots;
+  L.off_red = L.off_left + ((size_t)H / kDcNC + (size_t)W + (size_t)W / kDcNC) * kDsRB * sTA;
+  L.off_xch = L.off_red + (size_t)3 * kDsRB * W * sTA;
+  L.off_ring = (L.off_xch + (size_t)kDsRB * W * sTA + 127) & ~(size_t)127;
+  L.bytes = L.off_ring + ring;
+  return L;
+}
+
+template <typename T, typename TA, int NKG, bool INVERSE>
+__global__ void __cluster_dims__(kDcNC, 1, 1) __launch_bounds__(256, 1)
+    k_dct_cluster(int H, int W, const T* __restrict__ b, int64_t ldb, const TA* __restrict__ tab, TA* __restrict__ X,
+                  T* __restrict__ e, int64_t lde, GmgState* __restrict__ st) {
+  namespace cg = cooperative_groups;
+  extern __shared__ __align__(128) unsigned char dc_smem[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int crank = (int)cl.block_rank();
+  const DctClusterLayout lay = dct_cluster_layout(INVERSE, H, W, sizeof(T), sizeof(TA));
+  const int hc = H / kDcNC, wc = W / kDcNC;
+  uint64_t* full = reinterpret_cast<uint64_t*>(dc_smem);
+  TA* L0 = reinterpret_cast<TA*>(dc_smem + lay.off_left);  // [k][r], k < hc
+  TA* L1 = L0 + (size_t)hc * kDsRB;                        // [i][r], i < W
+  TA* L2 = L1 + (size_t)W * kDsRB;                         // [kl][r], kl < wc
+  TA* red = reinterpret_cast<TA*>(dc_smem + lay.off_red);  // [group - 1][r][c]
+  TA* xch = reinterpret_cast<TA*>(dc_smem + lay.off_xch);  // [r][c]
+  unsigned char* ring = dc_smem + lay.off_ring;
+  const TA* cx = tab;                          // cx[k W + i]
+  const TA* cy = cx + 2 * (int64_t)W * W;      // cy[m H + j]
+  const TA* lx = cy + (int64_t)H * H;
+  const TA* ly = lx + W;
+  const TA* cxs = ly + H;                      // C_x^T split by output columns
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int cw = (W + 31) & ~31;
+  const int c = tid % cw, kg = tid / cw;       // column and thread group
+  const int r0 = (blockIdx.x / kDcNC) * kDsRB; // the cluster's first row (m forward, j inverse)
+  const int nph = INVERSE ? 1 : 3;
+  // source of phase q for this CTA, its row stride in bytes and its row length in elements
+  auto phase_src = [&](int q, const unsigned char*& src, int64_t& ldbytes, int& rowlen) {
+    if (INVERSE) {
+      src = reinterpret_cast<const unsigned char*>(X + (int64_t)crank * hc * W);
+      ldbytes = (int64_t)W * sizeof(TA);
+      rowlen = W;
+    } else if (q == 0) {
+      src = reinterpret_cast<const unsigned char*>(b + (int64_t)crank * hc * ldb);
+      ldbytes = ldb * (int64_t)sizeof(T);
+      rowlen = W;
+    } else if (q == 1) {
+      src = reinterpret_cast<const unsigned char*>(cxs + (int64_t)crank * W * wc);
+      ldbytes = (int64_t)wc * sizeof(TA);
+      rowlen = wc;
+    } else {
+      src = reinterpret_cast<const unsigned char*>(cx + (int64_t)crank * wc * W);
+      ldbytes = (int64_t)W * sizeof(TA);
+      rowlen = W;
+    }
+  };
+  if (tid == 0) {
+    for (int k = 0; k < lay.nch; ++k) mbar_init(full + k, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (tid < 32) {  // warp 0 issues the whole stream (every chunk has its own place)
+    const int lane = tid;
+    size_t off = 0;
+    int ch = 0;
+    for (int q = 0; q < nph; ++q) {
+      int rows;
+      size_t rb;
+      dct_cluster_phase(INVERSE, q, H, W, sizeof(T), sizeof(TA), rows, rb);
+      const unsigned char* src;
+      int64_t ldbytes;
+      int rowlen;
+      phase_src(q, src, ldbytes, rowlen);
+      for (int row0 = 0; row0 < rows; row0 += kDsKC, ++ch) {
+        const int nr = min(kDsKC, rows - row0);
+        if (lane == 0) mbar_arrive_expect_tx(full + ch, (uint32_t)(nr * rb));
+        if (ldbytes == (int64_t)rb) {
+          if (lane == 0) bulk_g2s(ring + off, src + (int64_t)row0 * rb, (uint32_t)(nr * rb), full + ch);
+        } else if (lane < nr) {
+          bulk_g2s(ring + off + (size_t)lane * rb, src + (int64_t)(row0 + lane) * ldbytes, (uint32_t)rb, full + ch);
+        }
+        off += (size_t)nr * rb;
+      }
+    }
+  }
+  // the first left factor: forward C_y[r0 + r, crank hc + j] at L0[j][r]; inverse
+  // C_y[crank hc + m, r0 + r] at L0[m][r]
+  for (int q = tid; q < hc * kDsRB; q += nt) {
+    const int k = q / kDsRB, r = q - k * kDsRB;
+    const int row = r0 + r, kk = crank * hc + k;
+    L0[q] = row < H ? (INVERSE ? cy[(int64_t)kk * H + row] : cy[(int64_t)row * H + kk]) : (TA)0;
+  }
+  __syncthreads();
+  bool ok = true;
+  TA acc[kDsRB];
+#pragma unroll
+  for (int r = 0; r < kDsRB; ++r) acc[r] = (TA)0;
+  size_t off = 0;
+  int ch = 0;
+  for (int q = 0; q < nph; ++q) {
+    int rows;
+    size_t rb;
+    dct_cluster_phase(INVERSE, q, H, W, sizeof(T), sizeof(TA), rows, rb);
+    const unsigned char* src;
+    int64_t ldbytes;
+    int rowlen;
+    phase_src(q, src, ldbytes, rowlen);
+    const TA* left = q == 0 ? L0 : (q == 1 ? L1 : L2);
+    for (int row0 = 0; row0 < rows; row0 += kDsKC, ++ch) {
+      const int nr = min(kDsKC, rows - row0);
+      if (!mbar_wait(full + ch, 0)) ok = false;
+      if (c < rowlen) {
+        if (!INVERSE && q == 0 && !std::is_same<T, TA>::value)
+          dct_stream_consume<NKG>(reinterpret_cast<const T*>(ring + off), rowlen, c, kg, nr, left + row0 * kDsRB, acc);
+        else
+          dct_stream_consume<NKG>(reinterpret_cast<const TA*>(ring + off), rowlen, c, kg, nr, left + row0 * kDsRB,
+                                  acc);
+      }
+      off += (size_t)nr * rb;
+    }
+    // the phase's products are complete: sum the thread groups
+    if (NKG > 1) {
+      if (kg > 0 && c < rowlen) {
+#pragma unroll
+        for (int r = 0; r < kDsRB; ++r) red[((size_t)(kg - 1) * kDsRB + r) * W + c] = acc[r];
+      }
+      __syncthreads();
+    }
+    TA v[kDsRB];
+#pragma unroll
+    for (int r = 0; r < kDsRB; ++r) {
+      v[r] = acc[r];
+      acc[r] = (TA)0;
+      if (kg == 0 && c < rowlen) {
+#pragma unroll
+        for (int g = 1; g < NKG; ++g) v[r] += red[((size_t)(g - 1) * kDsRB + r) * W + c];
+      }
+    }
+    const bool partial = INVERSE || q != 1;  // sums over a share of the contraction
+    if (partial) {  // publish, synchronise the cluster, add the partials in rank order
+      if (kg == 0 && c < W) {
+#pragma unroll
+        for (int r = 0; r < kDsRB; ++r) xch[(size_t)r * W + c] = v[r];
+      }
+      cl.sync();
+      if (kg == 0 && c < W) {
+#pragma unroll
+        for (int r = 0; r < kDsRB; ++r) v[r] = (TA)0;
+        for (int rk = 0; rk < kDcNC; ++rk) {
+          const TA* px = cl.map_shared_rank(xch, rk);
+#pragma unroll
+          for (int r = 0; r < kDsRB; ++r) v[r] += px[(size_t)r * W + c];
+        }
+      }
+      cl.sync();  // every CTA has read the partials before any overwrites its own
+    }
+    if (kg == 0) {
+#pragma unroll
+      for (int r = 0; r < kDsRB; ++r) {
+        const int row = r0 + r;
+        if (INVERSE) {
+          if (c < W && c / wc == crank && row < H) e[(int64_t)row * lde + c] = (T)v[r];
+        } else if (q == 0) {
+          if (c < W) L1[c * kDsRB + r] = v[r];
+        } else if (q == 1) {
+          if (c < wc) {
+            const int k = crank * wc + c;
+            L2[c * kDsRB + r] = (row == 0 && k == 0) || row >= H ? (TA)0 : v[r] / (ly[row < H ? row : 0] + lx[k]);
+          }
+        } else if (c < W && c / wc == crank && row < H) {
+          X[(int64_t)row * W + c] = v[r];
+        }
+      }
+    }
+    __syncthreads();  // the next phase's left factor is written
+  }
+  if (!ok) {
+    atomicExch(&st->dev_error, kDevErrBulkWait);
+    for (int k = 0; k < lay.nch; ++k) mbar_wait(full + k, 0);
+  }
+}
+
 template <typename T>
 static size_t coarse_dct_smem(int H, int W) {
   return (size_t)(2 * W * W + H * H + W + H + 2 * H * W) * sizeof(T);
@@ -778,6 +1018,22 @@ static void coarse_dct_tables(int H, int W, std::vector<double>& tab) {
   basis(H, cy, ly);
   for (int k = 0; k < W; ++k)
     for (int i = 0; i < W; ++i) cxt[(size_t)i * W + k] = cx[(size_t)k * W + i];
+}
+
+// The same tables followed by C_x^T split by output columns for a cluster of nc CTAs
+// (k_dct_cluster): part c holds cxt[i][c W / nc + kl] at c W (W / nc) + i (W / nc) + kl, so each
+// CTA's share of the product T1 C_x^T is one contiguous block of rows.
+static void coarse_dct_tables_split(int H, int W, int nc, std::vector<double>& tab) {
+  coarse_dct_tables(H, W, tab);
+  const size_t base = tab.size();
+  const int wc = W / nc;
+  tab.resize(base + (size_t)W * W, 0.0);
+  const double* cxt = tab.data() + (size_t)W * W;
+  double* sp = tab.data() + base;
+  for (int c = 0; c < nc; ++c)
+    for (int i = 0; i < W; ++i)
+      for (int kl = 0; kl < wc; ++kl)
+        sp[(size_t)c * W * wc + (size_t)i * wc + kl] = cxt[(size_t)i * W + c * wc + kl];
 }
 // Levels up to this many cells a side run inside the single-block tail kernel; larger
 // open-box levels use the fused tiled kernels (two launches per level and cycle).
@@ -1052,6 +1308,8 @@ struct sg_gmg_plan {
   int coarse_dct = 0;
   int coarse_dct_multi = 0;  // above kDctMaxSide: the four-product form (k_dct_gemm), scratch at off_dct_x
   int coarse_dct_stream = 0;  // ... run as the two streaming launches (k_dct_stream)
+  int coarse_dct_cluster = 0;  // ... on clusters of kDcNC CTAs (k_dct_cluster), when they fit
+  int64_t dct_cluster_smem[2] = {0, 0};  // forward, inverse
   int dct_fp64 = 0;           // the transform's arithmetic and tables in float64 (FP64 and mixed precision)
   // events recorded around the fused fine-level post launches of kernel-by-kernel solves
   // (pairs, consumed in order; sg_gmg_set_post_events)
@@ -1520,6 +1778,20 @@ static int set_dct_stream_smem(const sg_gmg_plan* p) {
     default: SG_DS_ATTR(1) break;
   }
 #undef SG_DS_ATTR
+  if (e == cudaSuccess && p->coarse_dct_cluster) {
+    const int bf = (int)p->dct_cluster_smem[0], bi = (int)p->dct_cluster_smem[1];
+#define SG_DC_ATTR(NKG)                                                                                            \
+  if (e == cudaSuccess)                                                                                            \
+    e = cudaFuncSetAttribute(k_dct_cluster<T, TA, NKG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bf);   \
+  if (e == cudaSuccess)                                                                                            \
+    e = cudaFuncSetAttribute(k_dct_cluster<T, TA, NKG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bi);
+    switch (dct_stream_groups(p->levels.back().W)) {
+      case 4: SG_DC_ATTR(4) break;
+      case 2: SG_DC_ATTR(2) break;
+      default: SG_DC_ATTR(1) break;
+    }
+#undef SG_DC_ATTR
+  }
   return e == cudaSuccess ? SG_OK : fail(SG_ERR_CUDA, "cosine-transform stream smem: %s", cudaGetErrorString(e));
 }
 
@@ -1528,6 +1800,14 @@ static void dct_stream_launch_g(const sg_gmg_plan* p, const Level& C, cudaStream
   const TA* tab = (const TA*)(p->ws + p->off_dct);
   TA* X = (TA*)(p->ws + p->off_dct_x);
   const int cw = (C.W + 31) / 32 * 32;
+  if (p->coarse_dct_cluster) {
+    const dim3 gc((unsigned)(((C.H + kDsRB - 1) / kDsRB) * kDcNC)), bc(cw * NKG);
+    SG_LAUNCH((k_dct_cluster<T, TA, NKG, false><<<gc, bc, (size_t)p->dct_cluster_smem[0], s>>>(
+        C.H, C.W, ws_ptr<T>(p, C.off_b), C.ld, tab, X, nullptr, 0, state_ptr(p))));
+    SG_LAUNCH((k_dct_cluster<T, TA, NKG, true><<<gc, bc, (size_t)p->dct_cluster_smem[1], s>>>(
+        C.H, C.W, nullptr, 0, tab, X, ws_ptr<T>(p, C.off_e), C.ld, state_ptr(p))));
+    return;
+  }
   const dim3 g((C.H + kDsRB - 1) / kDsRB), b(cw * NKG);
   const size_t sm = (size_t)p->dct_stream_smem;
   SG_LAUNCH((k_dct_stream<T, TA, NKG, false><<<g, b, sm, s>>>(C.H, C.W, ws_ptr<T>(p, C.off_b), C.ld, tab, X, nullptr,
@@ -1904,7 +2184,10 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
     }
     p->coarse_dct = 1;
     p->coarse_dct_multi = std::max(last.H, last.W) > kDctMaxSide ? 1 : 0;
-    coarse_dct_tables(last.H, last.W, p->dct);
+    if (p->coarse_dct_multi && last.H % kDcNC == 0 && last.W % kDcNC == 0)
+      coarse_dct_tables_split(last.H, last.W, kDcNC, p->dct);  // + C_x^T split for k_dct_cluster
+    else
+      coarse_dct_tables(last.H, last.W, p->dct);
   } else {
     std::vector<uint8_t> lastcode = last.analytic ? pack_codes(fl, fu, fv, last.H, last.W) : last.code;
     if (!coarsest_pinv(lastcode, last.H, last.W, p->pinv)) {
@@ -1947,6 +2230,19 @@ int sg_gmg_plan_create(sg_gmg_plan** out, int64_t H, int64_t W, int mask_mode, c
                                                                            : dct_stream_fits<float, float>(C));
     p->coarse_dct_stream = p->coarse_dct_multi && fits ? 1 : 0;
     p->dct_fp64 = precision == SG_GMG_FP64 || (precision == SG_GMG_MIXED && (!p->coarse_dct_multi || fits)) ? 1 : 0;
+    if (p->coarse_dct_stream) {
+      const size_t sT = precision == SG_GMG_FP64 ? 8 : 4, sTA = p->dct_fp64 ? 8 : 4;
+      const DctClusterLayout lf = dct_cluster_layout(false, C.H, C.W, sT, sTA);
+      const DctClusterLayout li = dct_cluster_layout(true, C.H, C.W, sT, sTA);
+      const size_t split_off = (2 * (size_t)C.W * C.W + (size_t)C.H * C.H + C.W + C.H) * sTA;
+      const bool cfit = C.H % kDcNC == 0 && C.W % kDcNC == 0 && ((size_t)(C.W / kDcNC) * sTA) % 16 == 0 &&
+                        split_off % 16 == 0 && p->dct.size() == 3 * (size_t)C.W * C.W + (size_t)C.H * C.H + C.W + C.H &&
+                        std::max(lf.bytes, li.bytes) <= (size_t)kDsSmemBudget && lf.nch <= kDsMaxSlots &&
+                        li.nch <= kDsMaxSlots;
+      p->coarse_dct_cluster = cfit ? 1 : 0;
+      p->dct_cluster_smem[0] = (int64_t)lf.bytes;
+      p->dct_cluster_smem[1] = (int64_t)li.bytes;
+    }
     p->dct_stream_smem = !p->coarse_dct_stream ? 0
                          : (int64_t)(p->dct_fp64 ? dct_stream_layout<double>(C.H, C.W).bytes
                                                  : dct_stream_layout<float>(C.H, C.W).bytes);
@@ -2271,7 +2567,7 @@ int sg_gmg_set_post_events(sg_gmg_plan* plan, void* const* events, int n_pairs) 
 int sg_gmg_coarse_solve_kind(const sg_gmg_plan* plan) {
   if (!plan) return -1;
   if (!plan->coarse_dct) return 0;
-  return plan->coarse_dct_stream ? 3 : (plan->coarse_dct_multi ? 2 : 1);
+  return plan->coarse_dct_cluster ? 4 : (plan->coarse_dct_stream ? 3 : (plan->coarse_dct_multi ? 2 : 1));
 }
 
 int sg_gmg_fine_kernel_async(sg_gmg_plan* plan, int which, void* p, int64_t ld_p, void* stream) {

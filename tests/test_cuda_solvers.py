@@ -153,7 +153,7 @@ def test_gmg_one_cycle_large_cosine_coarsest_vs_oracle(shape, coarsest, cycle, p
     plan = solver.current_plan()
     Wc = plan.level_shape(plan.num_levels - 1)[1]
     streams = (Wc * (8 if precision == "fp64" else 4)) % 16 == 0
-    assert plan.coarse_solve_kind() == plan.COARSE_SOLVE_KINDS[3 if streams else 2]
+    assert plan.coarse_solve_kind() in (plan.COARSE_SOLVE_KINDS[3:] if streams else plan.COARSE_SOLVE_KINDS[2:3])
 
 
 def test_gmg_large_cosine_coarsest_reaches_1e8_in_no_more_cycles():
