@@ -426,7 +426,7 @@ int sg_gmg_fine_fused(const sg_gmg_plan* plan);
 /* How the plan solves its coarsest level exactly: 0 dense pseudo-inverse, 1 cosine transform
  * in one block, 2 cosine transform as four tiled products, 3 cosine transform as two launches
  * streaming their operands into shared memory with bulk asynchronous copies (when the
- * level's rows are whole 16-byte units), 4 the same on clusters of two CTAs that split every
+ * level's rows are whole 16-byte units), 4 the same on clusters of four CTAs that split every
  * product (when each CTA's share of the stream fits in its shared memory); -1 for a NULL
  * plan. No counterpart in the reference. */
 int sg_gmg_coarse_solve_kind(const sg_gmg_plan* plan);

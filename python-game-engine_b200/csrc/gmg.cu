@@ -767,7 +767,7 @@ __global__ void __launch_bounds__(256, 1) k_dct_stream(int H, int W, const T* __
 // synchronises, and every CTA adds the kDcNC partials in rank order (so all hold the same
 // bits of T1); X and e are written by column shares. Rows, chunks and waits as in
 // k_dct_stream, except that every chunk has its own place in shared memory.
-constexpr int kDcNC = 2;
+constexpr int kDcNC = 4;
 
 struct DctClusterLayout {
   int nch;          // chunks in the stream

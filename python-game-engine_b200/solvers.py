@@ -338,7 +338,7 @@ class GMGPlan:
 
     COARSE_SOLVE_KINDS = ("pseudo-inverse", "cosine transform (one block)", "cosine transform (four products)",
                           "cosine transform (two streaming launches)",
-                          "cosine transform (two streaming launches on 2-CTA clusters)")
+                          "cosine transform (two streaming launches on 4-CTA clusters)")
 
     def set_post_events(self, events):
         """Record the torch.cuda.Events (timing enabled, each already recorded once so that it
