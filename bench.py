@@ -562,7 +562,7 @@ def run_ours(args):
             dist.destroy_process_group()
         return 0
     # ---- end to end through the public API with host buffers
-    ms_e2e, _, _, _ = timed(sim, args.steps, 1, e2e=True)
+    ms_e2e, _, _, _ = timed(sim, args.steps, args.warmup, e2e=True)
     ms_e2e = max_over_ranks(ms_e2e)
     e2e_value = world * cells * args.steps / (ms_e2e / 1e3)
     h2d = 6 * 8 * len(sim.plumes)
