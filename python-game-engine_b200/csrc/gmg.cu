@@ -1311,6 +1311,8 @@ struct sg_gmg_plan {
   int coarse_dct_cluster = 0;  // ... on clusters of kDcNC CTAs (k_dct_cluster), when they fit
   int64_t dct_cluster_smem[2] = {0, 0};  // forward, inverse
   int dct_fp64 = 0;           // the transform's arithmetic and tables in float64 (FP64 and mixed precision)
+  // the first cycle of a graph solve from a zero guess (set while its graph is captured)
+  mutable sg::FirstCycle fc{nullptr, 0, 0, 0, 0, 0.0, 0.0};
   // events recorded around the fused fine-level post launches of kernel-by-kernel solves
   // (pairs, consumed in order; sg_gmg_set_post_events)
   mutable std::vector<cudaEvent_t> post_ev;
@@ -1701,11 +1703,13 @@ static void launch_post_final(const sg_gmg_plan* p, TP* pp, int64_t ldp, cudaStr
   if (staged) {
     SG_LAUNCH(k_gmg_post_final_stage<TC, TP, SW, RPT, NW, MB><<<post_final_grid<TC>(p), 32 * NW, 0, s>>>(
         ws_ptr<TC>(p, L.off_e2), ws_ptr<TC>(p, L.off_b), ws_ptr<TC>(p, p->off_b2), state_ptr(p), L.ld, L.H, L.W,
-        ws_ptr<TC>(p, C.off_e), C.ld, C.H, C.W, (TC)p->omega, pp, ldp, r64, (double*)(p->ws + p->off_partial)));
+        ws_ptr<TC>(p, C.off_e), C.ld, C.H, C.W, (TC)p->omega, pp, ldp, r64, (double*)(p->ws + p->off_partial),
+        p->fc));
   } else {
     SG_LAUNCH(k_gmg_post_final_reg<TC, TP, SW, RPT, NW, MB><<<post_final_grid<TC>(p), 32 * NW, 0, s>>>(
         ws_ptr<TC>(p, L.off_e2), ws_ptr<TC>(p, L.off_b), ws_ptr<TC>(p, p->off_b2), state_ptr(p), L.ld, L.H, L.W,
-        ws_ptr<TC>(p, C.off_e), C.ld, C.H, C.W, (TC)p->omega, pp, ldp, r64, (double*)(p->ws + p->off_partial)));
+        ws_ptr<TC>(p, C.off_e), C.ld, C.H, C.W, (TC)p->omega, pp, ldp, r64, (double*)(p->ws + p->off_partial),
+        p->fc));
   }
   if (ev1) cudaEventRecord(ev1, s);
 }
@@ -1931,9 +1935,12 @@ static void prologue(const sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div, i
   // from a zero guess the fused fine level carries the residual from here on (b0 / r64), so
   // the FP64 rhs itself is not kept
   TP* bkeep = (zero_guess && p->fused_ir && p->inner <= 1) ? nullptr : bf;
+  // the first cycle of such a solve forms r64 from the divergence itself (FirstCycle), so the
+  // prologue does not write it
   SG_LAUNCH(k_gmg_rhs<TD, TP, TC><<<g, block2d(), 0, s>>>(L.H, L.W, div, ldd, st, m, bkeep, p->ld_bfine, part,
                                                           zero_guess ? pp : nullptr, ldp, ws_ptr<TC>(p, L.off_b), L.ld,
-                                                          r64, p->remove_mean));
+                                                          (zero_guess && p->fc.active) ? nullptr : r64,
+                                                          p->remove_mean));
   SG_LAUNCH(k_gmg_finalize_norm<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st));
   if (zero_guess) {
     SG_LAUNCH(k_gmg_finalize_rel<<<1, 1024, 0, s>>>(part, (int)(g.x * g.y), st, h, use_handle, 0));
@@ -2004,6 +2011,16 @@ static int build_graph(sg_gmg_plan* p, TP* pp, int64_t ldp, const TD* div, int64
   SG_CUDA_TRY(cudaGraphCreate(&g, 0), "cudaGraphCreate");
   cudaGraphConditionalHandle h;
   SG_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, g, 0, 0), "cudaGraphConditionalHandleCreate");
+  // a zero-guess solve on the fused fine level starts from p = 0 and r64 = alpha div: its first
+  // post kernel forms both itself when the divergence rows can be staged (16-byte units)
+  struct FcGuard {
+    const sg_gmg_plan* p;
+    ~FcGuard() { p->fc = FirstCycle{nullptr, 0, 0, 0, 0, 0.0, 0.0}; }
+  } fc_guard{p};
+  const bool fc_ok = zero_guess && p->fused_ir && p->inner <= 1 && ((uintptr_t)div % 16) == 0 &&
+                     ((size_t)ldd * sizeof(TD)) % 16 == 0;
+  p->fc = FirstCycle{fc_ok ? (const void*)div : nullptr, ldd, sizeof(TD) == 8 ? 1 : 0, p->remove_mean ? 1 : 0,
+                     fc_ok ? 1 : 0, 0.0, 0.0};
   SG_CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
               "begin capture");
   unsigned long long c0 = counter();

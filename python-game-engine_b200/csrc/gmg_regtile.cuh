@@ -22,6 +22,27 @@
 
 constexpr int kRW = 64;  // tile columns: 32 lanes x 2
 
+// The first cycle of a solve from a zero guess, for the fused fine-level post kernel: p is 0
+// on entry (not read), and when div is set the carried float64 residual r64 starts as
+// alpha div (- the fluid mean with sub_mean), formed here from the divergence instead of being
+// written by the prologue and read back. div: float32 (f64 = 0) or float64 values, row stride
+// ldd. active = 0: an ordinary cycle. alpha and mean are filled in on the device from the
+// solve state by the kernel that takes the struct.
+struct FirstCycle {
+  const void* div;
+  int64_t ldd;
+  int f64;
+  int sub_mean;
+  int active;
+  double alpha, mean;
+};
+__device__ __forceinline__ double first_cycle_rhs(const FirstCycle& fc, int64_t o) {
+  const double d = fc.f64 ? ((const double*)fc.div)[o] : (double)((const float*)fc.div)[o];
+  double x = fc.alpha * d;
+  if (fc.sub_mean) x -= fc.mean;
+  return x;
+}
+
 template <typename T>
 struct Pair;
 template <>
@@ -471,14 +492,15 @@ __device__ __forceinline__ void reg_post_final_body(RegXchg<TC, NWARP>& x, const
                                                     const TC* __restrict__ bsrc, TC* __restrict__ bdst, int64_t ld,
                                                     int H, int W, const TC* __restrict__ ec, int64_t ldc, int Hc,
                                                     int Wc, TC omega, TP* __restrict__ p, int64_t ldp,
-                                                    TP* __restrict__ r64, int i0, int j0, double& sq) {
+                                                    TP* __restrict__ r64, int i0, int j0, double& sq,
+                                                    const FirstCycle& fc = FirstCycle{nullptr, 0, 0, 0, 0, 0.0, 0.0}) {
   using S = RegPre<TC, SW, RPT, NWARP>;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int i = i0 + 2 * lane, j = j0 + w * RPT;
   const bool cols_owned = 2 * lane >= S::HALO && 2 * lane < S::HALO + S::TXO && (!BOUNDED || i < W);
   const int r_lo = S::HALO - w * RPT, r_hi = S::HALO + S::TYO - w * RPT;
   // p and r64 are only needed after the sweeps: start bringing the owned rows into L2 now
-  if (cols_owned) {
+  if (cols_owned && !fc.active) {
 #pragma unroll
     for (int r = 0; r < RPT; ++r) {
       if (r < r_lo || r >= r_hi || (BOUNDED && j + r >= H)) continue;
@@ -502,7 +524,11 @@ __device__ __forceinline__ void reg_post_final_body(RegXchg<TC, NWARP>& x, const
     if (!SG_IN_BOUNDS(jj >= 0 && jj < H && i >= 0 && (BOUNDED || i + 1 < W))) continue;
     const int64_t o = (int64_t)jj * ld + i;
     TP acc[2];
-    if (r64 && !BOUNDED) {
+    if (fc.active && r64) {  // the first cycle's residual, from the divergence
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+        acc[q] = (!BOUNDED || i + q < W) ? (TP)first_cycle_rhs(fc, (int64_t)jj * fc.ldd + i + q) : (TP)0;
+    } else if (r64 && !BOUNDED) {
       const VP t = *reinterpret_cast<const VP*>(r64 + o);
       acc[0] = t.x;
       acc[1] = t.y;
@@ -539,8 +565,8 @@ __device__ __forceinline__ void reg_post_final_body(RegXchg<TC, NWARP>& x, const
     }
     TP* pc = p + (int64_t)jj * ldp + i;
     if (!BOUNDED) {
-      pc[0] = pc[0] + xv[0];
-      pc[1] = pc[1] + xv[1];
+      pc[0] = (fc.active ? (TP)0 : pc[0]) + xv[0];
+      pc[1] = (fc.active ? (TP)0 : pc[1]) + xv[1];
       if (r64) {
         VP t;
         t.x = acc[0];
@@ -557,7 +583,7 @@ __device__ __forceinline__ void reg_post_final_body(RegXchg<TC, NWARP>& x, const
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         if (i + q >= W) continue;
-        pc[q] = pc[q] + xv[q];
+        pc[q] = (fc.active ? (TP)0 : pc[q]) + xv[q];
         if (r64) r64[o + q] = acc[q];
         bdst[o + q] = (TC)acc[q];
         sq += (double)acc[q] * (double)acc[q];
@@ -572,7 +598,7 @@ __global__ void __launch_bounds__(32 * NWARP, MINB)
     k_gmg_post_final_reg(const TC* __restrict__ e_in, TC* __restrict__ b0, TC* __restrict__ b1,
                          const GmgState* __restrict__ st, int64_t ld, int H, int W, const TC* __restrict__ ec,
                          int64_t ldc, int Hc, int Wc, TC omega, TP* __restrict__ p, int64_t ldp, TP* __restrict__ r64,
-                         double* __restrict__ partial) {
+                         double* __restrict__ partial, FirstCycle fc) {
   using S = RegPre<TC, SW, RPT, NWARP>;
   __shared__ RegXchg<TC, NWARP> x;
   const bool odd = st->cycles & 1;
@@ -582,12 +608,15 @@ __global__ void __launch_bounds__(32 * NWARP, MINB)
   const int j0 = blockIdx.y * S::TYO - S::HALO;
   const bool inside = i0 >= 0 && i0 + kRW <= W && j0 >= 0 && j0 + NWARP * RPT <= H;
   double sq = 0.0;
+  fc.active = fc.active && st->cycles == 0;
+  fc.alpha = st->alpha;
+  fc.mean = st->bmean;
   if (inside)
     reg_post_final_body<TC, TP, SW, RPT, NWARP, false>(x, e_in, bsrc, bdst, ld, H, W, ec, ldc, Hc, Wc, omega, p, ldp,
-                                                      r64, i0, j0, sq);
+                                                      r64, i0, j0, sq, fc);
   else
     reg_post_final_body<TC, TP, SW, RPT, NWARP, true>(x, e_in, bsrc, bdst, ld, H, W, ec, ldc, Hc, Wc, omega, p, ldp,
-                                                     r64, i0, j0, sq);
+                                                     r64, i0, j0, sq, fc);
   const double s = block_sum(sq);
   if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
 }

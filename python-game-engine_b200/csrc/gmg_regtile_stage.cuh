@@ -25,7 +25,8 @@ __device__ __forceinline__ void reg_post_final_body_staged(RegXchg<TC, NWARP>& x
                                                            TC* __restrict__ bdst, int64_t ld, int H, int W,
                                                            const TC* __restrict__ ec, int64_t ldc, int Hc, int Wc,
                                                            TC omega, TP* __restrict__ p, int64_t ldp,
-                                                           TP* __restrict__ r64, int i0, int j0, double& sq, bool& ok) {
+                                                           TP* __restrict__ r64, int i0, int j0, double& sq, bool& ok,
+                                                           const FirstCycle& fc, bool staged_any) {
   using S = RegPre<TC, SW, RPT, NWARP>;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int i = i0 + 2 * lane, j = j0 + w * RPT;
@@ -36,7 +37,7 @@ __device__ __forceinline__ void reg_post_final_body_staged(RegXchg<TC, NWARP>& x
   TC above[2], below[2];
   exchange_rows<TC, RPT, NWARP>(x, (2 * SW) & 1, e, w, lane, above, below);
   // every thread waits, so the block cannot retire while a copy is still landing
-  if (!mbar_wait(&sp.bar, 0)) ok = false;
+  if (staged_any && !mbar_wait(&sp.bar, 0)) ok = false;
   using VC = typename Pair<TC>::V;
   using VP = typename Pair<TP>::V;
   const int cs = 2 * lane - S::HALO;  // the thread's first column in the staged rows
@@ -52,7 +53,17 @@ __device__ __forceinline__ void reg_post_final_body_staged(RegXchg<TC, NWARP>& x
       continue;
     const int64_t o = (int64_t)jj * ld + i;
     TP acc[2];
-    if (r64) {
+    if (fc.active && r64) {  // the first cycle's residual, from the staged divergence rows
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int64_t so = (int64_t)k * S::TXO + cs + q;
+        const double d = fc.f64 ? reinterpret_cast<const double*>(sp.p)[so]
+                                : (double)reinterpret_cast<const float*>(sp.p)[so];
+        double x2 = fc.alpha * d;
+        if (fc.sub_mean) x2 -= fc.mean;
+        acc[q] = (TP)x2;
+      }
+    } else if (r64) {
       const VP t = *reinterpret_cast<const VP*>(sp.r + k * S::TXO + cs);
       acc[0] = t.x;
       acc[1] = t.y;
@@ -77,7 +88,13 @@ __device__ __forceinline__ void reg_post_final_body_staged(RegXchg<TC, NWARP>& x
         acc[q] += down - xv[q];
       }
     }
-    const VP pv = *reinterpret_cast<const VP*>(sp.p + k * S::TXO + cs);
+    VP pv;
+    if (fc.active) {  // p is 0 on a solve's first cycle from a zero guess
+      pv.x = (TP)0;
+      pv.y = (TP)0;
+    } else {
+      pv = *reinterpret_cast<const VP*>(sp.p + k * S::TXO + cs);
+    }
     VP pn;
     pn.x = pv.x + xv[0];
     pn.y = pv.y + xv[1];
@@ -106,7 +123,7 @@ __global__ void __launch_bounds__(32 * NWARP, MINB)
     k_gmg_post_final_stage(const TC* __restrict__ e_in, TC* __restrict__ b0, TC* __restrict__ b1,
                            GmgState* __restrict__ st, int64_t ld, int H, int W, const TC* __restrict__ ec,
                            int64_t ldc, int Hc, int Wc, TC omega, TP* __restrict__ p, int64_t ldp,
-                           TP* __restrict__ r64, double* __restrict__ partial) {
+                           TP* __restrict__ r64, double* __restrict__ partial, FirstCycle fc) {
   using S = RegPre<TC, SW, RPT, NWARP>;
   static_assert((S::TXO * sizeof(TP)) % 16 == 0, "staged rows must be whole 16-byte units");
   static_assert(2 * S::TYO <= 32 * NWARP, "one thread per staged row");
@@ -119,31 +136,43 @@ __global__ void __launch_bounds__(32 * NWARP, MINB)
   const int j0 = blockIdx.y * S::TYO - S::HALO;
   const bool inside = i0 >= 0 && i0 + kRW <= W && j0 >= 0 && j0 + NWARP * RPT <= H;
   double sq = 0.0;
+  fc.active = fc.active && st->cycles == 0;  // the first cycle of a solve from a zero guess
+  fc.alpha = st->alpha;
+  fc.mean = st->bmean;
   if (inside) {
     const int t = threadIdx.x;
-    if (t == 0) {
-      mbar_init(&sp.bar, 1);
-      mbar_fence_init();
-    }
-    __syncthreads();
-    constexpr uint32_t kRowBytes = S::TXO * sizeof(TP);
-    const int nrow = r64 ? 2 * S::TYO : S::TYO;
-    if (t == 0) mbar_arrive_expect_tx(&sp.bar, (uint32_t)nrow * kRowBytes);
-    if (t < nrow) {
-      const int k = t < S::TYO ? t : t - S::TYO;
-      const int64_t jj = j0 + S::HALO + k, ii = i0 + S::HALO;
-      if (t < S::TYO)
-        bulk_g2s(sp.p + k * S::TXO, p + jj * ldp + ii, kRowBytes, &sp.bar);
-      else
-        bulk_g2s(sp.r + k * S::TXO, r64 + jj * ld + ii, kRowBytes, &sp.bar);
+    // rows to stage: p and r64 (or p alone); on the first cycle only the divergence rows that
+    // form r64 (p is 0), or nothing without r64
+    const int nrow = fc.active ? (r64 ? S::TYO : 0) : (r64 ? 2 * S::TYO : S::TYO);
+    if (nrow > 0) {
+      if (t == 0) {
+        mbar_init(&sp.bar, 1);
+        mbar_fence_init();
+      }
+      __syncthreads();
+      constexpr uint32_t kRowBytes = S::TXO * sizeof(TP);
+      const uint32_t div_bytes = (uint32_t)S::TXO * (fc.f64 ? 8u : 4u);
+      if (t == 0) mbar_arrive_expect_tx(&sp.bar, (uint32_t)nrow * (fc.active ? div_bytes : kRowBytes));
+      if (t < nrow) {
+        const int k = t < S::TYO ? t : t - S::TYO;
+        const int64_t jj = j0 + S::HALO + k, ii = i0 + S::HALO;
+        if (fc.active)
+          bulk_g2s(reinterpret_cast<unsigned char*>(sp.p) + (size_t)k * div_bytes,
+                   reinterpret_cast<const unsigned char*>(fc.div) + (jj * fc.ldd + ii) * (fc.f64 ? 8 : 4), div_bytes,
+                   &sp.bar);
+        else if (t < S::TYO)
+          bulk_g2s(sp.p + k * S::TXO, p + jj * ldp + ii, kRowBytes, &sp.bar);
+        else
+          bulk_g2s(sp.r + k * S::TXO, r64 + jj * ld + ii, kRowBytes, &sp.bar);
+      }
     }
     bool ok = true;
     reg_post_final_body_staged<TC, TP, SW, RPT, NWARP>(x, sp, e_in, bsrc, bdst, ld, H, W, ec, ldc, Hc, Wc, omega, p,
-                                                       ldp, r64, i0, j0, sq, ok);
+                                                       ldp, r64, i0, j0, sq, ok, fc, nrow > 0);
     if (!ok) atomicExch(&st->dev_error, kDevErrBulkWait);
   } else {
     reg_post_final_body<TC, TP, SW, RPT, NWARP, true>(x, e_in, bsrc, bdst, ld, H, W, ec, ldc, Hc, Wc, omega, p, ldp,
-                                                     r64, i0, j0, sq);
+                                                     r64, i0, j0, sq, fc);
   }
   const double s = block_sum(sq);
   if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;

@@ -373,3 +373,30 @@ def test_gmg_fused_post_kernel_staged_and_unstaged_agree(precision, pdtype):
         out.append((p.clone(), solver.last_relres))
     assert torch.equal(out[0][0], out[1][0])
     assert out[0][1] == out[1][1]
+
+
+@pytest.mark.parametrize("precision,remove_mean", [("mixed", False), ("mixed", True), ("fp64", False)])
+def test_gmg_first_cycle_from_divergence_equals_prologue_residual(precision, remove_mean):
+    """A graph solve from a zero guess on the fused fine level lets its first post kernel take
+    p = 0 and, in mixed precision, form the carried float64 residual alpha div (- the fluid
+    mean) from the divergence itself; a divergence whose rows are off 16-byte boundaries falls
+    back to the prologue writing that residual and the kernel reading it. Both must give the
+    same bits: pressure, cycle count and relative residual."""
+    H, W = 1024, 1280
+    _, _, _, div = _problem(H, W, False, 9)
+    d = dev(div.astype(np.float32))
+    base = torch.zeros((H, W + 4), dtype=torch.float32, device="cuda")
+    base[:, 1:W + 1] = d
+    d_off = base[:, 1:W + 1]
+    assert d_off.data_ptr() % 16 != 0
+    out = []
+    for dd in (d, d_off):
+        p = torch.zeros((H, W), dtype=torch.float64, device="cuda")
+        solver = sg.GeometricMultigridSolver()
+        solver(p, dd, sg.OPEN_BOX, sg.OPEN_BOX, 0.7, 1.0, 1.0, tol=1e-8, max_cycles=30, precision=precision,
+               coarsest=32, omega=OMEGA, zero_initial_guess=True, remove_mean=remove_mean)
+        assert solver.current_plan().fine_fused()
+        out.append((p.clone(), solver.last_cycles, solver.last_relres))
+    assert out[0][1] == out[1][1] and out[0][1] >= 3
+    assert out[0][2] == out[1][2] and out[0][2] <= 1e-8
+    assert torch.equal(out[0][0], out[1][0])
