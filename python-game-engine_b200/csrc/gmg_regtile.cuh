@@ -495,12 +495,15 @@ __device__ __forceinline__ void reg_post_final_body(RegXchg<TC, NWARP>& x, const
                                                     TP* __restrict__ r64, int i0, int j0, double& sq,
                                                     const FirstCycle& fc = FirstCycle{nullptr, 0, 0, 0, 0, 0.0, 0.0}) {
   using S = RegPre<TC, SW, RPT, NWARP>;
+  // only mixed precision carries r64; the other instantiations compile without the first-cycle
+  // path (which would cost them registers)
+  const bool first = sizeof(TC) != sizeof(TP) && fc.active;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int i = i0 + 2 * lane, j = j0 + w * RPT;
   const bool cols_owned = 2 * lane >= S::HALO && 2 * lane < S::HALO + S::TXO && (!BOUNDED || i < W);
   const int r_lo = S::HALO - w * RPT, r_hi = S::HALO + S::TYO - w * RPT;
   // p and r64 are only needed after the sweeps: start bringing the owned rows into L2 now
-  if (cols_owned && !fc.active) {
+  if (cols_owned && !first) {
 #pragma unroll
     for (int r = 0; r < RPT; ++r) {
       if (r < r_lo || r >= r_hi || (BOUNDED && j + r >= H)) continue;
@@ -524,7 +527,7 @@ __device__ __forceinline__ void reg_post_final_body(RegXchg<TC, NWARP>& x, const
     if (!SG_IN_BOUNDS(jj >= 0 && jj < H && i >= 0 && (BOUNDED || i + 1 < W))) continue;
     const int64_t o = (int64_t)jj * ld + i;
     TP acc[2];
-    if (fc.active && r64) {  // the first cycle's residual, from the divergence
+    if (first && r64) {  // the first cycle's residual, from the divergence
 #pragma unroll
       for (int q = 0; q < 2; ++q)
         acc[q] = (!BOUNDED || i + q < W) ? (TP)first_cycle_rhs(fc, (int64_t)jj * fc.ldd + i + q) : (TP)0;
@@ -565,8 +568,8 @@ __device__ __forceinline__ void reg_post_final_body(RegXchg<TC, NWARP>& x, const
     }
     TP* pc = p + (int64_t)jj * ldp + i;
     if (!BOUNDED) {
-      pc[0] = (fc.active ? (TP)0 : pc[0]) + xv[0];
-      pc[1] = (fc.active ? (TP)0 : pc[1]) + xv[1];
+      pc[0] = (first ? (TP)0 : pc[0]) + xv[0];
+      pc[1] = (first ? (TP)0 : pc[1]) + xv[1];
       if (r64) {
         VP t;
         t.x = acc[0];
@@ -583,7 +586,7 @@ __device__ __forceinline__ void reg_post_final_body(RegXchg<TC, NWARP>& x, const
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         if (i + q >= W) continue;
-        pc[q] = (fc.active ? (TP)0 : pc[q]) + xv[q];
+        pc[q] = (first ? (TP)0 : pc[q]) + xv[q];
         if (r64) r64[o + q] = acc[q];
         bdst[o + q] = (TC)acc[q];
         sq += (double)acc[q] * (double)acc[q];
@@ -608,7 +611,7 @@ __global__ void __launch_bounds__(32 * NWARP, MINB)
   const int j0 = blockIdx.y * S::TYO - S::HALO;
   const bool inside = i0 >= 0 && i0 + kRW <= W && j0 >= 0 && j0 + NWARP * RPT <= H;
   double sq = 0.0;
-  fc.active = fc.active && st->cycles == 0;
+  fc.active = sizeof(TC) != sizeof(TP) && fc.active && st->cycles == 0;
   fc.alpha = st->alpha;
   fc.mean = st->bmean;
   if (inside)

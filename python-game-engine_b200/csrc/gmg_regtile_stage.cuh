@@ -53,7 +53,7 @@ __device__ __forceinline__ void reg_post_final_body_staged(RegXchg<TC, NWARP>& x
       continue;
     const int64_t o = (int64_t)jj * ld + i;
     TP acc[2];
-    if (fc.active && r64) {  // the first cycle's residual, from the staged divergence rows
+    if (sizeof(TC) != sizeof(TP) && fc.active && r64) {  // the first cycle's r64, from the staged divergence
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         const int64_t so = (int64_t)k * S::TXO + cs + q;
@@ -89,7 +89,7 @@ __device__ __forceinline__ void reg_post_final_body_staged(RegXchg<TC, NWARP>& x
       }
     }
     VP pv;
-    if (fc.active) {  // p is 0 on a solve's first cycle from a zero guess
+    if (sizeof(TC) != sizeof(TP) && fc.active) {  // p is 0 on a solve's first cycle from a zero guess
       pv.x = (TP)0;
       pv.y = (TP)0;
     } else {
@@ -136,7 +136,8 @@ __global__ void __launch_bounds__(32 * NWARP, MINB)
   const int j0 = blockIdx.y * S::TYO - S::HALO;
   const bool inside = i0 >= 0 && i0 + kRW <= W && j0 >= 0 && j0 + NWARP * RPT <= H;
   double sq = 0.0;
-  fc.active = fc.active && st->cycles == 0;  // the first cycle of a solve from a zero guess
+  // the first cycle of a solve from a zero guess (mixed precision only: the others carry no r64)
+  fc.active = sizeof(TC) != sizeof(TP) && fc.active && st->cycles == 0;
   fc.alpha = st->alpha;
   fc.mean = st->bmean;
   if (inside) {
