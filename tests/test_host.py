@@ -287,3 +287,61 @@ def test_batch_create_rejects_bad_scenes():
     assert rc == L.SG_ERR_ARG and not h.value and b"grid" in L.load().sg_last_error()
     rc, h = _batch_create([sc], tol=0.0)
     assert rc == L.SG_ERR_ARG and not h.value
+
+
+@pytest.mark.parametrize("H,W,coarsest,precision,kind", [
+    (64, 64, 8, L.SG_GMG_MIXED, 0), (2048, 2048, 32, L.SG_GMG_MIXED, 1), (2048, 2048, 128, L.SG_GMG_MIXED, 4),
+    (2048, 2048, 128, L.SG_GMG_FP64, 4), (2048, 2048, 128, L.SG_GMG_FP32, 4), (2048, 2048, 256, L.SG_GMG_MIXED, 3),
+    (300, 260, 80, L.SG_GMG_FP64, 2), (300, 260, 80, L.SG_GMG_MIXED, 2)])
+def test_gmg_coarse_solve_kind_is_decided_on_the_host(H, W, coarsest, precision, kind):
+    """Which exact coarsest solve a plan runs is fixed at plan creation: the dense pseudo-inverse
+    (<= 16 a side), the one-block cosine transform (<= 64), the streaming transform on 4-CTA
+    clusters when each CTA's share of its operands fits shared memory (128^2 in every precision),
+    the single-CTA streaming transform when the level's rows are whole 16-byte units (256^2),
+    and the four tiled products otherwise (a 75 x 65 level: rows of 65 values)."""
+    lib = L.load()
+    rc, h = _plan(H, W, coarsest=coarsest, precision=precision)
+    assert rc == L.SG_OK
+    try:
+        assert lib.sg_gmg_coarse_solve_kind(h) == kind
+    finally:
+        lib.sg_gmg_plan_destroy(h)
+    assert lib.sg_gmg_coarse_solve_kind(None) == -1
+
+
+def test_new_entry_points_reject_bad_arguments_without_a_gpu():
+    """The read-back staging copy, the float32-arithmetic forces / projection tail and the
+    multigrid timing hook validate their arguments before any launch."""
+    lib = L.load()
+    null = None
+    fake = ctypes.c_void_p(256)
+    # staging copy: 16-byte units only, strides at least the row length
+    rc = lib.sg_stage_copy(4, 40, fake, 48, fake, 48, null)
+    assert rc == L.SG_ERR_ARG and b"16 bytes" in lib.sg_last_error()
+    rc = lib.sg_stage_copy(4, 64, fake, 48, fake, 64, null)
+    assert rc == L.SG_ERR_ARG
+    assert lib.sg_stage_copy(0, 64, fake, 64, fake, 64, null) == L.SG_OK  # nothing to copy
+    # float32-arithmetic forces: grid, pointers, strides
+    rc = lib.sg_apply_forces_f32(0, 4, fake, 4, fake, 4, null, 0, 0.1, -9.8, 0.0, 1.0, 0.0, null)
+    assert rc == L.SG_ERR_ARG and b"grid" in lib.sg_last_error()
+    rc = lib.sg_apply_forces_f32(4, 4, fake, 3, fake, 4, null, 0, 0.1, -9.8, 0.0, 1.0, 0.0, null)
+    assert rc == L.SG_ERR_ARG
+    # float32-arithmetic projection tail: out of place only, known masks
+    a = [fake, 5, fake, 4, ctypes.c_void_p(512), 5, ctypes.c_void_p(768), 4, fake, 4]
+    rc = lib.sg_project_metrics_f32(4, 4, fake, 5, fake, 4, fake, 5, fake, 4, fake, 4, L.SG_MASK_OPEN, null, 0, null,
+                                    0, null, 0, 0, null, 0, 1.0, 0.25, 0.1, -1.0, 0.25, fake, 4, fake, 4, null)
+    assert rc == L.SG_ERR_ARG and b"out of place" in lib.sg_last_error()
+    rc = lib.sg_project_metrics_f32(4, 4, *a, 9, null, 0, null, 0, null, 0, 0, null, 0, 1.0, 0.25, 0.1, -1.0, 0.25,
+                                    fake, 4, fake, 4, null)
+    assert rc == L.SG_ERR_ARG
+    # timing hook: needs a plan, and events for every pair
+    assert lib.sg_gmg_set_post_events(None, None, 0) == L.SG_ERR_ARG
+    rc, h = _plan(256, 256)
+    assert rc == L.SG_OK
+    try:
+        assert lib.sg_gmg_set_post_events(h, None, 2) == L.SG_ERR_ARG
+        two = (ctypes.c_void_p * 2)(None, None)
+        assert lib.sg_gmg_set_post_events(h, two, 1) == L.SG_ERR_ARG
+        assert lib.sg_gmg_set_post_events(h, None, 0) == L.SG_OK
+    finally:
+        lib.sg_gmg_plan_destroy(h)
