@@ -164,7 +164,10 @@ __global__ void k_apply_forces_f32(int H, int W, float* __restrict__ v, int ldv,
 // and residual.py:6-42 on the projected field) as k_project_metrics walks it -- a warp owns 32
 // columns and walks kTailRowsF rows, each face projected once -- with float32 arithmetic in
 // place of the reference's float64 intermediates.
-constexpr int kTailRowsF = 8;
+#ifndef SG_TAIL_ROWS_F32
+#define SG_TAIL_ROWS_F32 8
+#endif
+constexpr int kTailRowsF = SG_TAIL_ROWS_F32;
 
 template <typename MK, int SM>
 __device__ __forceinline__ float proj_u_f32(int j, int i, int H, int W, float uk, float pc, float pn, const MK& m,
