@@ -165,7 +165,7 @@ __global__ void k_apply_forces_f32(int H, int W, float* __restrict__ v, int ldv,
 // columns and walks kTailRowsF rows, each face projected once -- with float32 arithmetic in
 // place of the reference's float64 intermediates.
 #ifndef SG_TAIL_ROWS_F32
-#define SG_TAIL_ROWS_F32 8
+#define SG_TAIL_ROWS_F32 4
 #endif
 constexpr int kTailRowsF = SG_TAIL_ROWS_F32;
 
