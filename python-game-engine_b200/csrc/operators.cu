@@ -187,7 +187,7 @@ __global__ void k_project(int H, int W, T* __restrict__ u, int64_t ldu, T* __res
 // from the adjacent lane, so each face is projected once (plus one u face per warp edge and
 // row). Every value is formed by the same expressions as the separate passes, so the
 // results are identical to them.
-constexpr int kTailRows = 8;
+constexpr int kTailRows = 4;
 
 template <typename T, int MM, int SM>
 __global__ void __launch_bounds__(kBX * kBY) k_project_metrics(
